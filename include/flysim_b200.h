@@ -1,0 +1,281 @@
+/*
+ * flysim_b200.h — C ABI of the B200-native flysim step engine.
+ *
+ * The reference (yc-h/flysim) has no plugin or FFI layer.  Its seam for the
+ * per-timestep integration is the abstract class NetSim (code/NetSim.h:80-109:
+ * DoEvt, SetPp, RunInit, Run, FileOut), created by GetNewSim
+ * (code/main.cpp:259-266).  Inside Run() the hot path is the pair
+ * EqsGnl2::Activation / EqsGnl2::Spike (code/Eqs.h:928-930), called once per
+ * step on state held in raw heap arrays owned by EqsGnl2 (code/Eqs.h:973-1118).
+ *
+ * This header replaces that seam with plain C entry points:
+ *   - fs_model_*   host side: parse network.conf / network.pro and build the
+ *                  network exactly as Parser::CSta/parse/DefMacro
+ *                  (code/parser.cpp:51-1407) and NetSimGnl2::SetPp/PostSetPp
+ *                  (code/NetSimGnl2_BulPp.cpp:27-727) do.  No GPU needed.
+ *   - fs_create / fs_step / ...  device side: one handle owns all device
+ *                  memory of one network instance on one GPU.
+ *   - fs_batch_*   many independent instances in one persistent launch.
+ *
+ * Conventions: every call returns an int status (FS_OK = 0, >0 error codes
+ * below); fs_last_error() gives a message.  No exceptions cross the ABI.
+ * One host thread per handle.  No torch types anywhere.
+ */
+#ifndef FLYSIM_B200_H
+#define FLYSIM_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FS_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  FS_OK = 0,
+  FS_ERR_ARG = 1,          /* bad argument / inconsistent description      */
+  FS_ERR_CUDA = 2,         /* CUDA runtime error (message has details)     */
+  FS_ERR_NOMEM = 3,        /* device or host allocation failed             */
+  FS_ERR_CAPACITY = 4,     /* an output buffer was too small               */
+  FS_ERR_PARSE = 5,        /* .conf/.pro could not be parsed               */
+  FS_ERR_UNSUPPORTED = 6,  /* network uses a feature the chosen mode lacks */
+  FS_ERR_TIMEOUT = 7,      /* a bounded device wait gave up                */
+  FS_ERR_IO = 8,           /* file open / write failed                     */
+  FS_ERR_NODEVICE = 9      /* no CUDA device visible                       */
+};
+
+/* ---- receptor indices (order of EqsGnl2::BgInit, code/EqsGnl2.cpp:288-332) */
+enum { FS_AMPA = 0, FS_GABA = 1, FS_ACH = 2, FS_GCL = 3, FS_NMDA = 4, FS_NREC = 5 };
+
+/* ---- ActCtr bits: same values as code/Inc.h:253-280 --------------------- */
+#define FS_ACT_AMPA 1u
+#define FS_ACT_GABA 2u
+#define FS_ACT_NMDA 4u
+#define FS_ACT_GAP 8u
+#define FS_ACT_ACH 32u
+#define FS_ACT_GCL 64u
+#define FS_ACT_INJ 128u
+#define FS_ACT_LIF 256u
+#define FS_ACT_LTP 8192u
+#define FS_ACT_STD 16384u
+#define FS_ACT_STP 32768u
+
+/* ---- NState bits: same values as code/Inc.h:225-231 --------------------- */
+#define FS_NS_FIRE 1u
+#define FS_NS_SPIKE 2u
+#define FS_NS_LP_FIRE 4u
+#define FS_NS_LP_SPIKE 8u
+#define FS_NS_MEMDV_OVF 16u
+#define FS_NS_MEMDV_UDF 32u
+
+/* ---- numeric modes ------------------------------------------------------ */
+enum {
+  /* FP32, reference operation order, std::mt19937 drive stream, ziggurat
+   * injection noise: the spike raster equals the reference's (-t 1) bit for
+   * bit.  Synaptic delays must be 0. */
+  FS_MODE_COMPAT = 0,
+  /* FP32 state, Philox drive, aggregated conductances with per-synapse
+   * integer delays (delay ring), deterministic fixed-point delivery. */
+  FS_MODE_FP32 = 1,
+  /* Same algorithm as FS_MODE_FP32 with FP64 state: accuracy reference. */
+  FS_MODE_FP64 = 2
+};
+
+/* ---- network description (plain arrays; copied at fs_create) ----------- */
+
+/* Per-neuron parameters, all arrays of length n_neurons.  They are the fields
+ * of ParBase2/ParLIF/NeuRepPar2<RP3,RP4>/ParStp2/ParLP2 of the reference
+ * (code/neuron_affi.h:97-221, code/receptor.h:167-182) stored as structure of
+ * arrays.  Receptor-indexed arrays are receptor-major: a[r * n + i]. */
+typedef struct fs_neurons {
+  uint32_t n;
+  const float *Vth, *El, *gl, *Cm, *Vreset, *df, *ef, *dVmax;
+  const int32_t *RfPed, *SpiDy;
+  const float *Vrev;   /* [FS_NREC*n] */
+  const float *dfst;   /* [FS_NREC*n] */
+  const float *nmda_dfxt, *nmda_efst, *nmda_as, *nmda_mg;
+  const float *ext_g;  /* [FS_NREC*n] efficacy of the external drive synapse */
+  const float *pb;     /* [FS_NREC*n] initial drive probability per step     */
+  const uint32_t *act; /* initial ActCtr bits                                */
+  const float *inj_mean, *inj_std; /* initial injection current (nA)        */
+  /* short-term plasticity (code/NetSimGnl2_BulPp.cpp:186-200) */
+  const float *stp_pv, *stp_dfD, *stp_efD, *stp_aF, *stp_dfF, *stp_efF,
+              *stp_aCap, *stp_dfCap, *stp_aCar, *stp_dfCar, *stp_efCar;
+  /* long-term plasticity (code/NetSimGnl2_BulPp.cpp:180-183) */
+  const float *ltp_dfLP, *ltp_PosISI, *ltp_NegISI;
+  const int32_t *ltp_SpiLPDy;
+} fs_neurons;
+
+/* Reference-order synapse layout of one receptor (FS_MODE_COMPAT).
+ *  group gates: one gate per (presynaptic neuron, link) with >=2 targets,
+ *    (PSynFstGatA..L and PSynSloGat, code/NetSimGnl2_BulPp.cpp:393-464); the gate
+ *    decays with dfst of its first target gate_post0.
+ *  gather CSR by post: the gate indices summed into each post, in the order
+ *    of the reference's sorted PSyn* arrays (code/EqsGnl2.cpp:941-979).
+ *  single-target records: SynFst1/SynSlo1 (code/NetSimGnl2_BulPp.cpp:577-695)
+ *    after PostSetPp's sort by PosID; rec_pre is the reference's PreID (the
+ *    presynaptic POPULATION index, kept as the reference uses it). */
+typedef struct fs_rec_layout {
+  uint32_t n_gates;
+  const uint32_t *gate_pre, *gate_post0;
+  const float *gate_g;
+  const uint32_t *gather_rowptr; /* [n+1] */
+  const uint32_t *gather_gate;   /* [gather_rowptr[n]] */
+  uint32_t n_recs;
+  const uint32_t *rec_pre, *rec_post;
+  const float *rec_g;
+  const uint32_t *rec_rowptr;    /* [n+1] records of post i: [rowptr[i], rowptr[i+1]) */
+} fs_rec_layout;
+
+typedef struct fs_compat_layout {
+  fs_rec_layout rec[FS_NREC];
+  /* gap junction terms per neuron, in the order the reference accumulates
+   * them into Isyn (code/EqsGnl2.cpp:982-999 then :705-724):
+   *   Isyn[i] += g * (V[other] - V[i]) */
+  const uint32_t *gap_rowptr; /* [n+1] (may be NULL when there are none) */
+  const uint32_t *gap_other;
+  const float *gap_g;
+} fs_compat_layout;
+
+/* Flat synapse list for the production modes: one entry per (pre, post,
+ * receptor).  delay is in steps (0 = effect on the next step, as the
+ * reference). */
+typedef struct fs_syn_list {
+  uint64_t n;
+  const uint32_t *pre, *post;
+  const uint8_t *rec;
+  const float *g;
+  const uint16_t *delay;     /* may be NULL: all zero */
+} fs_syn_list;
+
+/* Tsodyks-Markram short-term plasticity for the production modes, per
+ * presynaptic neuron (arrays of length n, NULL = off for everybody).  The TM
+ * state (u, x) of a synapse depends only on its presynaptic spike train and
+ * these parameters, so it is kept once per presynaptic neuron. */
+typedef struct fs_tm_params {
+  const uint8_t *enabled;
+  const float *U, *tau_rec, *tau_fac; /* ms */
+} fs_tm_params;
+
+typedef struct fs_net_desc {
+  float dt;                 /* ms */
+  uint32_t act_ctr;         /* global ActCtr (STP/STD/LTP mode bits)      */
+  fs_neurons neurons;
+  const fs_compat_layout *compat; /* required by FS_MODE_COMPAT           */
+  const fs_syn_list *syn;         /* required by FS_MODE_FP32/FP64        */
+  const fs_tm_params *tm;         /* optional (production modes)          */
+} fs_net_desc;
+
+typedef struct fs_run_opts {
+  int mode;            /* FS_MODE_*                                       */
+  int device;          /* CUDA device ordinal                             */
+  uint32_t chunk_steps;/* steps per device launch batch (0 = default 1000)*/
+  uint64_t philox_key; /* production modes: drive stream key              */
+} fs_run_opts;
+
+/* Per-call step outputs (host memory, caller owned; NULL = not wanted). */
+typedef struct fs_step_out {
+  uint32_t *spike_count;   /* [nsteps]: number of neurons with SPIKE set   */
+  uint32_t *spike_idx;     /* ascending neuron ids, steps concatenated     */
+  uint64_t spike_cap;      /* capacity of spike_idx                         */
+  uint64_t spike_total;    /* out: number written                           */
+  float *V;                /* [nsteps*n] membrane potential after the step */
+  float *Irep;             /* [nsteps*FS_NREC*n] receptor currents (Nets.Irep) */
+  uint32_t *nstate;        /* [nsteps*n] NState after the step             */
+  /* gating variables of selected single-target records (GatingVariable
+   * output, code/NetSimGnl2_info.cpp:701-758); FS_MODE_COMPAT only */
+  const uint32_t *gv_sel;  /* (receptor << 28) | record index in fs_rec_layout order */
+  uint32_t gv_n;
+  float *gv_st;            /* [nsteps*gv_n] st after the step              */
+  float *gv_xt;            /* [nsteps*gv_n] xt after the step (NMDA)       */
+} fs_step_out;
+
+typedef struct fs_handle fs_handle;
+
+/* ---- library ------------------------------------------------------------ */
+int fs_abi_version(void);
+const char *fs_last_error(const fs_handle *h); /* h may be NULL: global error */
+int fs_device_count(int *count);
+
+/* ---- device engine: replaces EqsGnl2's state + Activation/Spike -------- */
+/* Allocates and uploads one network (code/NetSimGnl2_BulPp.cpp:27-727 is the
+ * reference's equivalent set-up). */
+int fs_create(const fs_net_desc *desc, const fs_run_opts *opts, fs_handle **out);
+int fs_destroy(fs_handle *h);
+/* VarInit + reseed (code/EqsGnl2.cpp:339-401, code/NetSimGnl2.cpp:313-330):
+ * mt_seed seeds the std::mt19937 drive stream (compat), jcong_seed the
+ * ziggurat congruential state (compat); production modes use philox_key and
+ * mt_seed as the stream counter offset. */
+int fs_reset(fs_handle *h, uint32_t mt_seed, uint32_t jcong_seed);
+/* DoEvt (code/NetSimGnl2.cpp:52-141) expressed as parameter writes on the
+ * neuron range [first, first+count).  They take effect at the next fs_step. */
+int fs_set_drive(fs_handle *h, uint32_t first, uint32_t count, int rec, float pb);
+int fs_set_act(fs_handle *h, uint32_t first, uint32_t count, uint32_t clear_mask, uint32_t set_mask);
+int fs_set_injection(fs_handle *h, uint32_t first, uint32_t count, float mean, float std);
+/* Runs nsteps steps of Activation+Spike (code/NetSimGnl2.cpp:231-264 minus
+ * events and output) and returns what the output writers need. */
+int fs_step(fs_handle *h, uint32_t nsteps, fs_step_out *out);
+/* Device-resident variant for timing: runs nsteps with no host copies; the
+ * per-step spike counts stay on the device. */
+int fs_run(fs_handle *h, uint32_t nsteps);
+/* Synchronise and report counters. */
+int fs_sync(fs_handle *h);
+int fs_stats(fs_handle *h, uint64_t *steps_done, uint64_t *spikes_total, uint64_t *kernel_launches);
+/* Average device duration (ms) of the dominant kernel of the last fs_run /
+ * fs_step call, measured with CUDA events on the engine stream. */
+int fs_kernel_time(fs_handle *h, double *ms_per_launch, uint64_t *launches);
+/* Copy state out (V, Count, NState) for checks; arrays of length n. */
+int fs_get_state(fs_handle *h, float *V, int32_t *Count, uint32_t *NState);
+/* Full conductance view for checks: RVs (FS_NREC*n) after the last step and
+ * Isyn (n). */
+int fs_get_syn_state(fs_handle *h, float *g, float *Isyn);
+
+/* ---- host model: parser + network builder (no GPU) --------------------- */
+typedef struct fs_model fs_model;
+typedef struct fs_model_opts {
+  float dt;              /* -dt (ms), default 0.1 */
+  uint32_t flags;        /* FS_ACT_STP / FS_ACT_STD / FS_ACT_LTP as on the CLI */
+  int user_seed_set;     /* -udfsed given (sets the STD bit too, as the reference) */
+  uint32_t user_seed;
+  int threads;           /* -t (affects set-up RNG draws only)          */
+  int repeats;           /* -rp                                          */
+  const char *out_mem, *out_spike, *out_rate; /* -om/-os/-or or NULL     */
+} fs_model_opts;
+
+int fs_model_load(const char *conf_path, const char *pro_path, const fs_model_opts *opts, fs_model **out);
+int fs_model_free(fs_model *m);
+const char *fs_model_error(void);
+/* View of the built network (valid until fs_model_free). */
+int fs_model_desc(fs_model *m, const fs_net_desc **desc);
+int fs_model_info(fs_model *m, uint32_t *n_neurons, uint32_t *n_pops, uint64_t *n_syn_entries,
+                  uint32_t *n_events, uint32_t *n_outputs);
+/* Seed used by repeat r (1-based), as rseeds[r-1] of the reference. */
+int fs_model_seed(fs_model *m, int repeat, uint32_t *seed);
+/* Runs the full protocol (all repeats) on the device engine and writes the
+ * output files of the .pro, exactly as NetSimGnl2::Run/FileOut
+ * (code/NetSimGnl2.cpp:266-358, code/NetSimGnl2_info.cpp:548-769). */
+int fs_model_run(fs_model *m, const fs_run_opts *opts, const char *out_dir, double *run_seconds);
+
+/* Engine plug-in: the NetSim seam as a table of C function pointers.  The
+ * protocol driver (events, repeats, output files) calls these; fs_model_run
+ * plugs in the device engine. */
+typedef struct fs_engine_vtbl {
+  int (*reset)(void *ctx, uint32_t mt_seed, uint32_t jcong_seed);
+  int (*set_drive)(void *ctx, uint32_t first, uint32_t count, int rec, float pb);
+  int (*set_act)(void *ctx, uint32_t first, uint32_t count, uint32_t clear_mask, uint32_t set_mask);
+  int (*set_injection)(void *ctx, uint32_t first, uint32_t count, float mean, float std);
+  int (*step)(void *ctx, uint32_t nsteps, fs_step_out *out);
+  const char *(*error)(void *ctx);
+} fs_engine_vtbl;
+int fs_model_run_with(fs_model *m, const fs_engine_vtbl *eng, void *ctx, const char *out_dir,
+                      uint32_t chunk_steps, double *run_seconds);
+/* The device engine's table (ctx = fs_handle*). */
+const fs_engine_vtbl *fs_device_engine(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
