@@ -1,0 +1,348 @@
+"""flysim_b200 — B200-native per-timestep integration for flysim networks.
+
+Python mirror of the C ABI in include/flysim_b200.h (ctypes; no torch types).
+The native library is built in-tree by :mod:`flysim_b200.build`; importing
+this package never falls back to Python or CPU code — every call that needs
+the engine goes to the CUDA library and fails loudly if it is missing.
+
+Reference interface mirrored: the flysim command line (code/main.cpp) and its
+NetSim seam (code/NetSim.h:80-109): load a .conf/.pro pair, run the protocol,
+get the .pro's output files; or drive the step engine directly (reset, drive
+and injection changes, steps) as NetSimGnl2::Run/DoEvt do.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+LIB_PATH = os.path.join(BUILD, "libflysim_b200.so")
+
+FS_OK, FS_ERR_ARG, FS_ERR_CUDA, FS_ERR_NOMEM, FS_ERR_CAPACITY, FS_ERR_PARSE, FS_ERR_UNSUPPORTED, \
+    FS_ERR_TIMEOUT, FS_ERR_IO, FS_ERR_NODEVICE = range(10)
+FS_AMPA, FS_GABA, FS_ACH, FS_GCL, FS_NMDA, FS_NREC = 0, 1, 2, 3, 4, 5
+FS_MODE_COMPAT, FS_MODE_FP32, FS_MODE_FP64 = 0, 1, 2
+MODES = {"compat": FS_MODE_COMPAT, "fp32": FS_MODE_FP32, "fp64": FS_MODE_FP64}
+ACT = dict(AMPA=1, GABA=2, NMDA=4, GAP=8, ACH=32, GCL=64, INJ=128, LIF=256, LTP=8192, STD=16384, STP=32768)
+NS_FIRE, NS_SPIKE = 1, 2
+DEFAULT_ACT = ACT["AMPA"] | ACT["GABA"] | ACT["NMDA"] | ACT["ACH"] | ACT["GCL"] | ACT["GAP"] | ACT["LIF"]
+
+_f = C.POINTER(C.c_float)
+_u32 = C.POINTER(C.c_uint32)
+_i32 = C.POINTER(C.c_int32)
+_u8 = C.POINTER(C.c_uint8)
+_u16 = C.POINTER(C.c_uint16)
+
+
+class FsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("flysim_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+class Neurons(C.Structure):
+    _fields_ = [("n", C.c_uint32)] + [(k, _f) for k in ("Vth", "El", "gl", "Cm", "Vreset", "df", "ef", "dVmax")] + \
+        [("RfPed", _i32), ("SpiDy", _i32), ("Vrev", _f), ("dfst", _f), ("nmda_dfxt", _f), ("nmda_efst", _f),
+         ("nmda_as", _f), ("nmda_mg", _f), ("ext_g", _f), ("pb", _f), ("act", _u32), ("inj_mean", _f),
+         ("inj_std", _f)] + \
+        [(k, _f) for k in ("stp_pv", "stp_dfD", "stp_efD", "stp_aF", "stp_dfF", "stp_efF", "stp_aCap",
+                           "stp_dfCap", "stp_aCar", "stp_dfCar", "stp_efCar")] + \
+        [("ltp_dfLP", _f), ("ltp_PosISI", _f), ("ltp_NegISI", _f), ("ltp_SpiLPDy", _i32)]
+
+
+class RecLayout(C.Structure):
+    _fields_ = [("n_gates", C.c_uint32), ("gate_pre", _u32), ("gate_post0", _u32), ("gate_g", _f),
+                ("gather_rowptr", _u32), ("gather_gate", _u32), ("n_recs", C.c_uint32), ("rec_pre", _u32),
+                ("rec_post", _u32), ("rec_g", _f), ("rec_rowptr", _u32)]
+
+
+class CompatLayout(C.Structure):
+    _fields_ = [("rec", RecLayout * FS_NREC), ("gap_rowptr", _u32), ("gap_other", _u32), ("gap_g", _f)]
+
+
+class SynList(C.Structure):
+    _fields_ = [("n", C.c_uint64), ("pre", _u32), ("post", _u32), ("rec", _u8), ("g", _f), ("delay", _u16)]
+
+
+class TmParams(C.Structure):
+    _fields_ = [("enabled", _u8), ("U", _f), ("tau_rec", _f), ("tau_fac", _f)]
+
+
+class NetDesc(C.Structure):
+    _fields_ = [("dt", C.c_float), ("act_ctr", C.c_uint32), ("neurons", Neurons),
+                ("compat", C.POINTER(CompatLayout)), ("syn", C.POINTER(SynList)), ("tm", C.POINTER(TmParams))]
+
+
+class RunOpts(C.Structure):
+    _fields_ = [("mode", C.c_int), ("device", C.c_int), ("chunk_steps", C.c_uint32), ("philox_key", C.c_uint64)]
+
+
+class StepOut(C.Structure):
+    _fields_ = [("spike_count", _u32), ("spike_idx", _u32), ("spike_cap", C.c_uint64), ("spike_total", C.c_uint64),
+                ("V", _f), ("Irep", _f), ("nstate", _u32), ("gv_sel", _u32), ("gv_n", C.c_uint32),
+                ("gv_st", _f), ("gv_xt", _f)]
+
+
+class ModelOpts(C.Structure):
+    _fields_ = [("dt", C.c_float), ("flags", C.c_uint32), ("user_seed_set", C.c_int), ("user_seed", C.c_uint32),
+                ("threads", C.c_int), ("repeats", C.c_int), ("out_mem", C.c_char_p), ("out_spike", C.c_char_p),
+                ("out_rate", C.c_char_p)]
+
+
+class EngineVtbl(C.Structure):
+    _fields_ = [("reset", C.c_void_p), ("set_drive", C.c_void_p), ("set_act", C.c_void_p),
+                ("set_injection", C.c_void_p), ("step", C.c_void_p), ("error", C.c_void_p)]
+
+
+_LIB: Optional[C.CDLL] = None
+
+
+def lib() -> C.CDLL:
+    """The native library (built in-tree).  Raises if it was not built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise FsError(FS_ERR_IO, "native library missing: %s (run flysim_b200.build.build())" % LIB_PATH)
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    sig = {
+        "fs_abi_version": (C.c_int, []),
+        "fs_last_error": (C.c_char_p, [vp]),
+        "fs_device_count": (C.c_int, [C.POINTER(C.c_int)]),
+        "fs_create": (C.c_int, [C.POINTER(NetDesc), C.POINTER(RunOpts), C.POINTER(vp)]),
+        "fs_destroy": (C.c_int, [vp]),
+        "fs_reset": (C.c_int, [vp, C.c_uint32, C.c_uint32]),
+        "fs_set_drive": (C.c_int, [vp, C.c_uint32, C.c_uint32, C.c_int, C.c_float]),
+        "fs_set_act": (C.c_int, [vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]),
+        "fs_set_injection": (C.c_int, [vp, C.c_uint32, C.c_uint32, C.c_float, C.c_float]),
+        "fs_step": (C.c_int, [vp, C.c_uint32, C.POINTER(StepOut)]),
+        "fs_run": (C.c_int, [vp, C.c_uint32]),
+        "fs_sync": (C.c_int, [vp]),
+        "fs_stats": (C.c_int, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+        "fs_kernel_time": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
+        "fs_debug_expf": (C.c_int, [_f, _f, C.c_uint64]),
+        "fs_get_state": (C.c_int, [vp, _f, _i32, _u32]),
+        "fs_get_syn_state": (C.c_int, [vp, _f, _f]),
+        "fs_model_load": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(ModelOpts), C.POINTER(vp)]),
+        "fs_model_free": (C.c_int, [vp]),
+        "fs_model_error": (C.c_char_p, []),
+        "fs_model_desc": (C.c_int, [vp, C.POINTER(C.POINTER(NetDesc))]),
+        "fs_model_info": (C.c_int, [vp, _u32, _u32, C.POINTER(C.c_uint64), _u32, _u32]),
+        "fs_model_seed": (C.c_int, [vp, C.c_int, _u32]),
+        "fs_model_run": (C.c_int, [vp, C.POINTER(RunOpts), C.c_char_p, C.POINTER(C.c_double)]),
+        "fs_model_run_with": (C.c_int, [vp, C.POINTER(EngineVtbl), vp, C.c_char_p, C.c_uint32,
+                                        C.POINTER(C.c_double)]),
+        "fs_device_engine": (C.POINTER(EngineVtbl), []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = L
+    return L
+
+
+def exported_symbols() -> Sequence[str]:
+    return [n for n in ("fs_abi_version", "fs_last_error", "fs_device_count", "fs_create", "fs_destroy",
+                        "fs_reset", "fs_set_drive", "fs_set_act", "fs_set_injection", "fs_step", "fs_run",
+                        "fs_sync", "fs_stats", "fs_kernel_time", "fs_debug_expf", "fs_get_state",
+                        "fs_get_syn_state", "fs_model_load", "fs_model_free", "fs_model_error",
+                        "fs_model_desc", "fs_model_info", "fs_model_seed", "fs_model_run",
+                        "fs_model_run_with", "fs_device_engine")]
+
+
+def _check(rc: int, h=None):
+    if rc != FS_OK:
+        L = lib()
+        msg = L.fs_last_error(h) if h is not None else L.fs_last_error(None)
+        raise FsError(rc, (msg or b"").decode(errors="replace"))
+
+
+def device_count() -> int:
+    c = C.c_int(0)
+    lib().fs_device_count(C.byref(c))
+    return c.value
+
+
+# ---------------------------------------------------------------------------
+class Model:
+    """A parsed and built network (Parser + SetPp of the reference)."""
+
+    def __init__(self, conf: str, pro: str, dt: float = 0.1, stp: bool = False, std: bool = False,
+                 ltp: bool = False, repeats: int = 1, threads: int = 1, user_seed: Optional[int] = None,
+                 out_mem: Optional[str] = None, out_spike: Optional[str] = None, out_rate: Optional[str] = None):
+        L = lib()
+        o = ModelOpts()
+        o.dt = dt
+        o.flags = (ACT["STP"] if stp else 0) | (ACT["STD"] if std else 0) | (ACT["LTP"] if ltp else 0)
+        o.user_seed_set = 1 if user_seed is not None else 0
+        o.user_seed = int(user_seed or 0)
+        o.threads = threads
+        o.repeats = repeats
+        o.out_mem = out_mem.encode() if out_mem else None
+        o.out_spike = out_spike.encode() if out_spike else None
+        o.out_rate = out_rate.encode() if out_rate else None
+        h = C.c_void_p()
+        rc = L.fs_model_load(conf.encode(), pro.encode(), C.byref(o), C.byref(h))
+        if rc != FS_OK:
+            raise FsError(rc, L.fs_model_error().decode(errors="replace"))
+        self._h = h
+        self.dt = dt
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fs_model_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def desc(self) -> "C.POINTER(NetDesc)":
+        p = C.POINTER(NetDesc)()
+        _check(lib().fs_model_desc(self._h, C.byref(p)))
+        return p
+
+    def info(self) -> Dict[str, int]:
+        a, b, d, e = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
+        s = C.c_uint64()
+        _check(lib().fs_model_info(self._h, C.byref(a), C.byref(b), C.byref(s), C.byref(d), C.byref(e)))
+        return dict(neurons=a.value, populations=b.value, synapses=s.value, events=d.value, outputs=e.value)
+
+    def seed(self, repeat: int = 1) -> int:
+        v = C.c_uint32()
+        _check(lib().fs_model_seed(self._h, repeat, C.byref(v)))
+        return v.value
+
+    def run(self, out_dir: str, mode: str = "compat", device: int = 0, chunk_steps: int = 0) -> float:
+        """Runs the whole protocol on the GPU and writes the .pro's output files."""
+        o = RunOpts(MODES[mode], device, chunk_steps, 0)
+        secs = C.c_double()
+        rc = lib().fs_model_run(self._h, C.byref(o), out_dir.encode(), C.byref(secs))
+        if rc != FS_OK:
+            raise FsError(rc, lib().fs_model_error().decode(errors="replace"))
+        return secs.value
+
+    def run_with(self, vtbl, ctx, out_dir: str, chunk_steps: int = 1000) -> float:
+        secs = C.c_double()
+        rc = lib().fs_model_run_with(self._h, vtbl, ctx, out_dir.encode(), chunk_steps, C.byref(secs))
+        if rc != FS_OK:
+            raise FsError(rc, lib().fs_model_error().decode(errors="replace"))
+        return secs.value
+
+
+# ---------------------------------------------------------------------------
+class Engine:
+    """One network instance on one GPU (fs_create ... fs_destroy)."""
+
+    def __init__(self, desc, mode: str = "compat", device: int = 0, chunk_steps: int = 0, philox_key: int = 0):
+        L = lib()
+        self._keep = getattr(desc, "_keep", None)
+        o = RunOpts(MODES[mode], device, chunk_steps, philox_key)
+        h = C.c_void_p()
+        dp = desc if isinstance(desc, C._Pointer) else C.pointer(desc)
+        rc = L.fs_create(dp, C.byref(o), C.byref(h))
+        if rc != FS_OK:
+            raise FsError(rc, L.fs_last_error(None).decode(errors="replace"))
+        self._h = h
+        self.n = dp.contents.neurons.n
+        self.mode = mode
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def reset(self, seed: int, jcong_seed: Optional[int] = None):
+        _check(lib().fs_reset(self._h, seed, seed if jcong_seed is None else jcong_seed), self._h)
+
+    def set_drive(self, first: int, count: int, rec: int, pb: float):
+        _check(lib().fs_set_drive(self._h, first, count, rec, pb), self._h)
+
+    def set_act(self, first: int, count: int, clear_mask: int, set_mask: int):
+        _check(lib().fs_set_act(self._h, first, count, clear_mask, set_mask), self._h)
+
+    def set_injection(self, first: int, count: int, mean: float, std: float):
+        _check(lib().fs_set_injection(self._h, first, count, mean, std), self._h)
+
+    def step(self, nsteps: int, want_V: bool = False, spike_cap: Optional[int] = None):
+        """Runs nsteps; returns (list of per-step spike index arrays, V or None)."""
+        counts = np.zeros(nsteps, np.uint32)
+        cap = spike_cap if spike_cap is not None else max(1024, nsteps * self.n)
+        idx = np.zeros(cap, np.uint32)
+        V = np.zeros((nsteps, self.n), np.float32) if want_V else None
+        so = StepOut()
+        so.spike_count = counts.ctypes.data_as(_u32)
+        so.spike_idx = idx.ctypes.data_as(_u32)
+        so.spike_cap = cap
+        if V is not None:
+            so.V = V.ctypes.data_as(_f)
+        _check(lib().fs_step(self._h, nsteps, C.byref(so)), self._h)
+        offs = np.concatenate([[0], np.cumsum(counts.astype(np.int64))])
+        spikes = [idx[offs[i]:offs[i + 1]].copy() for i in range(nsteps)]
+        return spikes, V
+
+    def run(self, nsteps: int):
+        _check(lib().fs_run(self._h, nsteps), self._h)
+
+    def sync(self):
+        _check(lib().fs_sync(self._h), self._h)
+
+    def stats(self):
+        a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        _check(lib().fs_stats(self._h, C.byref(a), C.byref(b), C.byref(c)), self._h)
+        return dict(steps=a.value, spikes=b.value, launches=c.value)
+
+    def kernel_time(self):
+        ms, n = C.c_double(), C.c_uint64()
+        _check(lib().fs_kernel_time(self._h, C.byref(ms), C.byref(n)), self._h)
+        return ms.value, n.value
+
+    def state(self):
+        V = np.zeros(self.n, np.float32)
+        cnt = np.zeros(self.n, np.int32)
+        ns = np.zeros(self.n, np.uint32)
+        _check(lib().fs_get_state(self._h, V.ctypes.data_as(_f), cnt.ctypes.data_as(_i32),
+                                  ns.ctypes.data_as(_u32)), self._h)
+        return V, cnt, ns
+
+    def syn_state(self):
+        g = np.zeros(FS_NREC * self.n, np.float32)
+        isyn = np.zeros(self.n, np.float32)
+        _check(lib().fs_get_syn_state(self._h, g.ctypes.data_as(_f), isyn.ctypes.data_as(_f)), self._h)
+        return g.reshape(FS_NREC, self.n), isyn
+
+
+def device_engine_vtbl():
+    return lib().fs_device_engine()
+
+
+def debug_expf(x: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.zeros_like(x)
+    _check(lib().fs_debug_expf(x.ctypes.data_as(_f), y.ctypes.data_as(_f), x.size))
+    return y
+
+
+from .network import desc_from_arrays, NetArrays  # noqa: E402  (array-built networks)

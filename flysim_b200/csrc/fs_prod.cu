@@ -1,0 +1,931 @@
+// Production engine of the flysim step (FS_MODE_FP32 / FS_MODE_FP64).
+//
+// Same neuron model as the reference (VmEul + firing, code/EqsGnl2.cpp:152-251;
+// external Bernoulli drive per receptor, code/EqsGnl2.cpp:284-337), with the
+// synapse side restructured for the GPU:
+//
+//  * Linear receptors (AMPA, GABA, ACh, GluCl).  Every synapse gate of the
+//    reference obeys st <- st + inc on a presynaptic spike, st <- st*df
+//    otherwise (code/EqsGnl2.cpp:404-480, :866-917), and the post-synaptic
+//    conductance is sum(g*st).  With df shared by all targets of a presynaptic
+//    neuron, that sum obeys G(t) = df*G(t-1) + sum_spikes g*c, with
+//    c = inc + st_pre(t-1)*(1-df) computed once per spike from a per-neuron
+//    gate st_pre.  So a spike pushes g*c into a delay ring
+//    ring[receptor][(t+delay) mod slots][post] (64-bit fixed point, 2^-40 nS:
+//    integer atomics make the sum independent of arrival order), and each post
+//    folds its slot into G once per step.
+//  * NMDA.  The gate s is nonlinear in its own state (code/EqsGnl2.cpp:493) but
+//    depends only on the presynaptic spike train, so x_pre/s_pre are kept per
+//    presynaptic neuron, s_pre(t) is stored in a history ring, and each post
+//    pulls sum(g * s_pre(t-delay)) over its NMDA in-edges every step.
+//  * Drive: counter-based Philox-4x32-10 (Salmon et al., SC'11) keyed by
+//    (step, neuron), so no generator state is shared.
+//
+// One persistent cooperative kernel runs many steps.  A warp owns a chunk of
+// up to 32 consecutive post neurons (NMDA pull + neuron update + pushes of its
+// spikes).  Every value a neuron reads from another neuron was produced at
+// least min_delay steps earlier, so blocks only synchronise (bounded-wait grid
+// barrier) once every max(min_delay, 1) steps; the ring depth
+// slots = max_delay + min_delay + 2 keeps reuse of a slot out of the interval
+// that still reads it.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "fs_prod.cuh"
+#include "fs_device.cuh"
+
+namespace fsp {
+
+constexpr double kFix = 1099511627776.0;        // 2^40
+constexpr double kInvFix = 9.094947017729282e-13;  // 2^-40
+constexpr uint32_t kEdgeBudget = 256;            // NMDA in-edges per chunk round
+constexpr uint32_t kThreads = 256;
+
+enum { PL_NONE = 0, PL_STD = 1, PL_STP = 2, PL_TM = 3 };
+
+struct Params {
+  uint32_t n, slots, interval, nlin;
+  int lin_of_rec[4];
+  const float *Vth, *El, *gl, *Cm, *Vreset, *df, *ef, *dVmax;
+  const int32_t *RfPed, *SpiDy;
+  const float *Vrev, *dfst, *nmda_dfxt, *nmda_efst, *nmda_as, *nmda_mg, *ext_g, *pb;
+  const uint32_t *act;
+  const float *inj_mean, *inj_std;
+  const float *pdf;                      // [4n] decay of st_pre per linear receptor
+  const float *p_dfxt, *p_dfst, *p_efas; // NMDA presynaptic kinetics
+  const uint8_t *proj;                   // receptors a neuron projects with (bit r)
+  int plast;
+  const float *stp_pv, *stp_dfD, *stp_efD, *stp_aF, *stp_dfF, *stp_efF, *stp_aCap, *stp_dfCap,
+      *stp_aCar, *stp_dfCar, *stp_efCar;
+  const uint8_t *tm_on;
+  const float *tm_U, *tm_dfr, *tm_dff;
+  void *V, *G, *ext_st, *ext_x, *ext_s, *st_pre, *x_pre, *s_pre, *s_hist;
+  int32_t *Count;
+  uint32_t *NS;
+  float *D, *F, *Cap, *Car, *tm_u, *tm_x;
+  unsigned long long *ring;
+  const uint32_t *out_row, *out_code;
+  const float *out_w;
+  const uint32_t *in_row, *in_code;
+  const float *in_w;
+  const uint32_t *chunk_beg;
+  const uint32_t *block_chunk;
+  uint32_t key0, key1;
+  uint64_t t0;
+  uint32_t nsteps;
+  uint32_t *bits;
+  uint32_t words;
+  uint32_t *counts;
+  float *outV;
+  unsigned int *bar;
+  int *err;
+};
+
+// ---- Philox-4x32-10 -------------------------------------------------------
+__device__ __forceinline__ void philox(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c[0]), lo0 = 0xD2511F53u * c[0];
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]), lo1 = 0xCD9E8D57u * c[2];
+    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+__device__ __forceinline__ float u24(uint32_t x) { return (float)(x >> 8) * 5.9604644775390625e-08f; }
+
+// ---- bounded grid barrier ---------------------------------------------------
+__device__ __forceinline__ bool grid_sync(unsigned int *bar, unsigned int target, int *err) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(bar, 1u);
+    unsigned int spins = 0;
+    for (;;) {
+      if (*(volatile unsigned int *)bar >= target) break;
+      if (*(volatile int *)err) break;
+      if (++spins > (1u << 22)) {
+        atomicExch(err, 2);
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *(volatile int *)err == 0;
+}
+
+template <class T>
+__device__ __forceinline__ T ldcg_t(const T *p);
+template <>
+__device__ __forceinline__ float ldcg_t<float>(const float *p) { return __ldcg(p); }
+template <>
+__device__ __forceinline__ double ldcg_t<double>(const double *p) { return __ldcg(p); }
+
+template <class T>
+__device__ __forceinline__ T exp_t(T x);
+template <>
+__device__ __forceinline__ float exp_t<float>(float x) { return expf(x); }
+template <>
+__device__ __forceinline__ double exp_t<double>(double x) { return exp(x); }
+
+// ---- one chunk: NMDA pull, neuron update, presynaptic update, push --------
+template <class T>
+__device__ __forceinline__ void run_chunk(const Params &P, uint32_t c, uint64_t t, uint32_t s, uint32_t tm,
+                                          uint32_t lane, T *wprod) {
+  const uint32_t n = P.n, slots = P.slots;
+  const uint32_t p0 = P.chunk_beg[c], p1 = P.chunk_beg[c + 1];
+  const bool own = lane < (p1 - p0);
+  const uint32_t p = p0 + lane;
+  const uint32_t slot_prev = (tm == 0) ? slots - 1 : tm - 1;
+
+  // NMDA pull: G_nmda of the previous step's spike phase
+  T gn = (T)0;
+  if (P.in_row) {
+    const uint32_t eb = P.in_row[p0], ee = P.in_row[p1];
+    const uint32_t mb = own ? P.in_row[p] : 0u, me = own ? P.in_row[p + 1] : 0u;
+    const T *sh = (const T *)P.s_hist;
+    for (uint32_t base = eb; base < ee; base += kEdgeBudget) {
+      uint32_t code[8];
+      float w[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const uint32_t e = base + lane + 32u * u;
+        code[u] = 0xffffffffu;
+        w[u] = 0.0f;
+        if (e < ee) {
+          code[u] = __ldg(P.in_code + e);
+          w[u] = __ldg(P.in_w + e);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        T v = (T)0;
+        if (code[u] != 0xffffffffu) {
+          const uint32_t pre = code[u] & 0xffffffu, d = code[u] >> 24;
+          uint32_t sl = tm + slots - 1u - d;
+          if (sl >= slots) sl -= slots;
+          v = (T)w[u] * ldcg_t<T>(sh + (size_t)sl * n + pre);
+        }
+        wprod[lane + 32u * u] = v;
+      }
+      __syncwarp();
+      if (own) {
+        const uint32_t a = max(mb, base), b = min(me, base + kEdgeBudget);
+        for (uint32_t e = a; e < b; e++) gn += wprod[e - base];
+      }
+      __syncwarp();
+    }
+  }
+
+  bool spk = false;
+  T cinc[4] = {(T)0, (T)0, (T)0, (T)0};
+  if (own) {
+    const uint32_t a = P.act[p];
+    T *G = (T *)P.G, *est = (T *)P.ext_st;
+    T g[5];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      g[r] = (T)0;
+      const int ri = P.lin_of_rec[r];
+      if (ri >= 0) {
+        unsigned long long *rp = P.ring + ((size_t)ri * slots + slot_prev) * n + p;
+        const long long v = (long long)__ldcg(rp);
+        if (v) __stcg(rp, 0ull);
+        T Gr = G[(size_t)r * n + p];
+        Gr = (T)P.dfst[(size_t)r * n + p] * Gr + (T)((double)v * kInvFix);
+        G[(size_t)r * n + p] = Gr;
+        g[r] = Gr;
+      }
+    }
+    g[FS_NMDA] = gn;
+    // external drive (BgInit)
+    uint32_t rnd[4] = {(uint32_t)t, (uint32_t)(t >> 32), p, 0u};
+    philox(rnd, P.key0, P.key1);
+    const uint32_t bitsr[4] = {FS_ACT_AMPA, FS_ACT_GABA, FS_ACT_ACH, FS_ACT_GCL};
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      if (a & bitsr[r]) {
+        const float pb = P.pb[(size_t)r * n + p];
+        T st = est[(size_t)r * n + p];
+        if (pb > u24(rnd[r])) st = st + (T)1;
+        else st = st * (T)P.dfst[(size_t)r * n + p];
+        est[(size_t)r * n + p] = st;
+        g[r] = g[r] + (T)P.ext_g[(size_t)r * n + p] * st;
+      }
+    }
+    T isyn = (T)0;
+    if (a & (FS_ACT_NMDA | FS_ACT_INJ)) {
+      uint32_t r2[4] = {(uint32_t)t, (uint32_t)(t >> 32), p, 1u};
+      philox(r2, P.key0, P.key1);
+      if (a & FS_ACT_NMDA) {
+        T *ex = (T *)P.ext_x, *es = (T *)P.ext_s;
+        const float pb = P.pb[(size_t)FS_NMDA * n + p];
+        T xt = ex[p], st = es[p];
+        if (pb > u24(r2[0])) xt = xt + (T)1;
+        else xt = xt * (T)P.nmda_dfxt[p];
+        st = (T)P.dfst[(size_t)FS_NMDA * n + p] * st + (T)P.nmda_efst[p] * (T)P.nmda_as[p] * xt * ((T)1 - st);
+        ex[p] = xt;
+        es[p] = st;
+        g[FS_NMDA] = g[FS_NMDA] + (T)P.ext_g[(size_t)FS_NMDA * n + p] * st;
+      }
+      if (a & FS_ACT_INJ) {  // Box-Muller normal
+        const double u1 = ((double)(r2[1] >> 8) + 1.0) * 5.9604644775390625e-08;
+        const double u2 = (double)(r2[2] >> 8) * 5.9604644775390625e-08;
+        const double z = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+        isyn = (T)P.inj_mean[p] + (T)P.inj_std[p] * (T)z;
+      }
+    }
+    // VmEul + firing (code/EqsGnl2.cpp:152-251)
+    T *Vp = (T *)P.V;
+    T V = Vp[p];
+    int32_t cnt = P.Count[p];
+    uint32_t ns = P.NS[p];
+    const int32_t rf = P.RfPed[p], sd = P.SpiDy[p];
+    const T vreset = (T)P.Vreset[p];
+    bool fire_now = false;
+    if (ns & FS_NS_FIRE) {
+      fire_now = true;
+    } else {
+      const T v = V;
+      const T Ir0 = g[FS_AMPA] * ((T)P.Vrev[(size_t)FS_AMPA * n + p] - v);
+      const T Ir1 = g[FS_GABA] * ((T)P.Vrev[(size_t)FS_GABA * n + p] - v);
+      const T Ir2 = g[FS_NMDA] * ((T)P.Vrev[(size_t)FS_NMDA * n + p] - v) /
+                    ((T)1 + (T)P.nmda_mg[p] * exp_t<T>((T)-0.062 * v) / (T)3.57);
+      const T Ir3 = g[FS_ACH] * ((T)P.Vrev[(size_t)FS_ACH * n + p] - v);
+      const T Ir4 = g[FS_GCL] * ((T)P.Vrev[(size_t)FS_GCL * n + p] - v);
+      T I = Ir0 + Ir1 + Ir2 + Ir3 + Ir4 + isyn * (T)1e3 + (T)P.gl[p] * (T)P.El[p] * (T)1e3;
+      I = (T)1e-3 * I / (T)P.Cm[p];
+      const T dv = (T)P.dVmax[p];
+      if (I > dv) {
+        I = dv;
+        ns = (ns | FS_NS_MEMDV_OVF) & ~FS_NS_MEMDV_UDF;
+      } else if (I < -dv) {
+        I = -dv;
+        ns = (ns & ~FS_NS_MEMDV_OVF) | FS_NS_MEMDV_UDF;
+      } else {
+        ns &= ~(FS_NS_MEMDV_OVF | FS_NS_MEMDV_UDF);
+      }
+      V = (T)P.df[p] * v + (T)P.ef[p] * I;
+      if (V > (T)P.Vth[p]) {
+        ns |= FS_NS_FIRE;
+        fire_now = true;
+      }
+    }
+    if (fire_now) {
+      if (cnt < rf) {
+        V = (cnt == 0) ? (T)0 : vreset;
+        if (cnt == sd) ns |= FS_NS_SPIKE;
+        else ns &= ~FS_NS_SPIKE;
+        cnt++;
+      } else {
+        cnt = 0;
+        ns &= ~FS_NS_FIRE;
+      }
+    }
+    Vp[p] = V;
+    P.Count[p] = cnt;
+    P.NS[p] = ns;
+    if (P.outV) P.outV[(size_t)s * n + p] = (float)V;
+    spk = (ns & FS_NS_SPIKE) != 0;
+    // presynaptic state: increment per spike, then plasticity update
+    const uint8_t pj = P.proj[p];
+    if (pj) {
+      T inc = (T)1;
+      if (P.plast == PL_STD) inc = (T)P.D[p];
+      else if (P.plast == PL_STP) inc = (T)P.D[p] * (T)P.F[p];
+      else if (P.plast == PL_TM && P.tm_on[p]) {
+        T u = (T)P.tm_u[p], x = (T)P.tm_x[p];
+        const T U = (T)P.tm_U[p];
+        if (spk) {
+          u = u + U * ((T)1 - u);
+          const T rel = u * x;
+          inc = rel;
+          x = x - rel;
+        } else {
+          u = U + (u - U) * (T)P.tm_dff[p];
+          x = (T)1 + (x - (T)1) * (T)P.tm_dfr[p];
+        }
+        P.tm_u[p] = (float)u;
+        P.tm_x[p] = (float)x;
+      }
+      T *sp = (T *)P.st_pre;
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        if (pj & (1u << r)) {
+          T st = sp[(size_t)r * n + p];
+          const T pd = (T)P.pdf[(size_t)r * n + p];
+          if (spk) {
+            cinc[r] = inc + st * ((T)1 - pd);
+            st = st + inc;
+          } else {
+            st = st * pd;
+          }
+          sp[(size_t)r * n + p] = st;
+        }
+      }
+      if (pj & (1u << FS_NMDA)) {
+        T *xp = (T *)P.x_pre, *sq = (T *)P.s_pre;
+        T x = xp[p], sv = sq[p];
+        if (spk) x = x + inc;
+        else x = x * (T)P.p_dfxt[p];
+        sv = (T)P.p_dfst[p] * sv + (T)P.p_efas[p] * x * ((T)1 - sv);
+        xp[p] = x;
+        sq[p] = sv;
+        __stcg((T *)P.s_hist + (size_t)tm * n + p, sv);
+      }
+      if (P.plast == PL_STD) {
+        P.D[p] = spk ? P.D[p] * (1.0f - P.stp_pv[p]) : P.stp_dfD[p] * P.D[p] + P.stp_efD[p];
+      } else if (P.plast == PL_STP) {
+        float Dv = P.D[p], Fv = P.F[p], Cp = P.Cap[p], Cr = P.Car[p];
+        if (spk) {
+          Cr += P.stp_aCar[p];
+          Cp += P.stp_aCap[p];
+          Fv += (Cp + Cr) * (1.0f - Fv) * P.stp_aF[p];
+          Dv *= (1.0f - P.stp_pv[p] * Fv);
+        } else {
+          Cr = P.stp_dfCar[p] * Cr + P.stp_efCar[p];
+          Cp = P.stp_dfCap[p] * Cp;
+          Fv = P.stp_dfF[p] * Fv + P.stp_efF[p] * (Cp + Cr) * (1.0f - Fv) * P.stp_aF[p];
+          Dv = P.stp_dfD[p] * Dv + P.stp_efD[p];
+        }
+        P.D[p] = Dv; P.F[p] = Fv; P.Cap[p] = Cp; P.Car[p] = Cr;
+      }
+    }
+    if (spk && P.bits) atomicOr(P.bits + (size_t)s * P.words + (p >> 5), 1u << (p & 31));
+  }
+  // spike count and pushes of this warp's spikes
+  uint32_t m = __ballot_sync(fsd::kFull, spk);
+  if (lane == 0 && m) atomicAdd(P.counts + s, (unsigned)__popc(m));
+  while (m) {
+    const int j = __ffs(m) - 1;
+    m &= m - 1;
+    const uint32_t q = p0 + (uint32_t)j;
+    T cj[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) cj[r] = __shfl_sync(fsd::kFull, cinc[r], j);
+    const uint32_t ob = P.out_row[q], oe = P.out_row[q + 1];
+    for (uint32_t e = ob + lane; e < oe; e += 32) {
+      const uint32_t code = __ldg(P.out_code + e);
+      const float w = __ldg(P.out_w + e);
+      const uint32_t post = code & 0x3fffffu, r = (code >> 22) & 3u, d = code >> 24;
+      uint32_t sl = tm + d;
+      if (sl >= slots) sl -= slots;
+      const T cv = (r == 0) ? cj[0] : (r == 1) ? cj[1] : (r == 2) ? cj[2] : cj[3];
+      const T val = (T)w * cv;
+      const long long fx = __double2ll_rn((double)val * kFix);
+      const int ri = P.lin_of_rec[r];
+      atomicAdd(P.ring + ((size_t)ri * slots + sl) * n + post, (unsigned long long)fx);
+    }
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_prod(const __grid_constant__ Params P) {
+  __shared__ T wbuf[kThreads / 32][kEdgeBudget];
+  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const uint32_t cb = P.block_chunk[blockIdx.x], ce = P.block_chunk[blockIdx.x + 1];
+  uint32_t nbar = 0;
+  uint32_t tm = (uint32_t)(P.t0 % P.slots);
+  for (uint32_t s = 0; s < P.nsteps; s++) {
+    const uint64_t t = P.t0 + s;
+    for (uint32_t c = cb + wid; c < ce; c += nw) run_chunk<T>(P, c, t, s, tm, lane, wbuf[wid]);
+    if (++tm == P.slots) tm = 0;
+    if (((s + 1) % P.interval) == 0 && s + 1 < P.nsteps) {
+      nbar++;
+      if (!grid_sync(P.bar, nbar * gridDim.x, P.err)) return;
+    }
+  }
+}
+
+// ---- host side -------------------------------------------------------------
+struct Prod {
+  bool fp64 = false;
+  uint32_t n = 0, sm = 148;
+  Params P{};
+  std::vector<void *> allocs;
+  uint64_t t = 0;  // steps done since reset
+  uint32_t d_min = 0, d_max = 0;
+  uint32_t blocks = 0, chunks = 0;
+  uint64_t lin_edges = 0, nmda_edges = 0;
+  uint32_t nlin = 0;
+  uint32_t chunk_steps = 1000;
+  // per-launch buffers
+  uint32_t *counts = nullptr, *bits = nullptr, *offsets = nullptr, *idx = nullptr;
+  float *outV = nullptr;
+  uint64_t cap_steps = 0, outv_steps = 0;
+  unsigned int *bar = nullptr;
+  int *err = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  double ms = 0.0;
+  uint64_t kl = 0;
+  uint64_t key = 0;
+  std::vector<uint32_t> host_counts;
+};
+
+namespace {
+
+template <class X>
+int dal(Prod *p, X **ptr, size_t count, std::string &err) {
+  *ptr = nullptr;
+  if (!count) return FS_OK;
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, count * sizeof(X));
+  if (e != cudaSuccess) {
+    err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    return FS_ERR_NOMEM;
+  }
+  p->allocs.push_back(q);
+  *ptr = (X *)q;
+  return FS_OK;
+}
+template <class X>
+int dup(Prod *p, X **ptr, const X *src, size_t count, cudaStream_t st, std::string &err) {
+  int rc = dal(p, ptr, count, err);
+  if (rc || !count) return rc;
+  cudaError_t e = src ? cudaMemcpyAsync(*ptr, src, count * sizeof(X), cudaMemcpyHostToDevice, st)
+                      : cudaMemsetAsync(*ptr, 0, count * sizeof(X), st);
+  if (e != cudaSuccess) {
+    err = std::string("upload: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  return FS_OK;
+}
+
+int ensure_buffers(Prod *p, uint32_t steps, bool wantV, std::string &err) {
+  int rc;
+  if (steps > p->cap_steps) {
+    const uint32_t words = (p->n + 31) / 32;
+    if ((rc = dal(p, &p->counts, steps, err)) || (rc = dal(p, &p->bits, (size_t)steps * words, err)) ||
+        (rc = dal(p, &p->offsets, (size_t)steps + 1, err)) || (rc = dal(p, &p->idx, (size_t)steps * p->n, err)))
+      return rc;
+    p->cap_steps = steps;
+  }
+  if (wantV && steps > p->outv_steps) {
+    if ((rc = dal(p, &p->outV, (size_t)steps * p->n, err))) return rc;
+    p->outv_steps = steps;
+  }
+  return FS_OK;
+}
+
+int launch(Prod *p, uint32_t nsteps, bool want_bits, bool wantV, cudaStream_t st, uint64_t *launches,
+           std::string &err) {
+  int rc = ensure_buffers(p, nsteps, wantV, err);
+  if (rc) return rc;
+  const uint32_t words = (p->n + 31) / 32;
+  cudaError_t e = cudaMemsetAsync(p->counts, 0, (size_t)nsteps * 4, st);
+  if (e == cudaSuccess && want_bits) e = cudaMemsetAsync(p->bits, 0, (size_t)nsteps * words * 4, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(p->bar, 0, 4, st);
+  if (e != cudaSuccess) {
+    err = std::string("memset: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  Params P = p->P;
+  P.t0 = p->t;
+  P.nsteps = nsteps;
+  P.bits = want_bits ? p->bits : nullptr;
+  P.words = words;
+  P.counts = p->counts;
+  P.outV = wantV ? p->outV : nullptr;
+  P.bar = p->bar;
+  P.err = p->err;
+  void *args[] = {&P};
+  cudaEventRecord(p->e0, st);
+  if (p->fp64) e = cudaLaunchCooperativeKernel((void *)k_prod<double>, p->blocks, kThreads, args, 0, st);
+  else e = cudaLaunchCooperativeKernel((void *)k_prod<float>, p->blocks, kThreads, args, 0, st);
+  cudaEventRecord(p->e1, st);
+  if (e != cudaSuccess) {
+    err = std::string("cooperative launch: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  p->t += nsteps;
+  if (launches) *launches += 1;
+  p->kl += 1;
+  return FS_OK;
+}
+
+int finish(Prod *p, cudaStream_t st, std::string &err) {
+  cudaError_t e = cudaEventSynchronize(p->e1);
+  if (e != cudaSuccess) {
+    err = std::string("kernel: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  float ms = 0;
+  cudaEventElapsedTime(&ms, p->e0, p->e1);
+  p->ms += ms;
+  int h = 0;
+  e = cudaMemcpy(&h, p->err, 4, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    err = std::string("error word: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  if (h) {
+    err = "grid barrier wait gave up (device error word set)";
+    return FS_ERR_TIMEOUT;
+  }
+  return FS_OK;
+}
+
+}  // namespace
+
+int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t sm_count, cudaStream_t st,
+                std::string &err) {
+  *out = nullptr;
+  const fs_neurons &v = d->neurons;
+  const uint32_t n = v.n;
+  if (n >= (1u << 22)) {
+    err = "production modes support up to 4,194,303 neurons per handle";
+    return FS_ERR_UNSUPPORTED;
+  }
+  if (d->act_ctr & FS_ACT_LTP) {
+    err = "production modes do not implement LTP (use FS_MODE_COMPAT)";
+    return FS_ERR_UNSUPPORTED;
+  }
+  if (d->compat && d->compat->gap_rowptr && d->compat->gap_rowptr[n] != 0) {
+    err = "production modes do not implement gap junctions (use FS_MODE_COMPAT)";
+    return FS_ERR_UNSUPPORTED;
+  }
+  Prod *p = new Prod();
+  p->fp64 = (o.mode == FS_MODE_FP64);
+  p->n = n;
+  p->sm = sm_count;
+  p->key = o.philox_key;
+  p->chunk_steps = o.chunk_steps ? o.chunk_steps : 1000;
+  Params &P = p->P;
+  P.n = n;
+  const size_t nr = (size_t)FS_NREC * n;
+  const fs_syn_list &S = *d->syn;
+  // ---- receptor kinetics seen by each presynaptic neuron ----
+  std::vector<float> pdf((size_t)4 * n, -1.0f), p_dfxt(n, -1.0f), p_dfst(n, -1.0f), p_efas(n, -1.0f);
+  std::vector<uint8_t> proj(n, 0);
+  bool present[5] = {false, false, false, false, false};
+  uint32_t dmin = 0xffffffffu, dmax = 0;
+  uint64_t nlin_e = 0, nnm_e = 0;
+  for (uint64_t e = 0; e < S.n; e++) {
+    const uint32_t a = S.pre[e], b = S.post[e], r = S.rec[e];
+    const uint32_t dl = S.delay ? S.delay[e] : 0;
+    if (a >= n || b >= n || r >= FS_NREC) {
+      err = "synapse list: index out of range";
+      delete p;
+      return FS_ERR_ARG;
+    }
+    if (dl > 255) {
+      err = "synapse delays above 255 steps are not supported";
+      delete p;
+      return FS_ERR_UNSUPPORTED;
+    }
+    dmin = std::min(dmin, dl);
+    dmax = std::max(dmax, dl);
+    present[r] = true;
+    proj[a] |= (uint8_t)(1u << r);
+    auto same = [&](float &slot, float val) -> bool {
+      if (slot < 0.0f) { slot = val; return true; }
+      return slot == val;
+    };
+    bool ok;
+    if (r != FS_NMDA) {
+      ok = same(pdf[(size_t)r * n + a], v.dfst[(size_t)r * n + b]);
+      nlin_e++;
+    } else {
+      ok = same(p_dfxt[a], v.nmda_dfxt[b]) && same(p_dfst[a], v.dfst[(size_t)FS_NMDA * n + b]) &&
+           same(p_efas[a], v.nmda_efst[b] * v.nmda_as[b]);
+      nnm_e++;
+    }
+    if (!ok) {
+      err = "production modes need one receptor time constant per (presynaptic neuron, receptor); "
+            "targets of a neuron differ (use FS_MODE_COMPAT)";
+      delete p;
+      return FS_ERR_UNSUPPORTED;
+    }
+  }
+  if (S.n == 0) dmin = 0;
+  p->d_min = dmin;
+  p->d_max = dmax;
+  p->lin_edges = nlin_e;
+  p->nmda_edges = nnm_e;
+  P.slots = dmax + dmin + 2;
+  P.interval = std::max<uint32_t>(1, dmin);
+  for (int r = 0; r < 4; r++) P.lin_of_rec[r] = present[r] ? (int)(p->nlin++) : -1;
+  P.nlin = p->nlin;
+  for (auto &x : pdf) if (x < 0) x = 0;
+  for (auto *vv : {&p_dfxt, &p_dfst, &p_efas}) for (auto &x : *vv) if (x < 0) x = 0;
+  // ---- CSR of linear out-edges (by pre) and NMDA in-edges (by post) ----
+  std::vector<uint32_t> out_row(n + 1, 0), in_row(n + 1, 0);
+  for (uint64_t e = 0; e < S.n; e++) {
+    if (S.rec[e] == FS_NMDA) in_row[S.post[e] + 1]++;
+    else out_row[S.pre[e] + 1]++;
+  }
+  for (uint32_t i = 0; i < n; i++) { out_row[i + 1] += out_row[i]; in_row[i + 1] += in_row[i]; }
+  std::vector<uint32_t> out_code(nlin_e), in_code(nnm_e);
+  std::vector<float> out_w(nlin_e), in_w(nnm_e);
+  {
+    std::vector<uint32_t> fo(out_row.begin(), out_row.end() - 1), fi(in_row.begin(), in_row.end() - 1);
+    for (uint64_t e = 0; e < S.n; e++) {
+      const uint32_t dl = S.delay ? S.delay[e] : 0;
+      if (S.rec[e] == FS_NMDA) {
+        const uint32_t q = fi[S.post[e]]++;
+        in_code[q] = S.pre[e] | (dl << 24);
+        in_w[q] = S.g[e];
+      } else {
+        const uint32_t q = fo[S.pre[e]]++;
+        out_code[q] = S.post[e] | ((uint32_t)S.rec[e] << 22) | (dl << 24);
+        out_w[q] = S.g[e];
+      }
+    }
+  }
+  // ---- chunks: <= 32 consecutive posts and <= kEdgeBudget NMDA in-edges ----
+  std::vector<uint32_t> chunk_beg;
+  chunk_beg.push_back(0);
+  {
+    uint32_t start = 0;
+    while (start < n) {
+      uint32_t end = start + 1;
+      while (end < n && end - start < 32 && in_row[end + 1] - in_row[start] <= kEdgeBudget) end++;
+      chunk_beg.push_back(end);
+      start = end;
+    }
+  }
+  const uint32_t nchunks = (uint32_t)chunk_beg.size() - 1;
+  p->chunks = nchunks;
+  // ---- grid: all blocks co-resident; chunks split by estimated cost ----
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p->fp64 ? (const void *)k_prod<double> : (const void *)k_prod<float>,
+                                                kThreads, 0);
+  if (occ < 1) occ = 1;
+  uint32_t blocks = sm_count * (uint32_t)std::min(occ, 4);
+  const uint32_t want = (nchunks + (kThreads / 32) - 1) / (kThreads / 32);
+  blocks = std::max<uint32_t>(1, std::min(blocks, std::max<uint32_t>(want, 1)));
+  p->blocks = blocks;
+  std::vector<double> cost(nchunks);
+  double total = 0;
+  for (uint32_t c = 0; c < nchunks; c++) {
+    const uint32_t a = chunk_beg[c], b = chunk_beg[c + 1];
+    cost[c] = 40.0 + 2.0 * (b - a) + (double)(in_row[b] - in_row[a]);
+    total += cost[c];
+  }
+  std::vector<uint32_t> block_chunk(blocks + 1, nchunks);
+  block_chunk[0] = 0;
+  {
+    double acc = 0;
+    uint32_t b = 1;
+    for (uint32_t c = 0; c < nchunks && b < blocks; c++) {
+      acc += cost[c];
+      while (b < blocks && acc >= total * b / blocks) block_chunk[b++] = c + 1;
+    }
+    for (; b < blocks; b++) block_chunk[b] = nchunks;
+  }
+  // ---- device arrays ----
+  int rc = 0;
+  const size_t T = p->fp64 ? 8 : 4;
+#define UPF(field, src, cnt) if ((rc = dup(p, (float **)&P.field, src, cnt, st, err))) goto fail
+#define UPI(field, src, cnt) if ((rc = dup(p, (int32_t **)&P.field, src, cnt, st, err))) goto fail
+#define UPU(field, src, cnt) if ((rc = dup(p, (uint32_t **)&P.field, src, cnt, st, err))) goto fail
+  UPF(Vth, v.Vth, n); UPF(El, v.El, n); UPF(gl, v.gl, n); UPF(Cm, v.Cm, n); UPF(Vreset, v.Vreset, n);
+  UPF(df, v.df, n); UPF(ef, v.ef, n); UPF(dVmax, v.dVmax, n); UPI(RfPed, v.RfPed, n); UPI(SpiDy, v.SpiDy, n);
+  UPF(Vrev, v.Vrev, nr); UPF(dfst, v.dfst, nr); UPF(nmda_dfxt, v.nmda_dfxt, n); UPF(nmda_efst, v.nmda_efst, n);
+  UPF(nmda_as, v.nmda_as, n); UPF(nmda_mg, v.nmda_mg, n); UPF(ext_g, v.ext_g, nr);
+  UPF(pb, v.pb, nr); UPU(act, v.act, n); UPF(inj_mean, v.inj_mean, n); UPF(inj_std, v.inj_std, n);
+  UPF(pdf, pdf.data(), pdf.size()); UPF(p_dfxt, p_dfxt.data(), n); UPF(p_dfst, p_dfst.data(), n);
+  UPF(p_efas, p_efas.data(), n);
+  if ((rc = dup(p, (uint8_t **)&P.proj, proj.data(), n, st, err))) goto fail;
+  UPF(stp_pv, v.stp_pv, n); UPF(stp_dfD, v.stp_dfD, n); UPF(stp_efD, v.stp_efD, n); UPF(stp_aF, v.stp_aF, n);
+  UPF(stp_dfF, v.stp_dfF, n); UPF(stp_efF, v.stp_efF, n); UPF(stp_aCap, v.stp_aCap, n);
+  UPF(stp_dfCap, v.stp_dfCap, n); UPF(stp_aCar, v.stp_aCar, n); UPF(stp_dfCar, v.stp_dfCar, n);
+  UPF(stp_efCar, v.stp_efCar, n);
+  P.plast = (d->act_ctr & FS_ACT_STP) ? PL_STP : (d->act_ctr & FS_ACT_STD) ? PL_STD : PL_NONE;
+  if (d->tm && d->tm->enabled) {
+    if (P.plast != PL_NONE) {
+      err = "Tsodyks-Markram parameters and the reference STD/STP flags are exclusive";
+      rc = FS_ERR_ARG;
+      goto fail;
+    }
+    P.plast = PL_TM;
+    std::vector<float> U(n), dfr(n), dff(n);
+    for (uint32_t i = 0; i < n; i++) {
+      U[i] = d->tm->U ? d->tm->U[i] : 0.2f;
+      const float tr = d->tm->tau_rec ? d->tm->tau_rec[i] : 200.0f, tf = d->tm->tau_fac ? d->tm->tau_fac[i] : 600.0f;
+      dfr[i] = tr > 0 ? std::exp(-d->dt / tr) : 0.0f;
+      dff[i] = tf > 0 ? std::exp(-d->dt / tf) : 0.0f;
+    }
+    if ((rc = dup(p, (uint8_t **)&P.tm_on, d->tm->enabled, n, st, err))) goto fail;
+    UPF(tm_U, U.data(), n); UPF(tm_dfr, dfr.data(), n); UPF(tm_dff, dff.data(), n);
+  }
+  // state
+  if ((rc = dup(p, (uint8_t **)&P.V, (const uint8_t *)nullptr, n * T, st, err)) ||
+      (rc = dup(p, (uint8_t **)&P.G, (const uint8_t *)nullptr, 4 * n * T, st, err)) ||
+      (rc = dup(p, (uint8_t **)&P.ext_st, (const uint8_t *)nullptr, 4 * n * T, st, err)) ||
+      (rc = dup(p, (uint8_t **)&P.ext_x, (const uint8_t *)nullptr, n * T, st, err)) ||
+      (rc = dup(p, (uint8_t **)&P.ext_s, (const uint8_t *)nullptr, n * T, st, err)) ||
+      (rc = dup(p, (uint8_t **)&P.st_pre, (const uint8_t *)nullptr, 4 * n * T, st, err)) ||
+      (rc = dup(p, (uint8_t **)&P.x_pre, (const uint8_t *)nullptr, n * T, st, err)) ||
+      (rc = dup(p, (uint8_t **)&P.s_pre, (const uint8_t *)nullptr, n * T, st, err)) ||
+      (rc = dup(p, (uint8_t **)&P.s_hist, (const uint8_t *)nullptr, (size_t)P.slots * n * T, st, err)) ||
+      (rc = dup(p, &P.Count, (const int32_t *)nullptr, n, st, err)) ||
+      (rc = dup(p, &P.NS, (const uint32_t *)nullptr, n, st, err)) ||
+      (rc = dup(p, &P.D, (const float *)nullptr, n, st, err)) || (rc = dup(p, &P.F, (const float *)nullptr, n, st, err)) ||
+      (rc = dup(p, &P.Cap, (const float *)nullptr, n, st, err)) || (rc = dup(p, &P.Car, (const float *)nullptr, n, st, err)) ||
+      (rc = dup(p, &P.tm_u, (const float *)nullptr, n, st, err)) || (rc = dup(p, &P.tm_x, (const float *)nullptr, n, st, err)) ||
+      (rc = dup(p, &P.ring, (const unsigned long long *)nullptr, (size_t)std::max<uint32_t>(1, p->nlin) * P.slots * n, st, err)))
+    goto fail;
+  // edges
+  UPU(out_row, out_row.data(), (size_t)n + 1); UPU(out_code, out_code.data(), out_code.size());
+  UPF(out_w, out_w.data(), out_w.size());
+  if (nnm_e) {
+    UPU(in_row, in_row.data(), (size_t)n + 1); UPU(in_code, in_code.data(), in_code.size());
+    UPF(in_w, in_w.data(), in_w.size());
+  } else {
+    P.in_row = nullptr;
+  }
+  UPU(chunk_beg, chunk_beg.data(), chunk_beg.size());
+  UPU(block_chunk, block_chunk.data(), block_chunk.size());
+  if ((rc = dal(p, &p->bar, 1, err)) || (rc = dal(p, &p->err, 1, err))) goto fail;
+  if (cudaMemsetAsync(p->err, 0, 4, st) != cudaSuccess) { rc = FS_ERR_CUDA; err = "memset"; goto fail; }
+  if (cudaEventCreate(&p->e0) != cudaSuccess || cudaEventCreate(&p->e1) != cudaSuccess) {
+    rc = FS_ERR_CUDA;
+    err = "event create";
+    goto fail;
+  }
+  if (cudaStreamSynchronize(st) != cudaSuccess) { rc = FS_ERR_CUDA; err = "upload sync"; goto fail; }
+#undef UPF
+#undef UPI
+#undef UPU
+  *out = p;
+  return FS_OK;
+fail:
+  prod_destroy(p);
+  return rc ? rc : FS_ERR_CUDA;
+}
+
+void prod_destroy(Prod *p) {
+  if (!p) return;
+  for (void *q : p->allocs) cudaFree(q);
+  if (p->e0) cudaEventDestroy(p->e0);
+  if (p->e1) cudaEventDestroy(p->e1);
+  delete p;
+}
+
+int prod_upload_params(Prod *p, const float *pb, const uint32_t *act, const float *inj_mean, const float *inj_std,
+                       cudaStream_t st, std::string &err) {
+  const size_t n = p->n;
+  cudaError_t e = cudaMemcpyAsync((void *)p->P.pb, pb, FS_NREC * n * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync((void *)p->P.act, act, n * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync((void *)p->P.inj_mean, inj_mean, n * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync((void *)p->P.inj_std, inj_std, n * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("parameter upload: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  return FS_OK;
+}
+
+__global__ void k_prod_init(const __grid_constant__ Params P, int fp64) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.n) return;
+  if (fp64) ((double *)P.V)[i] = -70.0;
+  else ((float *)P.V)[i] = -70.0f;
+  const uint32_t a = P.act[i];
+  if (a & FS_ACT_STP) { P.D[i] = 1.0f; P.F[i] = 1.0f; P.Cap[i] = 0.0f; P.Car[i] = 20.0f; }
+  else { P.D[i] = 1.0f; P.F[i] = 0.0f; }
+  if (P.tm_U) { P.tm_u[i] = P.tm_U[i]; P.tm_x[i] = 1.0f; }
+}
+
+int prod_reset(Prod *p, uint32_t seed, cudaStream_t st, std::string &err) {
+  const size_t n = p->n, T = p->fp64 ? 8 : 4;
+  Params &P = p->P;
+  cudaError_t e = cudaSuccess;
+  auto z = [&](void *ptr, size_t bytes) {
+    if (e == cudaSuccess && ptr && bytes) e = cudaMemsetAsync(ptr, 0, bytes, st);
+  };
+  z(P.G, 4 * n * T); z(P.ext_st, 4 * n * T); z(P.ext_x, n * T); z(P.ext_s, n * T);
+  z(P.st_pre, 4 * n * T); z(P.x_pre, n * T); z(P.s_pre, n * T); z(P.s_hist, (size_t)P.slots * n * T);
+  z(P.Count, n * 4); z(P.NS, n * 4); z(P.Cap, n * 4); z(P.Car, n * 4);
+  z(P.ring, (size_t)std::max<uint32_t>(1, p->nlin) * P.slots * n * 8);
+  z(p->err, 4);
+  if (e == cudaSuccess) {
+    k_prod_init<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, p->fp64 ? 1 : 0);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("reset: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  // stream key: user key and the run seed
+  P.key0 = (uint32_t)p->key ^ seed;
+  P.key1 = (uint32_t)(p->key >> 32) ^ 0x5eed5eedu;
+  p->t = 0;
+  p->ms = 0.0;
+  p->kl = 0;
+  return FS_OK;
+}
+
+int prod_step(Prod *p, uint32_t nsteps, fs_step_out *out, uint64_t *written, cudaStream_t st, uint64_t *launches,
+              uint64_t *spikes_total, std::string &err) {
+  const uint32_t n = p->n, words = (n + 31) / 32;
+  uint32_t chunk = p->chunk_steps;
+  if ((uint64_t)chunk * n > (64ull << 20)) chunk = (uint32_t)std::max<uint64_t>(1, (64ull << 20) / n);
+  uint32_t done = 0;
+  while (done < nsteps) {
+    const uint32_t b = std::min(chunk, nsteps - done);
+    const bool wantV = out && out->V;
+    int rc = launch(p, b, true, wantV, st, launches, err);
+    if (rc) return rc;
+    cudaError_t e = fsd::spikes_compact(p->bits, b, words, p->counts, p->offsets, p->idx, st, launches);
+    if (e != cudaSuccess) { err = cudaGetErrorString(e); return FS_ERR_CUDA; }
+    if ((rc = finish(p, st, err))) return rc;
+    uint32_t total = 0;
+    e = cudaMemcpyAsync(&total, p->offsets + b, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && out && out->spike_count)
+      e = cudaMemcpyAsync(out->spike_count + done, p->counts, (size_t)b * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { err = cudaGetErrorString(e); return FS_ERR_CUDA; }
+    if (out && out->spike_idx) {
+      if (*written + total > out->spike_cap) {
+        err = "spike_idx buffer too small";
+        return FS_ERR_CAPACITY;
+      }
+      e = cudaMemcpy(out->spike_idx + *written, p->idx, (size_t)total * 4, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) { err = cudaGetErrorString(e); return FS_ERR_CUDA; }
+    }
+    if (wantV) {
+      e = cudaMemcpy(out->V + (size_t)done * n, p->outV, (size_t)b * n * 4, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) { err = cudaGetErrorString(e); return FS_ERR_CUDA; }
+    }
+    if (out && (out->Irep || out->nstate || out->gv_n)) {
+      err = "production modes return spikes and V only";
+      return FS_ERR_UNSUPPORTED;
+    }
+    *written += total;
+    if (spikes_total) *spikes_total += total;
+    done += b;
+  }
+  return FS_OK;
+}
+
+int prod_run(Prod *p, uint32_t nsteps, cudaStream_t st, uint64_t *launches, std::string &err) {
+  uint32_t done = 0;
+  while (done < nsteps) {
+    const uint32_t b = std::min(p->chunk_steps, nsteps - done);
+    int rc = launch(p, b, false, false, st, launches, err);
+    if (rc) return rc;
+    done += b;
+  }
+  return FS_OK;
+}
+
+int prod_check(Prod *p, cudaStream_t st, uint64_t *spikes_total, std::string &err) {
+  int rc = finish(p, st, err);
+  if (rc) return rc;
+  (void)spikes_total;
+  return FS_OK;
+}
+
+void prod_kernel_time(Prod *p, double *ms_per_launch, uint64_t *launches) {
+  if (ms_per_launch) *ms_per_launch = p->kl ? p->ms / (double)p->kl : 0.0;
+  if (launches) *launches = p->kl;
+}
+
+int prod_get_state(Prod *p, float *V, int32_t *Count, uint32_t *NState, cudaStream_t st, std::string &err) {
+  const size_t n = p->n;
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess && V) {
+    if (p->fp64) {
+      std::vector<double> tmp(n);
+      e = cudaMemcpy(tmp.data(), p->P.V, n * 8, cudaMemcpyDeviceToHost);
+      for (size_t i = 0; i < n; i++) V[i] = (float)tmp[i];
+    } else {
+      e = cudaMemcpy(V, p->P.V, n * 4, cudaMemcpyDeviceToHost);
+    }
+  }
+  if (e == cudaSuccess && Count) e = cudaMemcpy(Count, p->P.Count, n * 4, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && NState) e = cudaMemcpy(NState, p->P.NS, n * 4, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    err = cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  return FS_OK;
+}
+
+void prod_info(const Prod *p, ProdInfo *info) {
+  info->n = p->n;
+  info->d_min = p->d_min;
+  info->d_max = p->d_max;
+  info->slots = p->P.slots;
+  info->interval = p->P.interval;
+  info->blocks = p->blocks;
+  info->threads = kThreads;
+  info->chunks = p->chunks;
+  info->lin_edges = p->lin_edges;
+  info->nmda_edges = p->nmda_edges;
+  info->lin_receptors = p->nlin;
+  info->fp64 = p->fp64 ? 1 : 0;
+}
+
+}  // namespace fsp

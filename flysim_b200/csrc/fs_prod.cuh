@@ -1,0 +1,34 @@
+// Production engine (FS_MODE_FP32 / FS_MODE_FP64): interface used by the C ABI.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+#include "flysim_b200.h"
+
+namespace fsp {
+
+struct Prod;
+
+int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t sm_count,
+                cudaStream_t st, std::string &err);
+void prod_destroy(Prod *p);
+int prod_upload_params(Prod *p, const float *pb, const uint32_t *act, const float *inj_mean,
+                       const float *inj_std, cudaStream_t st, std::string &err);
+int prod_reset(Prod *p, uint32_t seed, cudaStream_t st, std::string &err);
+int prod_step(Prod *p, uint32_t nsteps, fs_step_out *out, uint64_t *written, cudaStream_t st,
+              uint64_t *launches, uint64_t *spikes_total, std::string &err);
+int prod_run(Prod *p, uint32_t nsteps, cudaStream_t st, uint64_t *launches, std::string &err);
+int prod_check(Prod *p, cudaStream_t st, uint64_t *spikes_total, std::string &err);
+void prod_kernel_time(Prod *p, double *ms_per_launch, uint64_t *launches);
+int prod_get_state(Prod *p, float *V, int32_t *Count, uint32_t *NState, cudaStream_t st, std::string &err);
+
+// Layout facts for measurement (algorithmic bytes).
+struct ProdInfo {
+  uint32_t n, d_min, d_max, slots, interval, blocks, threads, chunks;
+  uint64_t lin_edges, nmda_edges;
+  uint32_t lin_receptors;
+  int fp64;
+};
+void prod_info(const Prod *p, ProdInfo *info);
+
+}  // namespace fsp

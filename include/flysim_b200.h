@@ -227,6 +227,9 @@ int fs_stats(fs_handle *h, uint64_t *steps_done, uint64_t *spikes_total, uint64_
 /* Average device duration (ms) of the dominant kernel of the last fs_run /
  * fs_step call, measured with CUDA events on the engine stream. */
 int fs_kernel_time(fs_handle *h, double *ms_per_launch, uint64_t *launches);
+/* Evaluates the device's glibc-exact float exp (the NMDA Mg-block exp of
+ * FS_MODE_COMPAT) on k host values, for checks against the host libm. */
+int fs_debug_expf(const float *x, float *y, uint64_t k);
 /* Copy state out (V, Count, NState) for checks; arrays of length n. */
 int fs_get_state(fs_handle *h, float *V, int32_t *Count, uint32_t *NState);
 /* Full conductance view for checks: RVs (FS_NREC*n) after the last step and

@@ -1,0 +1,148 @@
+"""Generates the golden fixtures: small .conf/.pro cases and the output files
+the flysim reference writes for them.
+
+The reference is built from its own sources by oracle/Makefile.ref into
+oracle/_ref/flysim_ref (this needs the reference tree, so it runs only where
+the sources are; the fixtures are committed).  Each case directory holds
+net.conf, net.pro, cmd (the reference's extra command-line flags) and the
+reference's output files.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import json
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from flysim_b200 import netgen  # noqa: E402
+
+REF = os.path.join(ROOT, "oracle", "_ref", "flysim_ref")
+
+OUTS = [{"name": "Spikes.dat", "type": "Spike", "pop": "AllPopulation"},
+        {"name": "FR.dat", "type": "FiringRate", "pop": "AllPopulation", "win": 50, "step": 10},
+        {"name": "FRs.dat", "type": "FiringRate", "pop": "AllPopulation", "win": 20, "step": 5, "sum": True}]
+
+
+def _misc_conf(path):
+    s = ""
+    for name, n in (("A", 30), ("B", 20), ("C", 1), ("D", 1)):
+        s += ("NeuralPopulation: %s\nN=%d\nC=0.5\nTaum=15\nRestPot=-65\nThreshold=-50\nResetPot=-60\n"
+              "RefractoryPeriod=2.5\nSpikeDly=0.3\n\n"
+              "Receptor:AMPA\nTau=3\nRevPot=0\nFreqExt=3000\nMeanExtEff=2.5\nEndReceptor\n\n"
+              "Receptor:Ach\nTau=4\nRevPot=0\nFreqExt=200\nMeanExtEff=1\nEndReceptor\n\n"
+              "Receptor:GluCl\nTau=6\nRevPot=-80\nFreqExt=100\nMeanExtEff=1\nEndReceptor\n\n"
+              "Receptor:GABA\nTau=5\nRevPot=-70\nEndReceptor\n\n"
+              "Receptor:NMDA\nTau=80\nTauXT=2\nRevPot=0\nFreqExt=50\nMeanExtEff=0.5\nEndReceptor\n\n") % (name, n)
+        links = {
+            "A": [("B", "Ach", 0.4, 0.3, None), ("A", "GAP", 0.01, 0.2, None), ("C", "GAP", 0.02, None, None),
+                  ("B", "NMDA", 0.1, 0.5, None)],
+            "B": [("A", "GluCl", 0.5, 0.03, None), ("A", "GABA", 1.5, 0.05, None), ("D", "Ach", 3, None, None),
+                  ("A", "Ach", 3, 0.5, 0.5)],
+            "C": [("D", "GAP", 0.05, None, None), ("A", "AMPA", 5, 0.5, None)],
+            "D": [],
+        }[name]
+        for tgt, rec, eff, conn, wgt in links:
+            s += "TargetPopulation: %s\nTargetReceptor=%s\nMeanEff=%s\n" % (tgt, rec, eff)
+            if conn is not None:
+                s += "Connectivity=%s\n" % conn
+            if wgt is not None:
+                s += "weight=%s\n" % wgt
+            s += "EndTargetPopulation\n\n"
+        s += "EndNeuralPopulation\n\n"
+    with open(path, "w") as f:
+        f.write(s)
+
+
+def _small_conf(path):
+    """Two 20-neuron populations with short-term plasticity parameters,
+    spike delay and a self-connected group."""
+    s = ""
+    for name, selfc in (("Exc1", False), ("Exc2", True)):
+        s += ("NeuralPopulation: %s\nN=20\nC=0.5\nTaum=20\nThreshold=-50\nRestPot=-70\nResetPot=-55\n"
+              "RefractoryPeriod=1.9\nSpikeDly=0.3\n" % name)
+        if name == "Exc1":
+            s += "STP_pv=0.6\nSTP_tD=300\nSTP_aF=1.0\nSTP_tF=7000\nSTP_aCap=2.0\nSTP_tCap=100\nSTP_aCar=3.0\nSTP_tCar=70\n"
+        if selfc:
+            s += "SelfConnection=true\n"
+        s += "\nReceptor:AMPA\nTau=5\nRevPot=-70\nFreqExt=8.4375\nMeanExtEff=2.1\nEndReceptor\n\n"
+        s += "TargetPopulation: Exc2\nTargetReceptor=AMPA\nMeanEff=4.2\n"
+        if name == "Exc1":
+            s += "Connectivity=0.5\n"
+        s += "EndTargetPopulation\n\nEndNeuralPopulation\n\n"
+    with open(path, "w") as f:
+        f.write(s)
+
+
+def cases():
+    c = {}
+    c["two_pop"] = dict(conf=lambda p: netgen.write_two_pop(p),
+                        pro=dict(t_end_ms=200, seeds=(7,), outputs=OUTS), flags=[])
+    c["two_pop_std"] = dict(conf=lambda p: netgen.write_two_pop(p, n_e=200, n_i=50),
+                            pro=dict(t_end_ms=150, seeds=(3,), outputs=OUTS), flags=["-STD"])
+    c["two_pop_stp"] = dict(conf=lambda p: netgen.write_two_pop(p, n_e=200, n_i=50),
+                            pro=dict(t_end_ms=150, seeds=(3,), outputs=OUTS), flags=["-STP"])
+
+    def conn_ltp(p):
+        netgen.write_connectome(netgen.connectome(n=150, regions=5, mean_degree=20, delays=False, seed=5), p,
+                                with_delays=False)
+    c["conn_ltp"] = dict(conf=conn_ltp, pro=dict(t_end_ms=200, seeds=(4,), outputs=OUTS), flags=["-LTP"])
+
+    def conn(p):
+        netgen.write_connectome(netgen.connectome(n=400, regions=8, mean_degree=40, delays=False, seed=2), p,
+                                with_delays=False)
+    c["conn"] = dict(conf=conn, pro=dict(t_end_ms=200, seeds=(11,), outputs=OUTS + [
+        {"name": "Isyn.dat", "type": "IsynSeparatedSum", "pop": ["n3", "n7"]},
+        {"name": "ov.dat", "type": "DeltaMemPotLimit", "pop": "AllPopulation", "align": True},
+        {"name": "gv.dat", "type": "GatingVariable", "pop": "n1"}]), flags=[])
+    c["repeats"] = dict(conf=lambda p: netgen.write_two_pop(p, n_e=160, n_i=40), pro=dict(
+        t_end_ms=100, seeds=(5, 9), outputs=OUTS,
+        events=[{"t": 30, "type": "ChangeExtFreq", "pop": "E", "f": 0},
+                {"t": 50, "type": "ChangeMembraneNoise", "pop": "AllPopulation", "mean": 0.2, "std": 0.5},
+                {"t": 70, "type": "ChangeExtFreq", "pop": "I", "rec": "NMDA", "f": 300}]), flags=["-rp", "3"])
+    c["misc"] = dict(conf=_misc_conf, pro=dict(t_end_ms=200, seeds=(21,), outputs=OUTS + [
+        {"name": "Isyn.dat", "type": "IsynSeparatedSum", "pop": ["C", "D"]},
+        {"name": "ov.dat", "type": "DeltaMemPotLimit", "pop": "AllPopulation"},
+        {"name": "sa.dat", "type": "Spike", "pop": ["B", "A"], "align": True},
+        {"name": "Mem.dat", "type": "MemPot", "pop": ["D", "C"]}],
+        events=[{"t": 100, "type": "ChangeExtFreq", "pop": "A", "rec": "Ach", "f": 0},
+                {"t": 150, "type": "ChangeMembraneNoise", "pop": "B", "mean": 0.3, "std": 2.0}]), flags=[])
+    c["small"] = dict(conf=_small_conf, pro=dict(
+        t_end_ms=1000, seeds=(12345,), groups={"Sti2": ["Exc2", "Exc1"]},
+        outputs=[{"name": "Spikes.dat", "type": "Spike", "pop": "Sti2"},
+                 {"name": "FRates.dat", "type": "FiringRate", "pop": "Exc2", "win": 50, "step": 10}],
+        events=[{"t": 300, "type": "ChangeExtFreq", "pop": "Exc1", "f": 24000},
+                {"t": 650, "type": "ChangeMembraneNoise", "pop": "Exc1", "mean": 0.43, "std": 0.03}]), flags=[])
+    return c
+
+
+def main():
+    if not os.path.exists(REF):
+        sys.exit("reference binary missing: build it with  make -f oracle/Makefile.ref")
+    for name, cs in cases().items():
+        d = os.path.join(HERE, name)
+        shutil.rmtree(d, ignore_errors=True)
+        os.makedirs(d)
+        cs["conf"](os.path.join(d, "net.conf"))
+        netgen.write_pro(os.path.join(d, "net.pro"), **cs["pro"])
+        with open(os.path.join(d, "cmd.json"), "w") as f:
+            json.dump(cs["flags"], f)
+        r = subprocess.run([REF, "-conf", "net.conf", "-pro", "net.pro"] + cs["flags"], cwd=d,
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.exit("reference failed on %s: %s" % (name, r.stderr[-400:]))
+        for junk in ("network.log", "ConfsInfo.log"):
+            p = os.path.join(d, junk)
+            if os.path.exists(p):
+                os.remove(p)
+        outs = sorted(f for f in os.listdir(d) if f not in ("net.conf", "net.pro", "cmd.json"))
+        print(name, outs)
+
+
+if __name__ == "__main__":
+    main()
