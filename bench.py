@@ -1,0 +1,375 @@
+"""Benchmark: per-timestep network integration of a 20,000-neuron
+connectome-shaped network on one B200 (flysim's headline workload).
+
+Workload (synthetic, seeded; the reference's connectome files are not
+available): 20,000 LIF neurons in 58 regions, lognormal out-degree (mean 120,
+sigma 1.0), 80% of targets inside the source's region, 70% excitatory
+(AMPA + NMDA) / 30% inhibitory (GABA), lognormal weights (median 1 nS,
+sigma 0.8, scaled per receptor), integer delays uniform 1-5 ms, external
+Poisson drive per region 1-4 kHz, dt = 0.1 ms, FP32 production mode.
+
+One bench "step" = 1 s of simulated time (10,000 timesteps).  The metric is
+simulated seconds per wall second; synaptic events/s is reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own CPU implementation (the flysim
+binary built from its sources into oracle/_ref by oracle/Makefile.ref) on the
+same network with delays set to 0 (the reference has no synaptic delays), on
+all host cores, through its own -rp repeat loop and its own Run-phase timer.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_NEURONS = 20000
+REGIONS = 58
+DT = 0.1
+STEPS_PER_BENCH_STEP = 10000  # 1 s simulated
+SEED = 1
+METRIC = "simulated seconds per wall second (20k-neuron connectome network)"
+UNIT = "sim-s/wall-s"
+
+
+def _env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def build_network(rank: int):
+    from flysim_b200 import netgen, network
+    c = netgen.connectome(n=N_NEURONS, regions=REGIONS, seed=SEED + rank)
+    return c, network.connectome_net(c, dt=DT, with_delays=True)
+
+
+def algorithmic_bytes(na, spikes: int, steps: int, avg_lin_out: float) -> float:
+    """Bytes a launch must move at minimum: per neuron-step 60 B of state
+    (V, LIF state, 2 conductance slots, NMDA post sum, ext gate: 24 B read,
+    20 B written; presynaptic NMDA x/s: 16 B); N/8 B of spike flags; 12 B per
+    NMDA in-edge per step (index, weight, s_pre gather); per spike 4 B of list
+    and 16 B per outgoing linear synapse (index, weight, 8 B fixed-point ring
+    update)."""
+    n = na.n
+    nmda_edges = int(np.count_nonzero(na.syn["rec"] == 4))
+    per_step = n * 60 + n / 8.0 + nmda_edges * 12
+    return steps * per_step + spikes * (4 + avg_lin_out * 16)
+
+
+def cpu_baseline_port(c, samples: int = 200):
+    """The oracle (CPU restatement of the reference step, one thread) on the
+    same network with delays 0, through the .conf route; bounded sample."""
+    import ctypes as C
+    import flysim_b200 as fb
+    from flysim_b200 import netgen
+    from flysim_b200 import build as fbuild
+    olib = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
+    if not os.path.exists(olib):
+        fbuild.build_oracle()
+    L = C.CDLL(olib)
+    L.oracle_engine.restype = C.POINTER(fb.EngineVtbl)
+    L.oracle_create.restype = C.c_void_p
+    L.oracle_create.argtypes = [C.POINTER(fb.NetDesc)]
+    L.oracle_destroy.argtypes = [C.c_void_p]
+    tmp = tempfile.mkdtemp()
+    try:
+        conf, pro = os.path.join(tmp, "net.conf"), os.path.join(tmp, "net.pro")
+        netgen.write_connectome(c, conf, with_delays=False)
+        netgen.write_pro(pro, samples * DT, seeds=(SEED,), outputs=())
+        m = fb.Model(conf, pro)
+        ctx = L.oracle_create(m.desc())
+        vt = L.oracle_engine().contents
+        reset = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint32, C.c_uint32)(vt.reset)
+        step = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint32, C.POINTER(fb.StepOut))(vt.step)
+        reset(ctx, SEED, SEED)
+        step(ctx, 20, None)  # warm caches
+        t0 = time.perf_counter()
+        step(ctx, samples, None)
+        dt_wall = time.perf_counter() - t0
+        L.oracle_destroy(ctx)
+        m.close()
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    sim_s = samples * DT * 1e-3
+    return {"value": sim_s / dt_wall, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "%d timesteps (%.0f ms simulated) of the same 20k-neuron network with delays 0, "
+                      "oracle/fs_oracle.cpp single thread, %.2f s wall" % (samples, samples * DT, dt_wall)}
+
+
+def run_reference(args, rank):
+    """--impl reference: the reference binary on the same network (delays 0)."""
+    ref = os.path.join(ROOT, "oracle", "_ref", "flysim_ref")
+    if rank != 0:
+        return 0
+    if not os.path.exists(ref):
+        print(json.dumps({"impl": "reference", "unavailable": "reference binary oracle/_ref/flysim_ref not built"}))
+        return 0
+    from flysim_b200 import netgen
+    c, _ = build_network(0)
+    sample_ms = float(os.environ.get("FS_REF_SAMPLE_MS", "20"))
+    reps = args.warmup + args.steps
+    tmp = tempfile.mkdtemp()
+    try:
+        netgen.write_connectome(c, os.path.join(tmp, "net.conf"), with_delays=False)
+        seeds = [SEED + i for i in range(reps)]
+        netgen.write_pro(os.path.join(tmp, "net.pro"), sample_ms, seeds=seeds,
+                         outputs=({"name": "Spikes.dat", "type": "Spike", "pop": "AllPopulation"},))
+        threads = os.cpu_count() or 1
+        t0 = time.time()
+        r = subprocess.run([ref, "-conf", "net.conf", "-pro", "net.pro", "-rp", str(reps), "-t", str(threads)],
+                           cwd=tmp, capture_output=True, text=True, timeout=3600)
+        setup_and_run = time.time() - t0
+        times = [float(x) for x in re.findall(r"real time=([0-9.eE+-]+)s 100%", r.stdout)]
+        if r.returncode != 0 or len(times) < reps:
+            print(json.dumps({"impl": "reference", "unavailable": "reference run failed (rc %d): %s" %
+                              (r.returncode, (r.stderr or r.stdout)[-200:].replace("\n", " "))}))
+            return 0
+        spikes = 0
+        for k in range(args.warmup + 1, reps + 1):
+            f = os.path.join(tmp, "Spikes.dat" + ("" if k == 1 else "_%d" % k))
+            spikes += sum(1 for _ in open(f)) if os.path.exists(f) else 0
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    timed = times[args.warmup:]
+    wall = sum(timed)
+    sim = len(timed) * sample_ms * 1e-3
+    value = sim / wall
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / len(timed),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "connectome-shaped network, 20000 neurons / 58 regions / %d connections, "
+                               "delays 0 (the reference has none), dt 0.1 ms; one step = %g ms simulated"
+                               % (c.n_connections, sample_ms),
+                   "threads": threads, "setup_and_run_s": round(setup_and_run, 1)},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": "%d repeats of %g ms simulated, flysim reference -t %d, Run-phase timer"
+                                   % (len(timed), sample_ms, threads)},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "spikes_per_step": spikes / max(1, len(timed)),
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="run this many timesteps once and exit (for ncu captures)")
+    args = ap.parse_args()
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local = _env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import torch
+    import torch.distributed as dist
+    import flysim_b200 as fb
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    c, na = build_network(rank)
+    eng = fb.Engine(na.desc, args.mode, device=local, chunk_steps=STEPS_PER_BENCH_STEP)
+    eng.reset(SEED + rank)
+    if args.profile_steps:
+        eng.run(args.profile_steps)
+        eng.sync()
+        print(json.dumps({"profile_steps": args.profile_steps, "stats": eng.stats()}))
+        return 0
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        eng.run_timed(STEPS_PER_BENCH_STEP)
+    s0 = eng.stats()
+    clocks = ClockSampler(local)
+    clocks.start()
+    dev_ms = []
+    kern_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        barrier()
+        dev_ms.append(eng.run_timed(STEPS_PER_BENCH_STEP))
+        kern_ms.append(eng.kernel_time()[0])
+        barrier()
+    clk = clocks.stop()
+    s1 = eng.stats()
+    total_ms = float(np.sum(dev_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    sim_s = args.steps * STEPS_PER_BENCH_STEP * DT * 1e-3
+    value = world * sim_s / (total_ms * 1e-3)
+    spikes = s1["spikes"] - s0["spikes"]
+    launches = s1["launches"] - s0["launches"]
+    # synaptic events: spikes x outgoing connections of the spiking neurons
+    # (a connection carrying AMPA+NMDA counts once); mean out-degree used
+    mean_out = c.n_connections / c.n
+    syn_events_per_s = world * spikes * mean_out / (total_ms * 1e-3)
+    lin = na.syn["rec"] != 4
+    avg_lin_out = float(np.count_nonzero(lin)) / na.n
+    k_ms = float(np.mean(kern_ms))
+    spikes_per_launch = spikes / max(1, args.steps)
+    alg = algorithmic_bytes(na, spikes_per_launch, STEPS_PER_BENCH_STEP, avg_lin_out)
+    peak, peak_kind = load_peaks()
+    achieved = alg / (k_ms * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "prod_fp32_connectome20k_traffic.json")
+    if os.path.exists(tp):
+        tj = json.load(open(tp))
+        traffic = tj.get("dram_bytes_per_timestep", 0) * STEPS_PER_BENCH_STEP
+
+    # e2e: through fs_step with host buffers: drive table up, spike lists down
+    e2e = None
+    if rank == 0 or world > 1:
+        pb_host = np.ascontiguousarray(na.fields["pb"].reshape(5, na.n)[0])
+        cuts = np.flatnonzero(np.diff(c.region)) + 1
+        starts = np.concatenate([[0], cuts])
+        region_bounds = list(zip(starts, np.concatenate([cuts, [na.n]])))
+        e2e_wall = []
+        h2d = 32 * na.n  # pb (5 receptors), act, injection mean/std, as uploaded on a parameter change
+        d2h = 0
+        for k in range(2):
+            flush.zero_()
+            barrier()
+            t0 = time.perf_counter()
+            # the per-region drive table is an input of the step: set it
+            # region by region (uploaded host -> device inside fs_step)
+            for lo, hi in region_bounds:
+                eng.set_drive(int(lo), int(hi - lo), 0, float(pb_host[lo]))
+            spk, _ = eng.step(STEPS_PER_BENCH_STEP, spike_cap=STEPS_PER_BENCH_STEP * 64)
+            t1 = time.perf_counter()
+            e2e_wall.append(t1 - t0)
+            d2h = 4 * STEPS_PER_BENCH_STEP + 4 * sum(int(x.size) for x in spk) + 4
+        e2e_s = float(np.median(e2e_wall))
+        if world > 1:
+            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": world * STEPS_PER_BENCH_STEP * DT * 1e-3 / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_port(c)
+        except Exception as ex:  # reported, not fatal
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "port", "sample": "failed: %s" % ex}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.mode == "fp32" else "f64",
+            "data": "synthetic",
+            "config": {"workload": "connectome-shaped network: %d LIF neurons, %d regions, %d connections "
+                                   "(%d synapse entries), delays 1-5 ms, drive 1-4 kHz, dt 0.1 ms, %s mode; "
+                                   "one step = 1 s simulated (10,000 timesteps)"
+                                   % (na.n, REGIONS, c.n_connections, na.n_syn, args.mode),
+                       "parallelism": "replicas" if world > 1 else "single GPU",
+                       "l2": "flushed (256 MB write) before every timed step; the ~%d MB working set is "
+                             "L2-resident within a step" % int((na.n_syn * 8 + na.n * 200) / 1e6)},
+            "syn_events_per_s": syn_events_per_s,
+            "spikes_per_step": spikes / args.steps,
+            "mean_rate_hz": spikes / args.steps / na.n,
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "note": "%s peak; algorithmic bytes per launch %.3g over %.2f ms (mean launch)"
+                                 % (peak_kind, alg, k_ms)},
+            "clocks": clk,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

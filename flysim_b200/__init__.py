@@ -123,6 +123,7 @@ def lib() -> C.CDLL:
         "fs_step": (C.c_int, [vp, C.c_uint32, C.POINTER(StepOut)]),
         "fs_run": (C.c_int, [vp, C.c_uint32]),
         "fs_sync": (C.c_int, [vp]),
+        "fs_run_timed": (C.c_int, [vp, C.c_uint32, C.POINTER(C.c_double)]),
         "fs_stats": (C.c_int, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "fs_kernel_time": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
         "fs_debug_expf": (C.c_int, [_f, _f, C.c_uint64]),
@@ -150,6 +151,7 @@ def lib() -> C.CDLL:
 def exported_symbols() -> Sequence[str]:
     return [n for n in ("fs_abi_version", "fs_last_error", "fs_device_count", "fs_create", "fs_destroy",
                         "fs_reset", "fs_set_drive", "fs_set_act", "fs_set_injection", "fs_step", "fs_run",
+                        "fs_run_timed",
                         "fs_sync", "fs_stats", "fs_kernel_time", "fs_debug_expf", "fs_get_state",
                         "fs_get_syn_state", "fs_model_load", "fs_model_free", "fs_model_error",
                         "fs_model_desc", "fs_model_info", "fs_model_seed", "fs_model_run",
@@ -305,6 +307,12 @@ class Engine:
 
     def run(self, nsteps: int):
         _check(lib().fs_run(self._h, nsteps), self._h)
+
+    def run_timed(self, nsteps: int) -> float:
+        """Runs nsteps on the device; returns the device time in ms (CUDA events)."""
+        ms = C.c_double()
+        _check(lib().fs_run_timed(self._h, nsteps, C.byref(ms)), self._h)
+        return ms.value
 
     def sync(self):
         _check(lib().fs_sync(self._h), self._h)

@@ -584,6 +584,22 @@ int fs_run(fs_handle *h, uint32_t nsteps) {
   return FS_OK;
 }
 
+int fs_run_timed(fs_handle *h, uint32_t nsteps, double *device_ms) {
+  if (!h) return set_err(nullptr, FS_ERR_ARG, "null handle");
+  CK(cudaSetDevice(h->device));
+  int rc = upload_params(h);
+  if (rc) return rc;
+  CK(cudaEventRecord(h->ev0, h->st));
+  rc = fs_run(h, nsteps);
+  if (rc) return rc;
+  CK(cudaEventRecord(h->ev1, h->st));
+  CK(cudaEventSynchronize(h->ev1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  if (device_ms) *device_ms = ms;
+  return fs_sync(h);
+}
+
 int fs_sync(fs_handle *h) {
   if (!h) return set_err(nullptr, FS_ERR_ARG, "null handle");
   CK(cudaStreamSynchronize(h->st));

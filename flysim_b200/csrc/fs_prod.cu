@@ -11,23 +11,29 @@
 //    neuron, that sum obeys G(t) = df*G(t-1) + sum_spikes g*c, with
 //    c = inc + st_pre(t-1)*(1-df) computed once per spike from a per-neuron
 //    gate st_pre.  So a spike pushes g*c into a delay ring
-//    ring[receptor][(t+delay) mod slots][post] (64-bit fixed point, 2^-40 nS:
+//    ring[receptor][post][(t+delay) mod S] (64-bit fixed point, 2^-40 nS:
 //    integer atomics make the sum independent of arrival order), and each post
 //    folds its slot into G once per step.
 //  * NMDA.  The gate s is nonlinear in its own state (code/EqsGnl2.cpp:493) but
 //    depends only on the presynaptic spike train, so x_pre/s_pre are kept per
-//    presynaptic neuron, s_pre(t) is stored in a history ring, and each post
-//    pulls sum(g * s_pre(t-delay)) over its NMDA in-edges every step.
+//    presynaptic neuron, s_pre(t) is stored in a history ring
+//    s_hist[pre][t mod S], and each post pulls sum(g * s_pre(t-1-delay)) over
+//    its NMDA in-edges.
 //  * Drive: counter-based Philox-4x32-10 (Salmon et al., SC'11) keyed by
 //    (step, neuron), so no generator state is shared.
 //
-// One persistent cooperative kernel runs many steps.  A warp owns a chunk of
-// up to 32 consecutive post neurons (NMDA pull + neuron update + pushes of its
-// spikes).  Every value a neuron reads from another neuron was produced at
-// least min_delay steps earlier, so blocks only synchronise (bounded-wait grid
-// barrier) once every max(min_delay, 1) steps; the ring depth
-// slots = max_delay + min_delay + 2 keeps reuse of a slot out of the interval
-// that still reads it.
+// Scheduling.  Every value a neuron reads from another neuron was produced
+// at least min_delay steps earlier.  The steps are therefore cut into
+// intervals of max(min_delay, 1) steps separated by a bounded-wait grid
+// barrier; inside an interval the neurons are independent.  A block owns a
+// contiguous range of post neurons and, per interval, (1) pulls the NMDA
+// conductances of all the interval's steps at once (one warp per post, the
+// in-edges split over the lanes, a butterfly reduction per step: the loads of
+// many steps overlap), then (2) advances its neurons one thread each through
+// the interval's steps with their state in registers, pushing the spikes of
+// each step into the delay ring (one warp per spike).  The ring depth
+// S = next power of two >= max_delay + min_delay + 2 keeps the reuse of a
+// slot out of any interval that still reads it.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -40,15 +46,16 @@
 
 namespace fsp {
 
-constexpr double kFix = 1099511627776.0;        // 2^40
+constexpr double kFix = 1099511627776.0;           // 2^40
 constexpr double kInvFix = 9.094947017729282e-13;  // 2^-40
-constexpr uint32_t kEdgeBudget = 256;            // NMDA in-edges per chunk round
 constexpr uint32_t kThreads = 256;
+constexpr uint32_t kTile = 256;  // post neurons advanced together (one per thread)
+constexpr uint32_t kLB = 16;     // steps per NMDA pull batch
 
 enum { PL_NONE = 0, PL_STD = 1, PL_STP = 2, PL_TM = 3 };
 
 struct Params {
-  uint32_t n, slots, interval, nlin;
+  uint32_t n, slots, mask, interval, nlin;
   int lin_of_rec[4];
   const float *Vth, *El, *gl, *Cm, *Vreset, *df, *ef, *dVmax;
   const int32_t *RfPed, *SpiDy;
@@ -67,13 +74,12 @@ struct Params {
   int32_t *Count;
   uint32_t *NS;
   float *D, *F, *Cap, *Car, *tm_u, *tm_x;
-  unsigned long long *ring;
+  unsigned long long *ring;              // [nlin][n][S]
   const uint32_t *out_row, *out_code;
   const float *out_w;
   const uint32_t *in_row, *in_code;
   const float *in_w;
-  const uint32_t *chunk_beg;
-  const uint32_t *block_chunk;
+  const uint32_t *block_post;            // [blocks+1] post range of each block
   uint32_t key0, key1;
   uint64_t t0;
   uint32_t nsteps;
@@ -83,6 +89,7 @@ struct Params {
   float *outV;
   unsigned int *bar;
   int *err;
+  unsigned long long *spike_total;  // spikes since reset
 };
 
 // ---- Philox-4x32-10 -------------------------------------------------------
@@ -100,20 +107,30 @@ __device__ __forceinline__ void philox(uint32_t c[4], uint32_t k0, uint32_t k1) 
 __device__ __forceinline__ float u24(uint32_t x) { return (float)(x >> 8) * 5.9604644775390625e-08f; }
 
 // ---- bounded grid barrier ---------------------------------------------------
-__device__ __forceinline__ bool grid_sync(unsigned int *bar, unsigned int target, int *err) {
+// bar[0] counts arrivals, bar[32] (its own 128-byte line) is the generation
+// the waiting blocks poll; the last block to arrive resets the count and
+// advances the generation.  Every wait is bounded: after ~2^24 polls the
+// block sets the error word and all blocks leave.
+__device__ __forceinline__ bool grid_sync(unsigned int *bar, int *err) {
   __syncthreads();
   if (threadIdx.x == 0) {
+    volatile unsigned int *gen = bar + 32;
+    const unsigned int g = *gen;
     __threadfence();
-    atomicAdd(bar, 1u);
-    unsigned int spins = 0;
-    for (;;) {
-      if (*(volatile unsigned int *)bar >= target) break;
-      if (*(volatile int *)err) break;
-      if (++spins > (1u << 22)) {
-        atomicExch(err, 2);
-        break;
+    const unsigned int arrived = atomicAdd(bar, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd((unsigned int *)gen, 1u);
+    } else {
+      unsigned int spins = 0;
+      while (*gen == g) {
+        if (*(volatile int *)err) break;
+        if (++spins > (1u << 24)) {
+          atomicExch(err, 2);
+          break;
+        }
       }
-      __nanosleep(64);
     }
     __threadfence();
   }
@@ -135,145 +152,312 @@ __device__ __forceinline__ float exp_t<float>(float x) { return expf(x); }
 template <>
 __device__ __forceinline__ double exp_t<double>(double x) { return exp(x); }
 
-// ---- one chunk: NMDA pull, neuron update, presynaptic update, push --------
 template <class T>
-__device__ __forceinline__ void run_chunk(const Params &P, uint32_t c, uint64_t t, uint32_t s, uint32_t tm,
-                                          uint32_t lane, T *wprod) {
-  const uint32_t n = P.n, slots = P.slots;
-  const uint32_t p0 = P.chunk_beg[c], p1 = P.chunk_beg[c + 1];
-  const bool own = lane < (p1 - p0);
-  const uint32_t p = p0 + lane;
-  const uint32_t slot_prev = (tm == 0) ? slots - 1 : tm - 1;
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(fsd::kFull, v, o);
+  return v;
+}
 
-  // NMDA pull: G_nmda of the previous step's spike phase
-  T gn = (T)0;
-  if (P.in_row) {
-    const uint32_t eb = P.in_row[p0], ee = P.in_row[p1];
-    const uint32_t mb = own ? P.in_row[p] : 0u, me = own ? P.in_row[p + 1] : 0u;
-    const T *sh = (const T *)P.s_hist;
-    for (uint32_t base = eb; base < ee; base += kEdgeBudget) {
-      uint32_t code[8];
-      float w[8];
+// ---- NMDA pull for L steps of a tile: gn[q][j] = sum_e w_e s_pre(tb+j-1-d_e)
+// FP32: the L values an edge needs are consecutive in its presynaptic row
+// s_hist[pre][*], so they are fetched as 16-byte vectors (about L/4 + 1 L2
+// requests per edge instead of L).
+template <int OFF>
+__device__ __forceinline__ void window_fma(float (&acc)[kLB], const float4 (&v)[kLB / 4 + 1], float w, uint32_t L) {
 #pragma unroll
-      for (int u = 0; u < 8; u++) {
-        const uint32_t e = base + lane + 32u * u;
-        code[u] = 0xffffffffu;
-        w[u] = 0.0f;
-        if (e < ee) {
-          code[u] = __ldg(P.in_code + e);
-          w[u] = __ldg(P.in_w + e);
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < 8; u++) {
-        T v = (T)0;
-        if (code[u] != 0xffffffffu) {
-          const uint32_t pre = code[u] & 0xffffffu, d = code[u] >> 24;
-          uint32_t sl = tm + slots - 1u - d;
-          if (sl >= slots) sl -= slots;
-          v = (T)w[u] * ldcg_t<T>(sh + (size_t)sl * n + pre);
-        }
-        wprod[lane + 32u * u] = v;
-      }
-      __syncwarp();
-      if (own) {
-        const uint32_t a = max(mb, base), b = min(me, base + kEdgeBudget);
-        for (uint32_t e = a; e < b; e++) gn += wprod[e - base];
-      }
-      __syncwarp();
+  for (int j = 0; j < (int)kLB; j++) {
+    if ((uint32_t)j < L) {
+      const int k = OFF + j;
+      const float4 q = v[k >> 2];
+      const float x = ((k & 3) == 0) ? q.x : ((k & 3) == 1) ? q.y : ((k & 3) == 2) ? q.z : q.w;
+      acc[j] += w * x;
     }
   }
+}
 
-  bool spk = false;
-  T cinc[4] = {(T)0, (T)0, (T)0, (T)0};
-  if (own) {
-    const uint32_t a = P.act[p];
-    T *G = (T *)P.G, *est = (T *)P.ext_st;
+__device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint32_t np, uint64_t tb, uint32_t L,
+                                              float (*gn)[kLB], uint32_t wid, uint32_t lane) {
+  const float4 *sh = (const float4 *)P.s_hist;
+  const uint32_t S4 = P.slots >> 2, qmask = S4 - 1, mask = P.mask;
+  const uint32_t nw = kThreads / 32;
+  for (uint32_t q = wid; q < np; q += nw) {
+    float acc[kLB];
+#pragma unroll
+    for (uint32_t j = 0; j < kLB; j++) acc[j] = 0.0f;
+    if (P.in_row) {
+      const uint32_t p = p0 + q;
+      const uint32_t e0 = __ldg(P.in_row + p), e1 = __ldg(P.in_row + p + 1);
+      // two edges per lane per round, their vector loads issued together
+      for (uint32_t e = e0 + lane; e < e1; e += 64) {
+        const bool two = e + 32 < e1;
+        uint32_t code[2];
+        float w[2];
+        code[0] = __ldg(P.in_code + e);
+        w[0] = __ldg(P.in_w + e);
+        code[1] = two ? __ldg(P.in_code + e + 32) : 0u;
+        w[1] = two ? __ldg(P.in_w + e + 32) : 0.0f;
+        float4 v[2][kLB / 4 + 1];
+        uint32_t off[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const uint32_t pre = code[h] & 0xffffffu, d = code[h] >> 24;
+          const float4 *row = sh + (size_t)pre * S4;
+          const uint32_t a = (uint32_t)(tb - 1u - d) & mask;
+          off[h] = a & 3u;
+          const uint32_t b0 = a >> 2, nb = (h == 0 || two) ? (off[h] + L + 3u) >> 2 : 0u;
+#pragma unroll
+          for (uint32_t i = 0; i < kLB / 4 + 1; i++)
+            v[h][i] = (i < nb) ? __ldcg(row + ((b0 + i) & qmask)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          switch (off[h]) {
+            case 0: window_fma<0>(acc, v[h], w[h], L); break;
+            case 1: window_fma<1>(acc, v[h], w[h], L); break;
+            case 2: window_fma<2>(acc, v[h], w[h], L); break;
+            default: window_fma<3>(acc, v[h], w[h], L); break;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < kLB; j++) {
+      if (j < L) {
+        const float v = warp_sum<float>(acc[j]);
+        if (lane == j) gn[q][j] = v;
+      }
+    }
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void nmda_pull(const Params &P, uint32_t p0, uint32_t np, uint64_t tb, uint32_t L,
+                                          T (*gn)[kLB], uint32_t wid, uint32_t lane) {
+  const T *sh = (const T *)P.s_hist;
+  const uint32_t S = P.slots, mask = P.mask;
+  const uint32_t nw = kThreads / 32;
+  for (uint32_t q = wid; q < np; q += nw) {
+    T acc[kLB];
+#pragma unroll
+    for (uint32_t j = 0; j < kLB; j++) acc[j] = (T)0;
+    if (P.in_row) {
+      const uint32_t p = p0 + q;
+      const uint32_t e0 = __ldg(P.in_row + p), e1 = __ldg(P.in_row + p + 1);
+      for (uint32_t e = e0 + lane; e < e1; e += 32) {
+        const uint32_t code = __ldg(P.in_code + e);
+        const T w = (T)__ldg(P.in_w + e);
+        const uint32_t pre = code & 0xffffffu, d = code >> 24;
+        const T *row = sh + (size_t)pre * S;
+        const uint32_t a = (uint32_t)(tb - 1u - d) & mask;
+#pragma unroll
+        for (uint32_t j = 0; j < kLB; j++)
+          if (j < L) acc[j] += w * ldcg_t<T>(row + ((a + j) & mask));
+      }
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < kLB; j++) {
+      if (j < L) {
+        const T v = warp_sum<T>(acc[j]);
+        if (lane == j) gn[q][j] = v;
+      }
+    }
+  }
+}
+
+// ---- spike pushes into the delay ring --------------------------------------
+// Threads start, start+stride, ... of a group walk the out-edges of neuron q
+// (four edges per thread per round, loads issued before the atomics) and add
+// w*c[receptor] as 2^-40 fixed point to ring[receptor][post][(tm+delay) mod S].
+template <class T>
+__device__ __forceinline__ void push_spike(const Params &P, uint32_t q, uint32_t tm, const T (&cj)[4],
+                                           uint32_t start, uint32_t stride) {
+  const uint32_t n = P.n, S = P.slots, mask = P.mask;
+  const uint32_t ob = __ldg(P.out_row + q), oe = __ldg(P.out_row + q + 1);
+  for (uint32_t e = ob + start; e < oe; e += 4 * stride) {
+    uint32_t code[4];
+    float w[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const uint32_t eu = e + u * stride;
+      code[u] = eu < oe ? __ldg(P.out_code + eu) : 0u;
+      w[u] = eu < oe ? __ldg(P.out_w + eu) : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      if (e + u * stride < oe) {
+        const uint32_t post = code[u] & 0x3fffffu, r = (code[u] >> 22) & 3u, d = code[u] >> 24;
+        const T cv = (r == 0) ? cj[0] : (r == 1) ? cj[1] : (r == 2) ? cj[2] : cj[3];
+        const long long fx = __double2ll_rn((double)((T)w[u] * cv) * kFix);
+        const int ri = P.lin_of_rec[r];
+        atomicAdd(P.ring + ((size_t)ri * n + post) * S + ((tm + d) & mask), (unsigned long long)fx);
+      }
+    }
+  }
+}
+
+// spikes of a block awaiting their push (shared memory)
+template <class T>
+struct SpikeList {
+  uint32_t *n, *p;
+  uint16_t *tm;
+  T (*c)[4];
+  uint32_t cap;
+};
+
+// ---- drive draws of L steps for a tile -------------------------------------
+// The external Bernoulli outcomes (bit r: receptor r hit this step) and the
+// injection noise depend on no state, so they are drawn for the whole batch
+// by all threads at once, off the neurons' per-step dependency chain.
+template <class T>
+__device__ __forceinline__ void draw_inputs(const Params &P, uint32_t p0, uint32_t np, uint64_t tb, uint32_t L,
+                                            uint8_t (*hits)[kLB], T (*gauss)[kLB]) {
+  const uint32_t n = P.n;
+  for (uint32_t idx = threadIdx.x; idx < np * L; idx += kThreads) {
+    const uint32_t q = idx / L, j = idx - q * L, p = p0 + q;
+    const uint64_t t = tb + j;
+    const uint32_t a = __ldg(P.act + p);
+    uint32_t rnd[4] = {(uint32_t)t, (uint32_t)(t >> 32), p, 0u};
+    philox(rnd, P.key0, P.key1);
+    uint32_t h = 0;
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+      if (__ldg(P.pb + (size_t)r * n + p) > u24(rnd[r])) h |= 1u << r;
+    if (a & (FS_ACT_NMDA | FS_ACT_INJ)) {
+      uint32_t r2[4] = {(uint32_t)t, (uint32_t)(t >> 32), p, 1u};
+      philox(r2, P.key0, P.key1);
+      if (__ldg(P.pb + (size_t)FS_NMDA * n + p) > u24(r2[0])) h |= 1u << FS_NMDA;
+      if (a & FS_ACT_INJ) {  // Box-Muller normal
+        const double u1 = ((double)(r2[1] >> 8) + 1.0) * 5.9604644775390625e-08;
+        const double u2 = (double)(r2[2] >> 8) * 5.9604644775390625e-08;
+        const double z = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+        gauss[q][j] = (T)__ldg(P.inj_mean + p) + (T)__ldg(P.inj_std + p) * (T)z;
+      }
+    }
+    hits[q][j] = (uint8_t)h;
+  }
+}
+
+// ---- L steps of a tile's neurons (thread per neuron), with the pushes ----
+// Per-neuron parameters and state stay in registers for the L steps; the
+// ring slot of the next step is fetched while the current step computes
+// (it is final: every push into it happened before the interval began); a
+// warp pushes the spikes of its own lanes, so a step needs no block barrier.
+template <class T>
+__device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint32_t np, uint32_t sb, uint32_t L,
+                                             T (*gn)[kLB], const uint8_t (*hits)[kLB],
+                                             const T (*gauss)[kLB], const SpikeList<T> &lst) {
+  const uint32_t tid = threadIdx.x, lane = tid & 31;
+  const uint32_t n = P.n, S = P.slots, mask = P.mask;
+  const bool own = tid < np;
+  const uint32_t p = own ? p0 + tid : p0;  // non-owners read a valid neuron, write nothing
+  // ---- parameters ----
+  const uint32_t a = P.act[p];
+  const uint8_t pj = P.proj[p];
+  const int32_t rf = __ldg(P.RfPed + p), sd = __ldg(P.SpiDy + p);
+  const T vth = (T)__ldg(P.Vth + p), vreset = (T)__ldg(P.Vreset + p), df = (T)__ldg(P.df + p),
+          ef = (T)__ldg(P.ef + p), dvm = (T)__ldg(P.dVmax + p), cm = (T)__ldg(P.Cm + p),
+          leak = (T)__ldg(P.gl + p) * (T)__ldg(P.El + p) * (T)1e3, mg = (T)__ldg(P.nmda_mg + p);
+  T vrev[5], dfs[5], extg[5];
+#pragma unroll
+  for (int r = 0; r < 5; r++) {
+    vrev[r] = (T)__ldg(P.Vrev + (size_t)r * n + p);
+    dfs[r] = (T)__ldg(P.dfst + (size_t)r * n + p);
+    extg[r] = (T)__ldg(P.ext_g + (size_t)r * n + p);
+  }
+  const T ndfxt = (T)__ldg(P.nmda_dfxt + p), nefas = (T)__ldg(P.nmda_efst + p) * (T)__ldg(P.nmda_as + p);
+  T pdf[4];
+#pragma unroll
+  for (int r = 0; r < 4; r++) pdf[r] = (T)__ldg(P.pdf + (size_t)r * n + p);
+  const T pdfxt = (T)__ldg(P.p_dfxt + p), pdfst = (T)__ldg(P.p_dfst + p), pefas = (T)__ldg(P.p_efas + p);
+  // ---- state ----
+  T V = ((T *)P.V)[p];
+  int32_t cnt = P.Count[p];
+  uint32_t ns = P.NS[p];
+  T G[4], est[4], sp[4];
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    G[r] = ((T *)P.G)[(size_t)r * n + p];
+    est[r] = ((T *)P.ext_st)[(size_t)r * n + p];
+    sp[r] = ((T *)P.st_pre)[(size_t)r * n + p];
+  }
+  T ex = ((T *)P.ext_x)[p], es = ((T *)P.ext_s)[p], xp = ((T *)P.x_pre)[p], spre = ((T *)P.s_pre)[p];
+  // ring slot of the first step
+  long long rv[4];
+  {
+    const uint32_t tprev = (uint32_t)(P.t0 + sb - 1u) & mask;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int ri = P.lin_of_rec[r];
+      rv[r] = (ri >= 0 && own) ? (long long)__ldcg(P.ring + ((size_t)ri * n + p) * S + tprev) : 0ll;
+    }
+  }
+  for (uint32_t j = 0; j < L; j++) {
+    const uint32_t s = sb + j;
+    const uint64_t t = P.t0 + s;
+    const uint32_t tm = (uint32_t)t & mask, tprev = (uint32_t)(t - 1u) & mask;
+    bool spk = false;
+    T cinc[4] = {0, 0, 0, 0};
+    // conductances of the previous step's spike phase
     T g[5];
 #pragma unroll
     for (int r = 0; r < 4; r++) {
       g[r] = (T)0;
       const int ri = P.lin_of_rec[r];
       if (ri >= 0) {
-        unsigned long long *rp = P.ring + ((size_t)ri * slots + slot_prev) * n + p;
-        const long long v = (long long)__ldcg(rp);
-        if (v) __stcg(rp, 0ull);
-        T Gr = G[(size_t)r * n + p];
-        Gr = (T)P.dfst[(size_t)r * n + p] * Gr + (T)((double)v * kInvFix);
-        G[(size_t)r * n + p] = Gr;
-        g[r] = Gr;
+        if (own && rv[r]) __stcg(P.ring + ((size_t)ri * n + p) * S + tprev, 0ull);
+        G[r] = dfs[r] * G[r] + (T)rv[r] * (T)kInvFix;  // exact power-of-two scale
+        g[r] = G[r];
+        // next step's slot (tm) is final since the interval began
+        rv[r] = (own && j + 1 < L) ? (long long)__ldcg(P.ring + ((size_t)ri * n + p) * S + tm) : 0ll;
       }
     }
-    g[FS_NMDA] = gn;
-    // external drive (BgInit)
-    uint32_t rnd[4] = {(uint32_t)t, (uint32_t)(t >> 32), p, 0u};
-    philox(rnd, P.key0, P.key1);
+    const uint32_t qs = tid < np ? tid : 0;
+    g[FS_NMDA] = gn[qs][j];
+    // external drive (BgInit): the Bernoulli outcomes of this step were drawn
+    // in the pull phase (bit r: receptor r hit)
+    const uint32_t hit = hits[qs][j];
     const uint32_t bitsr[4] = {FS_ACT_AMPA, FS_ACT_GABA, FS_ACT_ACH, FS_ACT_GCL};
 #pragma unroll
     for (int r = 0; r < 4; r++) {
       if (a & bitsr[r]) {
-        const float pb = P.pb[(size_t)r * n + p];
-        T st = est[(size_t)r * n + p];
-        if (pb > u24(rnd[r])) st = st + (T)1;
-        else st = st * (T)P.dfst[(size_t)r * n + p];
-        est[(size_t)r * n + p] = st;
-        g[r] = g[r] + (T)P.ext_g[(size_t)r * n + p] * st;
+        if (hit & (1u << r)) est[r] = est[r] + (T)1;
+        else est[r] = est[r] * dfs[r];
+        g[r] = g[r] + extg[r] * est[r];
       }
     }
     T isyn = (T)0;
-    if (a & (FS_ACT_NMDA | FS_ACT_INJ)) {
-      uint32_t r2[4] = {(uint32_t)t, (uint32_t)(t >> 32), p, 1u};
-      philox(r2, P.key0, P.key1);
-      if (a & FS_ACT_NMDA) {
-        T *ex = (T *)P.ext_x, *es = (T *)P.ext_s;
-        const float pb = P.pb[(size_t)FS_NMDA * n + p];
-        T xt = ex[p], st = es[p];
-        if (pb > u24(r2[0])) xt = xt + (T)1;
-        else xt = xt * (T)P.nmda_dfxt[p];
-        st = (T)P.dfst[(size_t)FS_NMDA * n + p] * st + (T)P.nmda_efst[p] * (T)P.nmda_as[p] * xt * ((T)1 - st);
-        ex[p] = xt;
-        es[p] = st;
-        g[FS_NMDA] = g[FS_NMDA] + (T)P.ext_g[(size_t)FS_NMDA * n + p] * st;
-      }
-      if (a & FS_ACT_INJ) {  // Box-Muller normal
-        const double u1 = ((double)(r2[1] >> 8) + 1.0) * 5.9604644775390625e-08;
-        const double u2 = (double)(r2[2] >> 8) * 5.9604644775390625e-08;
-        const double z = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
-        isyn = (T)P.inj_mean[p] + (T)P.inj_std[p] * (T)z;
-      }
+    if (a & FS_ACT_NMDA) {
+      if (hit & (1u << FS_NMDA)) ex = ex + (T)1;
+      else ex = ex * ndfxt;
+      es = dfs[FS_NMDA] * es + nefas * ex * ((T)1 - es);
+      g[FS_NMDA] = g[FS_NMDA] + extg[FS_NMDA] * es;
     }
+    if (a & FS_ACT_INJ) isyn = (T)gauss[qs][j];
     // VmEul + firing (code/EqsGnl2.cpp:152-251)
-    T *Vp = (T *)P.V;
-    T V = Vp[p];
-    int32_t cnt = P.Count[p];
-    uint32_t ns = P.NS[p];
-    const int32_t rf = P.RfPed[p], sd = P.SpiDy[p];
-    const T vreset = (T)P.Vreset[p];
     bool fire_now = false;
     if (ns & FS_NS_FIRE) {
       fire_now = true;
     } else {
       const T v = V;
-      const T Ir0 = g[FS_AMPA] * ((T)P.Vrev[(size_t)FS_AMPA * n + p] - v);
-      const T Ir1 = g[FS_GABA] * ((T)P.Vrev[(size_t)FS_GABA * n + p] - v);
-      const T Ir2 = g[FS_NMDA] * ((T)P.Vrev[(size_t)FS_NMDA * n + p] - v) /
-                    ((T)1 + (T)P.nmda_mg[p] * exp_t<T>((T)-0.062 * v) / (T)3.57);
-      const T Ir3 = g[FS_ACH] * ((T)P.Vrev[(size_t)FS_ACH * n + p] - v);
-      const T Ir4 = g[FS_GCL] * ((T)P.Vrev[(size_t)FS_GCL * n + p] - v);
-      T I = Ir0 + Ir1 + Ir2 + Ir3 + Ir4 + isyn * (T)1e3 + (T)P.gl[p] * (T)P.El[p] * (T)1e3;
-      I = (T)1e-3 * I / (T)P.Cm[p];
-      const T dv = (T)P.dVmax[p];
-      if (I > dv) {
-        I = dv;
+      const T Ir0 = g[FS_AMPA] * (vrev[FS_AMPA] - v);
+      const T Ir1 = g[FS_GABA] * (vrev[FS_GABA] - v);
+      const T Ir2 = g[FS_NMDA] * (vrev[FS_NMDA] - v) / ((T)1 + mg * exp_t<T>((T)-0.062 * v) / (T)3.57);
+      const T Ir3 = g[FS_ACH] * (vrev[FS_ACH] - v);
+      const T Ir4 = g[FS_GCL] * (vrev[FS_GCL] - v);
+      T I = Ir0 + Ir1 + Ir2 + Ir3 + Ir4 + isyn * (T)1e3 + leak;
+      I = (T)1e-3 * I / cm;
+      if (I > dvm) {
+        I = dvm;
         ns = (ns | FS_NS_MEMDV_OVF) & ~FS_NS_MEMDV_UDF;
-      } else if (I < -dv) {
-        I = -dv;
+      } else if (I < -dvm) {
+        I = -dvm;
         ns = (ns & ~FS_NS_MEMDV_OVF) | FS_NS_MEMDV_UDF;
       } else {
         ns &= ~(FS_NS_MEMDV_OVF | FS_NS_MEMDV_UDF);
       }
-      V = (T)P.df[p] * v + (T)P.ef[p] * I;
-      if (V > (T)P.Vth[p]) {
+      V = df * v + ef * I;
+      if (V > vth) {
         ns |= FS_NS_FIRE;
         fire_now = true;
       }
@@ -289,14 +473,10 @@ __device__ __forceinline__ void run_chunk(const Params &P, uint32_t c, uint64_t 
         ns &= ~FS_NS_FIRE;
       }
     }
-    Vp[p] = V;
-    P.Count[p] = cnt;
-    P.NS[p] = ns;
-    if (P.outV) P.outV[(size_t)s * n + p] = (float)V;
-    spk = (ns & FS_NS_SPIKE) != 0;
+    if (own && P.outV) P.outV[(size_t)s * n + p] = (float)V;
+    spk = own && (ns & FS_NS_SPIKE) != 0;
     // presynaptic state: increment per spike, then plasticity update
-    const uint8_t pj = P.proj[p];
-    if (pj) {
+    if (pj && own) {
       T inc = (T)1;
       if (P.plast == PL_STD) inc = (T)P.D[p];
       else if (P.plast == PL_STP) inc = (T)P.D[p] * (T)P.F[p];
@@ -315,30 +495,22 @@ __device__ __forceinline__ void run_chunk(const Params &P, uint32_t c, uint64_t 
         P.tm_u[p] = (float)u;
         P.tm_x[p] = (float)x;
       }
-      T *sp = (T *)P.st_pre;
 #pragma unroll
       for (int r = 0; r < 4; r++) {
         if (pj & (1u << r)) {
-          T st = sp[(size_t)r * n + p];
-          const T pd = (T)P.pdf[(size_t)r * n + p];
           if (spk) {
-            cinc[r] = inc + st * ((T)1 - pd);
-            st = st + inc;
+            cinc[r] = inc + sp[r] * ((T)1 - pdf[r]);
+            sp[r] = sp[r] + inc;
           } else {
-            st = st * pd;
+            sp[r] = sp[r] * pdf[r];
           }
-          sp[(size_t)r * n + p] = st;
         }
       }
       if (pj & (1u << FS_NMDA)) {
-        T *xp = (T *)P.x_pre, *sq = (T *)P.s_pre;
-        T x = xp[p], sv = sq[p];
-        if (spk) x = x + inc;
-        else x = x * (T)P.p_dfxt[p];
-        sv = (T)P.p_dfst[p] * sv + (T)P.p_efas[p] * x * ((T)1 - sv);
-        xp[p] = x;
-        sq[p] = sv;
-        __stcg((T *)P.s_hist + (size_t)tm * n + p, sv);
+        if (spk) xp = xp + inc;
+        else xp = xp * pdfxt;
+        spre = pdfst * spre + pefas * xp * ((T)1 - spre);
+        __stcg((T *)P.s_hist + (size_t)p * S + tm, spre);
       }
       if (P.plast == PL_STD) {
         P.D[p] = spk ? P.D[p] * (1.0f - P.stp_pv[p]) : P.stp_dfD[p] * P.D[p] + P.stp_efD[p];
@@ -358,48 +530,103 @@ __device__ __forceinline__ void run_chunk(const Params &P, uint32_t c, uint64_t 
         P.D[p] = Dv; P.F[p] = Fv; P.Cap[p] = Cp; P.Car[p] = Cr;
       }
     }
-    if (spk && P.bits) atomicOr(P.bits + (size_t)s * P.words + (p >> 5), 1u << (p & 31));
-  }
-  // spike count and pushes of this warp's spikes
-  uint32_t m = __ballot_sync(fsd::kFull, spk);
-  if (lane == 0 && m) atomicAdd(P.counts + s, (unsigned)__popc(m));
-  while (m) {
-    const int j = __ffs(m) - 1;
-    m &= m - 1;
-    const uint32_t q = p0 + (uint32_t)j;
-    T cj[4];
+    // spikes of this warp: outputs, and the spike list the block pushes at
+    // the end of the batch (a push lands >= min_delay steps ahead, so it may
+    // wait until the interval's end); a full list falls back to a push by
+    // this warp right away
+    uint32_t m = __ballot_sync(fsd::kFull, spk);
+    if (m) {
+      if (spk && P.bits) atomicOr(P.bits + (size_t)s * P.words + (p >> 5), 1u << (p & 31));
+      if (lane == 0) {
+        atomicAdd(P.counts + s, (unsigned)__popc(m));
+        atomicAdd(P.spike_total, (unsigned long long)__popc(m));
+      }
+      bool listed = false;
+      if (spk) {
+        const uint32_t k = atomicAdd(lst.n, 1u);
+        if (k < lst.cap) {
+          lst.p[k] = p;
+          lst.tm[k] = (uint16_t)tm;
 #pragma unroll
-    for (int r = 0; r < 4; r++) cj[r] = __shfl_sync(fsd::kFull, cinc[r], j);
-    const uint32_t ob = P.out_row[q], oe = P.out_row[q + 1];
-    for (uint32_t e = ob + lane; e < oe; e += 32) {
-      const uint32_t code = __ldg(P.out_code + e);
-      const float w = __ldg(P.out_w + e);
-      const uint32_t post = code & 0x3fffffu, r = (code >> 22) & 3u, d = code >> 24;
-      uint32_t sl = tm + d;
-      if (sl >= slots) sl -= slots;
-      const T cv = (r == 0) ? cj[0] : (r == 1) ? cj[1] : (r == 2) ? cj[2] : cj[3];
-      const T val = (T)w * cv;
-      const long long fx = __double2ll_rn((double)val * kFix);
-      const int ri = P.lin_of_rec[r];
-      atomicAdd(P.ring + ((size_t)ri * slots + sl) * n + post, (unsigned long long)fx);
+          for (int r = 0; r < 4; r++) lst.c[k][r] = cinc[r];
+          listed = true;
+        }
+      }
+      uint32_t over = __ballot_sync(fsd::kFull, spk && !listed);
+      while (over) {
+        const int jl = __ffs(over) - 1;
+        over &= over - 1;
+        const uint32_t q = __shfl_sync(fsd::kFull, p, jl);
+        T cj[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) cj[r] = __shfl_sync(fsd::kFull, cinc[r], jl);
+        push_spike<T>(P, q, tm, cj, lane, 32);
+      }
     }
+  }
+  if (own) {
+    ((T *)P.V)[p] = V;
+    P.Count[p] = cnt;
+    P.NS[p] = ns;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      ((T *)P.G)[(size_t)r * n + p] = G[r];
+      ((T *)P.ext_st)[(size_t)r * n + p] = est[r];
+      ((T *)P.st_pre)[(size_t)r * n + p] = sp[r];
+    }
+    ((T *)P.ext_x)[p] = ex;
+    ((T *)P.ext_s)[p] = es;
+    ((T *)P.x_pre)[p] = xp;
+    ((T *)P.s_pre)[p] = spre;
   }
 }
 
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_prod(const __grid_constant__ Params P) {
-  __shared__ T wbuf[kThreads / 32][kEdgeBudget];
-  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const uint32_t cb = P.block_chunk[blockIdx.x], ce = P.block_chunk[blockIdx.x + 1];
-  uint32_t nbar = 0;
-  uint32_t tm = (uint32_t)(P.t0 % P.slots);
-  for (uint32_t s = 0; s < P.nsteps; s++) {
-    const uint64_t t = P.t0 + s;
-    for (uint32_t c = cb + wid; c < ce; c += nw) run_chunk<T>(P, c, t, s, tm, lane, wbuf[wid]);
-    if (++tm == P.slots) tm = 0;
-    if (((s + 1) % P.interval) == 0 && s + 1 < P.nsteps) {
-      nbar++;
-      if (!grid_sync(P.bar, nbar * gridDim.x, P.err)) return;
+  // FP64 tiles are half as wide so the per-tile buffers stay in static
+  // shared memory
+  constexpr uint32_t kT = sizeof(T) == 4 ? kTile : kTile / 2;
+  constexpr uint32_t kCap = sizeof(T) == 4 ? 512 : 192;
+  __shared__ T gn[kT][kLB];
+  __shared__ T gauss[kT][kLB];
+  __shared__ uint8_t hits[kT][kLB];
+  __shared__ uint32_t l_n, l_p[kCap];
+  __shared__ uint16_t l_tm[kCap];
+  __shared__ T l_c[kCap][4];
+  const SpikeList<T> lst{&l_n, l_p, l_tm, l_c, kCap};
+  const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const uint32_t B0 = P.block_post[blockIdx.x], B1 = P.block_post[blockIdx.x + 1];
+  if (tid == 0) l_n = 0;
+  __syncthreads();
+  uint32_t s = 0;
+  while (s < P.nsteps) {
+    const uint32_t iv_end = min(P.nsteps, s + P.interval);
+    for (uint32_t bs = s; bs < iv_end; bs += kLB) {
+      const uint32_t L = min(kLB, iv_end - bs);
+      for (uint32_t tp0 = B0; tp0 < B1; tp0 += kT) {
+        const uint32_t np = min(kT, B1 - tp0);
+        if constexpr (sizeof(T) == 4) nmda_pull_f32(P, tp0, np, P.t0 + bs, L, (float (*)[kLB])gn, wid, lane);
+        else nmda_pull<T>(P, tp0, np, P.t0 + bs, L, gn, wid, lane);
+        draw_inputs<T>(P, tp0, np, P.t0 + bs, L, hits, gauss);
+        __syncthreads();
+        // warps without neurons in this tile skip the steps
+        if ((tid & ~31u) < np) neuron_steps<T>(P, tp0, np, bs, L, gn, hits, gauss, lst);
+        __syncthreads();
+        // the batch's spikes, pushed by the whole block
+        const uint32_t nl = min(l_n, kCap);
+        for (uint32_t k = 0; k < nl; k++) {
+          T cj[4];
+#pragma unroll
+          for (int r = 0; r < 4; r++) cj[r] = l_c[k][r];
+          push_spike<T>(P, l_p[k], l_tm[k], cj, tid, kThreads);
+        }
+        __syncthreads();
+        if (tid == 0) l_n = 0;
+      }
+    }
+    s = iv_end;
+    if (s < P.nsteps) {
+      if (!grid_sync(P.bar, P.err)) return;
     }
   }
 }
@@ -422,6 +649,7 @@ struct Prod {
   uint64_t cap_steps = 0, outv_steps = 0;
   unsigned int *bar = nullptr;
   int *err = nullptr;
+  unsigned long long *spike_total = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   double ms = 0.0;
   uint64_t kl = 0;
@@ -481,7 +709,7 @@ int launch(Prod *p, uint32_t nsteps, bool want_bits, bool wantV, cudaStream_t st
   const uint32_t words = (p->n + 31) / 32;
   cudaError_t e = cudaMemsetAsync(p->counts, 0, (size_t)nsteps * 4, st);
   if (e == cudaSuccess && want_bits) e = cudaMemsetAsync(p->bits, 0, (size_t)nsteps * words * 4, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(p->bar, 0, 4, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(p->bar, 0, 64 * 4, st);
   if (e != cudaSuccess) {
     err = std::string("memset: ") + cudaGetErrorString(e);
     return FS_ERR_CUDA;
@@ -495,6 +723,7 @@ int launch(Prod *p, uint32_t nsteps, bool want_bits, bool wantV, cudaStream_t st
   P.outV = wantV ? p->outV : nullptr;
   P.bar = p->bar;
   P.err = p->err;
+  P.spike_total = p->spike_total;
   void *args[] = {&P};
   cudaEventRecord(p->e0, st);
   if (p->fp64) e = cudaLaunchCooperativeKernel((void *)k_prod<double>, p->blocks, kThreads, args, 0, st);
@@ -609,7 +838,12 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
   p->d_max = dmax;
   p->lin_edges = nlin_e;
   p->nmda_edges = nnm_e;
-  P.slots = dmax + dmin + 2;
+  {
+    uint32_t need = dmax + dmin + 2, S = 8;
+    while (S < need) S <<= 1;
+    P.slots = S;
+    P.mask = S - 1;
+  }
   P.interval = std::max<uint32_t>(1, dmin);
   for (int r = 0; r < 4; r++) P.lin_of_rec[r] = present[r] ? (int)(p->nlin++) : -1;
   P.nlin = p->nlin;
@@ -639,47 +873,29 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
       }
     }
   }
-  // ---- chunks: <= 32 consecutive posts and <= kEdgeBudget NMDA in-edges ----
-  std::vector<uint32_t> chunk_beg;
-  chunk_beg.push_back(0);
-  {
-    uint32_t start = 0;
-    while (start < n) {
-      uint32_t end = start + 1;
-      while (end < n && end - start < 32 && in_row[end + 1] - in_row[start] <= kEdgeBudget) end++;
-      chunk_beg.push_back(end);
-      start = end;
-    }
-  }
-  const uint32_t nchunks = (uint32_t)chunk_beg.size() - 1;
-  p->chunks = nchunks;
-  // ---- grid: all blocks co-resident; chunks split by estimated cost ----
+  // ---- grid: all blocks co-resident; posts split by estimated cost ----
   int occ = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p->fp64 ? (const void *)k_prod<double> : (const void *)k_prod<float>,
                                                 kThreads, 0);
   if (occ < 1) occ = 1;
   uint32_t blocks = sm_count * (uint32_t)std::min(occ, 4);
-  const uint32_t want = (nchunks + (kThreads / 32) - 1) / (kThreads / 32);
-  blocks = std::max<uint32_t>(1, std::min(blocks, std::max<uint32_t>(want, 1)));
+  blocks = std::max<uint32_t>(1, std::min<uint32_t>(blocks, (n + 7) / 8));
   p->blocks = blocks;
-  std::vector<double> cost(nchunks);
-  double total = 0;
-  for (uint32_t c = 0; c < nchunks; c++) {
-    const uint32_t a = chunk_beg[c], b = chunk_beg[c + 1];
-    cost[c] = 40.0 + 2.0 * (b - a) + (double)(in_row[b] - in_row[a]);
-    total += cost[c];
-  }
-  std::vector<uint32_t> block_chunk(blocks + 1, nchunks);
-  block_chunk[0] = 0;
+  std::vector<uint32_t> block_post(blocks + 1, n);
+  block_post[0] = 0;
   {
+    // cost of a post: its NMDA in-edges (pull) plus a fixed update cost
+    const double upd = 24.0;
+    const double total = (double)nnm_e + upd * n;
     double acc = 0;
     uint32_t b = 1;
-    for (uint32_t c = 0; c < nchunks && b < blocks; c++) {
-      acc += cost[c];
-      while (b < blocks && acc >= total * b / blocks) block_chunk[b++] = c + 1;
+    for (uint32_t q = 0; q < n && b < blocks; q++) {
+      acc += upd + (double)(in_row[q + 1] - in_row[q]);
+      while (b < blocks && acc >= total * b / blocks) block_post[b++] = q + 1;
     }
-    for (; b < blocks; b++) block_chunk[b] = nchunks;
+    for (; b < blocks; b++) block_post[b] = n;
   }
+  p->chunks = blocks;
   // ---- device arrays ----
   int rc = 0;
   const size_t T = p->fp64 ? 8 : 4;
@@ -742,9 +958,10 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
   } else {
     P.in_row = nullptr;
   }
-  UPU(chunk_beg, chunk_beg.data(), chunk_beg.size());
-  UPU(block_chunk, block_chunk.data(), block_chunk.size());
-  if ((rc = dal(p, &p->bar, 1, err)) || (rc = dal(p, &p->err, 1, err))) goto fail;
+  UPU(block_post, block_post.data(), block_post.size());
+  if ((rc = dal(p, &p->bar, 64, err)) || (rc = dal(p, &p->err, 1, err)) ||
+      (rc = dup(p, &p->spike_total, (const unsigned long long *)nullptr, 1, st, err)))
+    goto fail;
   if (cudaMemsetAsync(p->err, 0, 4, st) != cudaSuccess) { rc = FS_ERR_CUDA; err = "memset"; goto fail; }
   if (cudaEventCreate(&p->e0) != cudaSuccess || cudaEventCreate(&p->e1) != cudaSuccess) {
     rc = FS_ERR_CUDA;
@@ -808,6 +1025,7 @@ int prod_reset(Prod *p, uint32_t seed, cudaStream_t st, std::string &err) {
   z(P.Count, n * 4); z(P.NS, n * 4); z(P.Cap, n * 4); z(P.Car, n * 4);
   z(P.ring, (size_t)std::max<uint32_t>(1, p->nlin) * P.slots * n * 8);
   z(p->err, 4);
+  z(p->spike_total, 8);
   if (e == cudaSuccess) {
     k_prod_init<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, p->fp64 ? 1 : 0);
     e = cudaGetLastError();
@@ -883,7 +1101,13 @@ int prod_run(Prod *p, uint32_t nsteps, cudaStream_t st, uint64_t *launches, std:
 int prod_check(Prod *p, cudaStream_t st, uint64_t *spikes_total, std::string &err) {
   int rc = finish(p, st, err);
   if (rc) return rc;
-  (void)spikes_total;
+  unsigned long long tot = 0;
+  cudaError_t e = cudaMemcpy(&tot, p->spike_total, 8, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    err = cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  if (spikes_total) *spikes_total = tot;
   return FS_OK;
 }
 

@@ -221,6 +221,9 @@ int fs_step(fs_handle *h, uint32_t nsteps, fs_step_out *out);
 /* Device-resident variant for timing: runs nsteps with no host copies; the
  * per-step spike counts stay on the device. */
 int fs_run(fs_handle *h, uint32_t nsteps);
+/* fs_run bracketed by CUDA events on the engine stream; returns the device
+ * time of the whole call (ms) after synchronising. */
+int fs_run_timed(fs_handle *h, uint32_t nsteps, double *device_ms);
 /* Synchronise and report counters. */
 int fs_sync(fs_handle *h);
 int fs_stats(fs_handle *h, uint64_t *steps_done, uint64_t *spikes_total, uint64_t *kernel_launches);
