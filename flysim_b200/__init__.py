@@ -78,7 +78,8 @@ class NetDesc(C.Structure):
 
 
 class RunOpts(C.Structure):
-    _fields_ = [("mode", C.c_int), ("device", C.c_int), ("chunk_steps", C.c_uint32), ("philox_key", C.c_uint64)]
+    _fields_ = [("mode", C.c_int), ("device", C.c_int), ("chunk_steps", C.c_uint32), ("philox_key", C.c_uint64),
+                ("blocks_per_sm", C.c_uint32)]
 
 
 class StepOut(C.Structure):
@@ -229,7 +230,7 @@ class Model:
 
     def run(self, out_dir: str, mode: str = "compat", device: int = 0, chunk_steps: int = 0) -> float:
         """Runs the whole protocol on the GPU and writes the .pro's output files."""
-        o = RunOpts(MODES[mode], device, chunk_steps, 0)
+        o = RunOpts(MODES[mode], device, chunk_steps, 0, 0)
         secs = C.c_double()
         rc = lib().fs_model_run(self._h, C.byref(o), out_dir.encode(), C.byref(secs))
         if rc != FS_OK:
@@ -248,10 +249,11 @@ class Model:
 class Engine:
     """One network instance on one GPU (fs_create ... fs_destroy)."""
 
-    def __init__(self, desc, mode: str = "compat", device: int = 0, chunk_steps: int = 0, philox_key: int = 0):
+    def __init__(self, desc, mode: str = "compat", device: int = 0, chunk_steps: int = 0, philox_key: int = 0,
+                 blocks_per_sm: int = 0):
         L = lib()
         self._keep = getattr(desc, "_keep", None)
-        o = RunOpts(MODES[mode], device, chunk_steps, philox_key)
+        o = RunOpts(MODES[mode], device, chunk_steps, philox_key, blocks_per_sm)
         h = C.c_void_p()
         dp = desc if isinstance(desc, C._Pointer) else C.pointer(desc)
         rc = L.fs_create(dp, C.byref(o), C.byref(h))

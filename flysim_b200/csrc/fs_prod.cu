@@ -51,6 +51,11 @@ constexpr double kInvFix = 9.094947017729282e-13;  // 2^-40
 constexpr uint32_t kThreads = 256;
 constexpr uint32_t kTile = 256;  // post neurons advanced together (one per thread)
 constexpr uint32_t kLB = 16;     // steps per NMDA pull batch
+// posts per tile (FP64 tiles are half as wide so the per-tile buffers stay
+// in static shared memory); per-tile buffers are step-major, [step][post],
+// so the per-step reads of consecutive threads hit consecutive banks
+template <class T>
+struct TileW { static constexpr uint32_t W = sizeof(T) == 4 ? kTile : kTile / 2; };
 
 enum { PL_NONE = 0, PL_STD = 1, PL_STP = 2, PL_TM = 3 };
 
@@ -159,27 +164,25 @@ __device__ __forceinline__ T warp_sum(T v) {
   return v;
 }
 
-// ---- NMDA pull for L steps of a tile: gn[q][j] = sum_e w_e s_pre(tb+j-1-d_e)
-// FP32: the L values an edge needs are consecutive in its presynaptic row
-// s_hist[pre][*], so they are fetched as 16-byte vectors (about L/4 + 1 L2
-// requests per edge instead of L).
-template <int OFF>
-__device__ __forceinline__ void window_fma(float (&acc)[kLB], const float4 (&v)[kLB / 4 + 1], float w, uint32_t L) {
-#pragma unroll
-  for (int j = 0; j < (int)kLB; j++) {
-    if ((uint32_t)j < L) {
-      const int k = OFF + j;
-      const float4 q = v[k >> 2];
-      const float x = ((k & 3) == 0) ? q.x : ((k & 3) == 1) ? q.y : ((k & 3) == 2) ? q.z : q.w;
-      acc[j] += w * x;
-    }
-  }
+// ---- NMDA pull for L steps of a tile: gn[j][q] = sum_e w_e s_pre(tb+j-1-d_e)
+// FP32: every neuron keeps its s history as 4 rows, row k shifted by k
+// slots (row k, element i = slot (i + k) mod S).  The L consecutive values an
+// edge needs then start on a 16-byte boundary of row (start mod 4), so they
+// arrive as ceil(L/4) aligned vector loads with every value in a fixed
+// register; each lane keeps four edges' loads in flight.
+constexpr uint32_t kSH = 4;  // shifted copies of the s history (FP32)
+
+__device__ __forceinline__ float comp4(const float4 &q, int k) {
+  return k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w;
 }
 
 __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint32_t np, uint64_t tb, uint32_t L,
-                                              float (*gn)[kLB], uint32_t wid, uint32_t lane) {
+                                              float (*gn)[kTile], uint32_t wid, uint32_t lane) {
+  constexpr int U = 4;                 // edges per lane per round
+  constexpr int NV = kLB / 4;          // vectors per edge window
   const float4 *sh = (const float4 *)P.s_hist;
   const uint32_t S4 = P.slots >> 2, qmask = S4 - 1, mask = P.mask;
+  const uint32_t nvl = (L + 3u) >> 2;  // vectors needed for L steps
   const uint32_t nw = kThreads / 32;
   for (uint32_t q = wid; q < np; q += nw) {
     float acc[kLB];
@@ -188,36 +191,32 @@ __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint
     if (P.in_row) {
       const uint32_t p = p0 + q;
       const uint32_t e0 = __ldg(P.in_row + p), e1 = __ldg(P.in_row + p + 1);
-      // two edges per lane per round, their vector loads issued together
-      for (uint32_t e = e0 + lane; e < e1; e += 64) {
-        const bool two = e + 32 < e1;
-        uint32_t code[2];
-        float w[2];
-        code[0] = __ldg(P.in_code + e);
-        w[0] = __ldg(P.in_w + e);
-        code[1] = two ? __ldg(P.in_code + e + 32) : 0u;
-        w[1] = two ? __ldg(P.in_w + e + 32) : 0.0f;
-        float4 v[2][kLB / 4 + 1];
-        uint32_t off[2];
+      for (uint32_t e = e0 + lane; e < e1; e += 32u * U) {
+        uint32_t code[U];
+        float w[U];
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-          const uint32_t pre = code[h] & 0xffffffu, d = code[h] >> 24;
-          const float4 *row = sh + (size_t)pre * S4;
+        for (int u = 0; u < U; u++) {
+          const uint32_t eu = e + 32u * u;
+          code[u] = eu < e1 ? __ldg(P.in_code + eu) : 0u;
+          w[u] = eu < e1 ? __ldg(P.in_w + eu) : 0.0f;
+        }
+        float4 v[U][NV];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const bool ok = e + 32u * u < e1;
+          const uint32_t pre = code[u] & 0xffffffu, d = code[u] >> 24;
           const uint32_t a = (uint32_t)(tb - 1u - d) & mask;
-          off[h] = a & 3u;
-          const uint32_t b0 = a >> 2, nb = (h == 0 || two) ? (off[h] + L + 3u) >> 2 : 0u;
+          const float4 *row = sh + ((size_t)pre * kSH + (a & 3u)) * S4;
+          const uint32_t i0 = a >> 2;
 #pragma unroll
-          for (uint32_t i = 0; i < kLB / 4 + 1; i++)
-            v[h][i] = (i < nb) ? __ldcg(row + ((b0 + i) & qmask)) : make_float4(0.f, 0.f, 0.f, 0.f);
+          for (int i = 0; i < NV; i++)
+            v[u][i] = (ok && (uint32_t)i < nvl) ? __ldcg(row + ((i0 + i) & qmask)) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-          switch (off[h]) {
-            case 0: window_fma<0>(acc, v[h], w[h], L); break;
-            case 1: window_fma<1>(acc, v[h], w[h], L); break;
-            case 2: window_fma<2>(acc, v[h], w[h], L); break;
-            default: window_fma<3>(acc, v[h], w[h], L); break;
-          }
+        for (int u = 0; u < U; u++) {
+#pragma unroll
+          for (int j = 0; j < (int)kLB; j++)
+            if ((uint32_t)j < L) acc[j] += w[u] * comp4(v[u][j >> 2], j & 3);
         }
       }
     }
@@ -225,7 +224,7 @@ __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint
     for (uint32_t j = 0; j < kLB; j++) {
       if (j < L) {
         const float v = warp_sum<float>(acc[j]);
-        if (lane == j) gn[q][j] = v;
+        if (lane == j) gn[j][q] = v;
       }
     }
   }
@@ -233,7 +232,7 @@ __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint
 
 template <class T>
 __device__ __forceinline__ void nmda_pull(const Params &P, uint32_t p0, uint32_t np, uint64_t tb, uint32_t L,
-                                          T (*gn)[kLB], uint32_t wid, uint32_t lane) {
+                                          T (*gn)[TileW<T>::W], uint32_t wid, uint32_t lane) {
   const T *sh = (const T *)P.s_hist;
   const uint32_t S = P.slots, mask = P.mask;
   const uint32_t nw = kThreads / 32;
@@ -259,7 +258,7 @@ __device__ __forceinline__ void nmda_pull(const Params &P, uint32_t p0, uint32_t
     for (uint32_t j = 0; j < kLB; j++) {
       if (j < L) {
         const T v = warp_sum<T>(acc[j]);
-        if (lane == j) gn[q][j] = v;
+        if (lane == j) gn[j][q] = v;
       }
     }
   }
@@ -311,10 +310,10 @@ struct SpikeList {
 // by all threads at once, off the neurons' per-step dependency chain.
 template <class T>
 __device__ __forceinline__ void draw_inputs(const Params &P, uint32_t p0, uint32_t np, uint64_t tb, uint32_t L,
-                                            uint8_t (*hits)[kLB], T (*gauss)[kLB]) {
+                                            uint8_t (*hits)[TileW<T>::W], T (*gauss)[TileW<T>::W]) {
   const uint32_t n = P.n;
   for (uint32_t idx = threadIdx.x; idx < np * L; idx += kThreads) {
-    const uint32_t q = idx / L, j = idx - q * L, p = p0 + q;
+    const uint32_t j = idx / np, q = idx - j * np, p = p0 + q;
     const uint64_t t = tb + j;
     const uint32_t a = __ldg(P.act + p);
     uint32_t rnd[4] = {(uint32_t)t, (uint32_t)(t >> 32), p, 0u};
@@ -331,10 +330,10 @@ __device__ __forceinline__ void draw_inputs(const Params &P, uint32_t p0, uint32
         const double u1 = ((double)(r2[1] >> 8) + 1.0) * 5.9604644775390625e-08;
         const double u2 = (double)(r2[2] >> 8) * 5.9604644775390625e-08;
         const double z = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
-        gauss[q][j] = (T)__ldg(P.inj_mean + p) + (T)__ldg(P.inj_std + p) * (T)z;
+        gauss[j][q] = (T)__ldg(P.inj_mean + p) + (T)__ldg(P.inj_std + p) * (T)z;
       }
     }
-    hits[q][j] = (uint8_t)h;
+    hits[j][q] = (uint8_t)h;
   }
 }
 
@@ -345,8 +344,8 @@ __device__ __forceinline__ void draw_inputs(const Params &P, uint32_t p0, uint32
 // warp pushes the spikes of its own lanes, so a step needs no block barrier.
 template <class T>
 __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint32_t np, uint32_t sb, uint32_t L,
-                                             T (*gn)[kLB], const uint8_t (*hits)[kLB],
-                                             const T (*gauss)[kLB], const SpikeList<T> &lst) {
+                                             T (*gn)[TileW<T>::W], const uint8_t (*hits)[TileW<T>::W],
+                                             const T (*gauss)[TileW<T>::W], const SpikeList<T> &lst) {
   const uint32_t tid = threadIdx.x, lane = tid & 31;
   const uint32_t n = P.n, S = P.slots, mask = P.mask;
   const bool own = tid < np;
@@ -413,10 +412,10 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
       }
     }
     const uint32_t qs = tid < np ? tid : 0;
-    g[FS_NMDA] = gn[qs][j];
+    g[FS_NMDA] = gn[j][qs];
     // external drive (BgInit): the Bernoulli outcomes of this step were drawn
     // in the pull phase (bit r: receptor r hit)
-    const uint32_t hit = hits[qs][j];
+    const uint32_t hit = hits[j][qs];
     const uint32_t bitsr[4] = {FS_ACT_AMPA, FS_ACT_GABA, FS_ACT_ACH, FS_ACT_GCL};
 #pragma unroll
     for (int r = 0; r < 4; r++) {
@@ -433,7 +432,7 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
       es = dfs[FS_NMDA] * es + nefas * ex * ((T)1 - es);
       g[FS_NMDA] = g[FS_NMDA] + extg[FS_NMDA] * es;
     }
-    if (a & FS_ACT_INJ) isyn = (T)gauss[qs][j];
+    if (a & FS_ACT_INJ) isyn = (T)gauss[j][qs];
     // VmEul + firing (code/EqsGnl2.cpp:152-251)
     bool fire_now = false;
     if (ns & FS_NS_FIRE) {
@@ -510,7 +509,13 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
         if (spk) xp = xp + inc;
         else xp = xp * pdfxt;
         spre = pdfst * spre + pefas * xp * ((T)1 - spre);
-        __stcg((T *)P.s_hist + (size_t)p * S + tm, spre);
+        if constexpr (sizeof(T) == 4) {
+#pragma unroll
+          for (uint32_t k = 0; k < kSH; k++)
+            __stcg((T *)P.s_hist + ((size_t)p * kSH + k) * S + ((tm - k) & mask), spre);
+        } else {
+          __stcg((T *)P.s_hist + (size_t)p * S + tm, spre);
+        }
       }
       if (P.plast == PL_STD) {
         P.D[p] = spk ? P.D[p] * (1.0f - P.stp_pv[p]) : P.stp_dfD[p] * P.D[p] + P.stp_efD[p];
@@ -585,11 +590,11 @@ template <class T>
 __global__ void __launch_bounds__(kThreads) k_prod(const __grid_constant__ Params P) {
   // FP64 tiles are half as wide so the per-tile buffers stay in static
   // shared memory
-  constexpr uint32_t kT = sizeof(T) == 4 ? kTile : kTile / 2;
+  constexpr uint32_t kT = TileW<T>::W;
   constexpr uint32_t kCap = sizeof(T) == 4 ? 512 : 192;
-  __shared__ T gn[kT][kLB];
-  __shared__ T gauss[kT][kLB];
-  __shared__ uint8_t hits[kT][kLB];
+  __shared__ T gn[kLB][kT];
+  __shared__ T gauss[kLB][kT];
+  __shared__ uint8_t hits[kLB][kT];
   __shared__ uint32_t l_n, l_p[kCap];
   __shared__ uint16_t l_tm[kCap];
   __shared__ T l_c[kCap][4];
@@ -605,7 +610,7 @@ __global__ void __launch_bounds__(kThreads) k_prod(const __grid_constant__ Param
       const uint32_t L = min(kLB, iv_end - bs);
       for (uint32_t tp0 = B0; tp0 < B1; tp0 += kT) {
         const uint32_t np = min(kT, B1 - tp0);
-        if constexpr (sizeof(T) == 4) nmda_pull_f32(P, tp0, np, P.t0 + bs, L, (float (*)[kLB])gn, wid, lane);
+        if constexpr (sizeof(T) == 4) nmda_pull_f32(P, tp0, np, P.t0 + bs, L, (float (*)[kTile])gn, wid, lane);
         else nmda_pull<T>(P, tp0, np, P.t0 + bs, L, gn, wid, lane);
         draw_inputs<T>(P, tp0, np, P.t0 + bs, L, hits, gauss);
         __syncthreads();
@@ -878,7 +883,9 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p->fp64 ? (const void *)k_prod<double> : (const void *)k_prod<float>,
                                                 kThreads, 0);
   if (occ < 1) occ = 1;
-  uint32_t blocks = sm_count * (uint32_t)std::min(occ, 4);
+  int per_sm = std::min(occ, 4);
+  if (o.blocks_per_sm) per_sm = std::min<int>(occ, (int)o.blocks_per_sm);
+  uint32_t blocks = sm_count * (uint32_t)per_sm;
   blocks = std::max<uint32_t>(1, std::min<uint32_t>(blocks, (n + 7) / 8));
   p->blocks = blocks;
   std::vector<uint32_t> block_post(blocks + 1, n);
@@ -941,7 +948,7 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
       (rc = dup(p, (uint8_t **)&P.st_pre, (const uint8_t *)nullptr, 4 * n * T, st, err)) ||
       (rc = dup(p, (uint8_t **)&P.x_pre, (const uint8_t *)nullptr, n * T, st, err)) ||
       (rc = dup(p, (uint8_t **)&P.s_pre, (const uint8_t *)nullptr, n * T, st, err)) ||
-      (rc = dup(p, (uint8_t **)&P.s_hist, (const uint8_t *)nullptr, (size_t)P.slots * n * T, st, err)) ||
+      (rc = dup(p, (uint8_t **)&P.s_hist, (const uint8_t *)nullptr, (size_t)P.slots * n * T * (p->fp64 ? 1 : kSH), st, err)) ||
       (rc = dup(p, &P.Count, (const int32_t *)nullptr, n, st, err)) ||
       (rc = dup(p, &P.NS, (const uint32_t *)nullptr, n, st, err)) ||
       (rc = dup(p, &P.D, (const float *)nullptr, n, st, err)) || (rc = dup(p, &P.F, (const float *)nullptr, n, st, err)) ||
@@ -1021,7 +1028,7 @@ int prod_reset(Prod *p, uint32_t seed, cudaStream_t st, std::string &err) {
     if (e == cudaSuccess && ptr && bytes) e = cudaMemsetAsync(ptr, 0, bytes, st);
   };
   z(P.G, 4 * n * T); z(P.ext_st, 4 * n * T); z(P.ext_x, n * T); z(P.ext_s, n * T);
-  z(P.st_pre, 4 * n * T); z(P.x_pre, n * T); z(P.s_pre, n * T); z(P.s_hist, (size_t)P.slots * n * T);
+  z(P.st_pre, 4 * n * T); z(P.x_pre, n * T); z(P.s_pre, n * T); z(P.s_hist, (size_t)P.slots * n * T * (p->fp64 ? 1 : kSH));
   z(P.Count, n * 4); z(P.NS, n * 4); z(P.Cap, n * 4); z(P.Car, n * 4);
   z(P.ring, (size_t)std::max<uint32_t>(1, p->nlin) * P.slots * n * 8);
   z(p->err, 4);

@@ -174,6 +174,8 @@ typedef struct fs_run_opts {
   int device;          /* CUDA device ordinal                             */
   uint32_t chunk_steps;/* steps per device launch batch (0 = default 1000)*/
   uint64_t philox_key; /* production modes: drive stream key              */
+  uint32_t blocks_per_sm; /* production modes: resident blocks per SM of the
+                             persistent kernel (0 = as many as fit, <= 4)  */
 } fs_run_opts;
 
 /* Per-call step outputs (host memory, caller owned; NULL = not wanted). */
