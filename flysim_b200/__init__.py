@@ -128,6 +128,7 @@ def lib() -> C.CDLL:
         "fs_stats": (C.c_int, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "fs_kernel_time": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
         "fs_debug_expf": (C.c_int, [_f, _f, C.c_uint64]),
+        "fs_debug_expf_noalloc": (C.c_int, [_f, _f, C.c_uint64]),
         "fs_get_state": (C.c_int, [vp, _f, _i32, _u32]),
         "fs_get_syn_state": (C.c_int, [vp, _f, _f]),
         "fs_model_load": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(ModelOpts), C.POINTER(vp)]),
@@ -153,7 +154,8 @@ def exported_symbols() -> Sequence[str]:
     return [n for n in ("fs_abi_version", "fs_last_error", "fs_device_count", "fs_create", "fs_destroy",
                         "fs_reset", "fs_set_drive", "fs_set_act", "fs_set_injection", "fs_step", "fs_run",
                         "fs_run_timed",
-                        "fs_sync", "fs_stats", "fs_kernel_time", "fs_debug_expf", "fs_get_state",
+                        "fs_sync", "fs_stats", "fs_kernel_time", "fs_debug_expf", "fs_debug_expf_noalloc",
+                        "fs_get_state",
                         "fs_get_syn_state", "fs_model_load", "fs_model_free", "fs_model_error",
                         "fs_model_desc", "fs_model_info", "fs_model_seed", "fs_model_run",
                         "fs_model_run_with", "fs_device_engine")]
@@ -352,6 +354,18 @@ def debug_expf(x: np.ndarray) -> np.ndarray:
     x = np.ascontiguousarray(x, np.float32)
     y = np.zeros_like(x)
     _check(lib().fs_debug_expf(x.ctypes.data_as(_f), y.ctypes.data_as(_f), x.size))
+    return y
+
+
+NOALLOC_MAX_K = 262144  # FS_NOALLOC_MAX_K
+
+
+def debug_expf_noalloc(x: np.ndarray) -> np.ndarray:
+    """fs_debug_expf_noalloc: the device expf without per-call device
+    allocation (at most NOALLOC_MAX_K values per call)."""
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.zeros_like(x)
+    _check(lib().fs_debug_expf_noalloc(x.ctypes.data_as(_f), y.ctypes.data_as(_f), x.size))
     return y
 
 

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 #include <cuda_runtime.h>
@@ -694,3 +695,84 @@ int fs_debug_expf(const float *x, float *y, uint64_t k) {
 }
 
 }  // extern "C"
+
+// ---- allocation-free device expf check ------------------------------------
+// fs_debug_expf_noalloc runs the same kernel as fs_debug_expf, with its
+// exception table and its staging buffers in one fixed device array instead
+// of four cudaMalloc'd ones.  Layout of the array (4 MiB):
+//   keys[kNaTable] u32 | vals[kNaTable] f32 | x[kNaMaxK] f32 | y[kNaMaxK] f32
+// Nothing in it must start at zero: the table is written once at set-up and
+// every x / y element a call reads is written earlier in the same call.
+namespace {
+constexpr uint64_t kNaMaxK = FS_NOALLOC_MAX_K;  // values per call
+constexpr uint32_t kNaTable = 1u << 18;         // exception entries (glibc expf has 140,931)
+constexpr size_t kNaBytes = (size_t)kNaTable * 8 + (size_t)kNaMaxK * 8;
+static __device__ __align__(256) unsigned char g_na_scratch[kNaBytes];
+
+constexpr int kNaDevices = 64;
+struct NaDevice {
+  bool ready;
+  uint32_t nk;
+  unsigned char *base;  // device address of g_na_scratch on this device
+};
+NaDevice g_na[kNaDevices];
+std::mutex g_na_mu;
+uint32_t g_na_keys[kNaTable];  // host staging of the table at set-up
+float g_na_vals[kNaTable];
+
+// One-time set-up on the current device `dev` (g_na_mu held): resolve the
+// scratch address and upload the expf exception table.
+int na_setup(int dev) {
+  fs_handle *h = nullptr;
+  unsigned char *base = nullptr;
+  CK(cudaGetSymbolAddress((void **)&base, g_na_scratch));
+  const std::string path = lib_dir() + "/expf_glibc.bin";
+  FILE *f = std::fopen(path.c_str(), "rb");
+  if (!f) return set_err(nullptr, FS_ERR_IO, "fs_debug_expf_noalloc: missing expf table " + path);
+  uint32_t magic = 0, n = 0;
+  bool ok = std::fread(&magic, 4, 1, f) == 1 && std::fread(&n, 4, 1, f) == 1 && magic == 0x46534554u &&
+            n <= kNaTable && std::fread(g_na_keys, 4, n, f) == n && std::fread(g_na_vals, 4, n, f) == n;
+  std::fclose(f);
+  if (!ok) return set_err(nullptr, FS_ERR_IO, "fs_debug_expf_noalloc: unreadable expf table " + path);
+  cudaStream_t st = cudaStreamPerThread;
+  CK(cudaMemcpyAsync(base, g_na_keys, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(base + (size_t)kNaTable * 4, g_na_vals, (size_t)n * 4, cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
+  g_na[dev].base = base;
+  g_na[dev].nk = n;
+  g_na[dev].ready = true;
+  return FS_OK;
+}
+}  // namespace
+
+extern "C" int fs_debug_expf_noalloc(const float *x, float *y, uint64_t k) {
+  fs_handle *h = nullptr;
+  if (k > kNaMaxK)
+    return set_err(nullptr, FS_ERR_ARG,
+                   "fs_debug_expf_noalloc: k = " + std::to_string(k) + " exceeds the fixed scratch of " +
+                       std::to_string(kNaMaxK) + " values per call; split the input or use fs_debug_expf");
+  if (k && (!x || !y)) return set_err(nullptr, FS_ERR_ARG, "fs_debug_expf_noalloc: null x or y");
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNaDevices) return set_err(nullptr, FS_ERR_ARG, "fs_debug_expf_noalloc: device ordinal >= 64");
+  NaDevice s;
+  {
+    std::lock_guard<std::mutex> lock(g_na_mu);
+    if (!g_na[dev].ready) {
+      const int rc = na_setup(dev);
+      if (rc) return rc;
+    }
+    s = g_na[dev];
+  }
+  if (k == 0) return FS_OK;
+  const uint32_t *dk = (const uint32_t *)s.base;
+  const float *dv = (const float *)(s.base + (size_t)kNaTable * 4);
+  float *dx = (float *)(s.base + (size_t)kNaTable * 8);
+  float *dy = dx + kNaMaxK;
+  cudaStream_t st = cudaStreamPerThread;
+  CK(cudaMemcpyAsync(dx, x, k * 4, cudaMemcpyHostToDevice, st));
+  CK(fsd::expf_ref_eval(dx, dy, k, dk, dv, s.nk, st));
+  CK(cudaMemcpyAsync(y, dy, k * 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return FS_OK;
+}

@@ -235,6 +235,21 @@ int fs_kernel_time(fs_handle *h, double *ms_per_launch, uint64_t *launches);
 /* Evaluates the device's glibc-exact float exp (the NMDA Mg-block exp of
  * FS_MODE_COMPAT) on k host values, for checks against the host libm. */
 int fs_debug_expf(const float *x, float *y, uint64_t k);
+/* Allocation-free variant of fs_debug_expf; no counterpart in the reference.
+ * For callers that must not allocate device memory per call: a process whose
+ * caching allocator already holds the device's free memory, or a host thread
+ * checking expf while a long fs_run is in flight (fs_debug_expf's cudaFree
+ * waits for the work in flight on the device).  Same kernel and results as
+ * fs_debug_expf, staged through one fixed 4 MiB static device array, so at
+ * most FS_NOALLOC_MAX_K values per call; a larger k returns FS_ERR_ARG.
+ * The first call on each device does a one-time set-up (scratch address
+ * lookup, upload of the expf exception table): make it before any stream
+ * capture begins.  All calls on one device share the scratch: overlapping
+ * calls (several host threads at once) race, so serialise them.  Nothing in
+ * the scratch has to start at zero.  Runs on the calling thread's default
+ * stream (cudaStreamPerThread) and returns when y is written. */
+#define FS_NOALLOC_MAX_K 262144u
+int fs_debug_expf_noalloc(const float *x, float *y, uint64_t k);
 /* Copy state out (V, Count, NState) for checks; arrays of length n. */
 int fs_get_state(fs_handle *h, float *V, int32_t *Count, uint32_t *NState);
 /* Full conductance view for checks: RVs (FS_NREC*n) after the last step and
