@@ -1,0 +1,131 @@
+"""Step-by-step float64 restatement of the production modes' semantics for
+small networks (test infrastructure only; nothing in the product imports it).
+
+Neuron model as the reference: exponential-Euler VmEul with the NMDA Mg
+block, the dV clamp and the firing state machine (code/EqsGnl2.cpp:152-251).
+Synapses as the production engine defines them:
+
+* linear receptors: the gate of a presynaptic neuron obeys st <- st + inc on
+  a spike and st <- st*df otherwise (code/EqsGnl2.cpp:866-917), so a spike at
+  step t adds w*(inc + st(t-1)*(1-df)) to the post's conductance, which
+  arrives in step t + 1 + delay and then decays by the post's df each step;
+* NMDA: per-presynaptic x/s kinetics (code/EqsGnl2.cpp:493), the post reads
+  w * s_pre(t - 1 - delay) in step t;
+* Tsodyks-Markram facilitation/depression per presynaptic neuron (u, x kept
+  in float32 between steps): on a spike u <- u + U(1-u), inc = u*x,
+  x <- x - inc; otherwise u relaxes to U with tau_fac and x to 1 with tau_rec.
+
+Only networks without external drive and with noiseless injection are
+covered (every input is then deterministic).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+AMPA, GABA, ACH, GCL, NMDA = range(5)
+ACT_INJ, ACT_NMDA = 128, 4
+NS_FIRE, NS_SPIKE = 1, 2
+
+
+def simulate(na, steps: int):
+    """Returns (spikes: list of index arrays per step, V: [steps, n] float64)."""
+    f, s = na.fields, na.syn
+    n = na.n
+    assert not np.any(f["pb"]), "external drive is random: not covered"
+    assert not np.any(f["inj_std"]), "injection noise is random: not covered"
+    get = lambda k: np.asarray(f[k], np.float64)  # noqa: E731
+    vrev = get("Vrev").reshape(5, n)
+    dfs = get("dfst").reshape(5, n)
+    vth, vreset, df, ef, dvm, cm = get("Vth"), get("Vreset"), get("df"), get("ef"), get("dVmax"), get("Cm")
+    leak = get("gl") * get("El") * 1e3
+    mg = get("nmda_mg")
+    rf = np.asarray(f["RfPed"], np.int64)
+    sd = np.asarray(f["SpiDy"], np.int64)
+    act = np.asarray(f["act"], np.int64)
+    inj = np.where(act & ACT_INJ, get("inj_mean"), 0.0)
+    pre = np.asarray(s["pre"], np.int64)
+    post = np.asarray(s["post"], np.int64)
+    rec = np.asarray(s["rec"], np.int64)
+    w = np.asarray(s["g"], np.float64)
+    dl = np.asarray(s["delay"], np.int64) if s.get("delay") is not None else np.zeros(pre.size, np.int64)
+    # presynaptic kinetics: the decay of a neuron's gate is its targets' df
+    pdf = np.zeros((4, n))
+    pdfxt, pdfst, pefas = np.zeros(n), np.zeros(n), np.zeros(n)
+    for e in range(pre.size):
+        a, b, r = pre[e], post[e], rec[e]
+        if r != NMDA:
+            pdf[r, a] = dfs[r, b]
+        else:
+            pdfxt[a] = f["nmda_dfxt"][b]
+            pdfst[a] = dfs[NMDA, b]
+            pefas[a] = np.float64(np.float32(f["nmda_efst"][b] * f["nmda_as"][b]))
+    tm = na.tm
+    tm_on = np.zeros(n, bool)
+    if tm is not None:
+        tm_on = np.asarray(tm["enabled"], bool)
+        U = np.broadcast_to(np.asarray(tm.get("U", 0.2), np.float32), (n,)).astype(np.float64)
+        dfr = np.exp(-np.float32(na.dt) / np.broadcast_to(np.asarray(tm.get("tau_rec", 200.0), np.float32), (n,)))
+        dff = np.exp(-np.float32(na.dt) / np.broadcast_to(np.asarray(tm.get("tau_fac", 600.0), np.float32), (n,)))
+        dfr, dff = dfr.astype(np.float32).astype(np.float64), dff.astype(np.float32).astype(np.float64)
+        tu = U.astype(np.float32)
+        tx = np.ones(n, np.float32)
+    dmax = int(dl.max()) if dl.size else 0
+    arrive = np.zeros((steps + dmax + 2, 4, n))
+    s_hist = np.zeros((steps + 1, n))
+    V = np.full(n, -70.0)
+    cnt = np.zeros(n, np.int64)
+    ns = np.zeros(n, np.int64)
+    G = np.zeros((4, n))
+    sp = np.zeros((4, n))
+    xp = np.zeros(n)
+    spre = np.zeros(n)
+    nm = rec == NMDA
+    spikes, Vout = [], np.zeros((steps, n))
+    for t in range(steps):
+        if t >= 1:
+            G = dfs[:4] * G + arrive[t - 1]
+        g = np.zeros((5, n))
+        g[:4] = G
+        idx = t - 1 - dl[nm]
+        sh = np.where(idx >= 0, s_hist[np.maximum(idx, 0), pre[nm]], 0.0)
+        g[NMDA] = np.bincount(post[nm], w[nm] * sh, n)
+        fire_now = (ns & NS_FIRE) != 0
+        v = V.copy()
+        Ir = g * (vrev - v)
+        Ir[NMDA] = g[NMDA] * (vrev[NMDA] - v) / (1.0 + mg * np.exp(-0.062 * v) / 3.57)
+        I = Ir.sum(0) + inj * 1e3 + leak
+        I = 1e-3 * I / cm
+        I = np.clip(I, -dvm, dvm)
+        Vi = df * v + ef * I
+        crossed = ~fire_now & (Vi > vth)
+        V = np.where(fire_now, V, Vi)
+        ns = np.where(crossed, ns | NS_FIRE, ns)
+        fire = fire_now | crossed
+        ref = fire & (cnt < rf)
+        V = np.where(ref, np.where(cnt == 0, 0.0, vreset), V)
+        ns = np.where(ref, np.where(cnt == sd, ns | NS_SPIKE, ns & ~NS_SPIKE), ns)
+        done = fire & ~ref
+        cnt = np.where(ref, cnt + 1, np.where(done, 0, cnt))
+        ns = np.where(done, ns & ~NS_FIRE, ns)
+        Vout[t] = V
+        spk = (ns & NS_SPIKE) != 0
+        spikes.append(np.nonzero(spk)[0].astype(np.uint32))
+        inc = np.ones(n)
+        if tm is not None:
+            u, x = tu.astype(np.float64), tx.astype(np.float64)
+            u_s = u + U * (1.0 - u)
+            rel = u_s * x
+            u_n = U + (u - U) * dff
+            x_n = 1.0 + (x - 1.0) * dfr
+            inc = np.where(tm_on & spk, rel, 1.0)
+            tu = np.where(tm_on, np.where(spk, u_s, u_n), u).astype(np.float32)
+            tx = np.where(tm_on, np.where(spk, x - rel, x_n), x).astype(np.float32)
+        cinc = inc + sp * (1.0 - pdf)
+        sp = np.where(spk, sp + inc, sp * pdf)
+        xp = np.where(spk, xp + inc, xp * pdfxt)
+        spre = pdfst * spre + pefas * xp * (1.0 - spre)
+        s_hist[t] = spre
+        if spk.any():
+            for e in np.nonzero(spk[pre] & ~nm)[0]:
+                arrive[t + dl[e], rec[e], post[e]] += w[e] * cinc[rec[e], pre[e]]
+    return spikes, Vout

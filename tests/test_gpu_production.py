@@ -1,0 +1,197 @@
+"""Production modes (FS_MODE_FP32 / FS_MODE_FP64) on the GPU.
+
+1. Semantics: small deterministic networks (a neuron driven by noiseless
+   injection projects through AMPA, GABA and NMDA synapses with delays of
+   0-255 steps, with and without Tsodyks-Markram plasticity) against the
+   float64 step-by-step restatement in tests/prod_model.py: identical spike
+   steps, membrane potentials within 1e-4 mV (FP64) / 2e-3 mV (FP32).
+2. FP32 against FP64 on the 20,000-neuron connectome network (58 regions,
+   delays 1-5 ms, 10 s): identical raster over the first 50 ms, E and I
+   population rates within 2 %, mean ISI CV within 5 %; the same on the
+   two-population E/I network (800/200); and production FP32 against the
+   reference-order compat path (whose random streams differ) within 2 % /
+   5 % on that network.
+3. Invariants: results do not depend on how the steps are split into calls,
+   on the number of resident blocks, or on repeated runs.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import prod_model
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_net(fb, delays_lin, delays_gaba, delays_nmda, tm=False, dt=0.1):
+    from flysim_b200 import network
+    k_lin, k_gaba, k_nmda = len(delays_lin), len(delays_gaba), len(delays_nmda)
+    n = 1 + k_lin + k_gaba + k_nmda + 1  # driver, targets, one unconnected control
+    f = network.neuron_fields(n, dt, receptors={
+        fb.FS_AMPA: dict(Tau=2.0, Vrev=0.0, FExt=0.0),
+        fb.FS_GABA: dict(Tau=5.0, Vrev=-80.0, FExt=0.0),
+        fb.FS_NMDA: dict(Tau=100.0, TauXT=2.0, Vrev=0.0, FExt=0.0),
+    })
+    f["act"][0] |= fb.ACT["INJ"]
+    f["inj_mean"][0] = 0.8  # fires at about 100 Hz
+    post = np.arange(1, n - 1, dtype=np.uint32)
+    rec = np.array([fb.FS_AMPA] * k_lin + [fb.FS_GABA] * k_gaba + [fb.FS_NMDA] * k_nmda, np.uint8)
+    g = np.array([6.0] * k_lin + [9.0] * k_gaba + [3.0] * k_nmda, np.float32)
+    d = np.array(list(delays_lin) + list(delays_gaba) + list(delays_nmda), np.uint16)
+    pre = np.zeros(post.size, np.uint32)
+    tmd = dict(enabled=(np.arange(n) == 0).astype(np.uint8), U=0.2, tau_rec=200.0, tau_fac=600.0) if tm else None
+    return network.desc_from_arrays(n, dt, f, pre, post, rec, g, d, tm=tmd)
+
+
+SMALL = {
+    "dmin0": ((0, 7, 23), (3,), (0, 13)),
+    "dmin10": ((10, 17, 49, 255), (12,), (10, 31)),
+}
+
+
+@pytest.mark.parametrize("mode,tol", [("fp64", 1e-4), ("fp32", 2e-3)])
+@pytest.mark.parametrize("tm", [False, True])
+@pytest.mark.parametrize("shape", sorted(SMALL))
+def test_small_network_matches_restatement(built, shape, tm, mode, tol):
+    na = _small_net(built, *SMALL[shape], tm=tm)
+    steps = 3000
+    ref_sp, ref_V = prod_model.simulate(na, steps)
+    e = built.Engine(na.desc, mode)
+    try:
+        e.reset(1)
+        sp, V = e.step(steps, want_V=True)
+    finally:
+        e.close()
+    assert sum(x.size for x in ref_sp) > 20
+    for t in range(steps):
+        np.testing.assert_array_equal(sp[t], ref_sp[t], err_msg="spikes differ at step %d" % t)
+    err = np.abs(V.astype(np.float64) - ref_V)
+    assert err.max() < tol, "max |dV| %.3g mV at step %d neuron %d" % (
+        err.max(), *np.unravel_index(err.argmax(), err.shape))
+    # every target felt its input, no earlier than its delay allows
+    first_spike = next(t for t in range(steps) if ref_sp[t].size)
+    moved = np.abs(ref_V - ref_V[:, -1:]) > 1e-9
+    dl = np.asarray(na.syn["delay"], np.int64)
+    for j, d in enumerate(dl):
+        tj = int(np.argmax(moved[:, j + 1]))
+        assert moved[:, j + 1].any() and tj >= first_spike + 1 + d
+
+
+def test_delay_above_ring_limit_is_rejected(built):
+    na = _small_net(built, (256,), (), ())
+    with pytest.raises(built.FsError, match="255"):
+        built.Engine(na.desc, "fp32")
+
+
+def _raster(e, steps, cap=20_000_000):
+    sp, _ = e.step(steps, spike_cap=cap)
+    t = np.concatenate([np.full(a.size, i, np.int64) for i, a in enumerate(sp)])
+    k = np.concatenate(sp).astype(np.int64)
+    return sp, t, k
+
+
+def _isi_cv(t, k, n, min_isi=4):
+    o = np.lexsort((t, k))
+    t, k = t[o], k[o]
+    same = k[1:] == k[:-1]
+    d = np.diff(t)[same].astype(np.float64)
+    kk = k[1:][same]
+    cnt = np.bincount(kk, minlength=n)
+    s1, s2 = np.bincount(kk, d, n), np.bincount(kk, d * d, n)
+    ok = cnt >= min_isi
+    m = s1 / np.maximum(cnt, 1)
+    v = s2 / np.maximum(cnt, 1) - m * m
+    return np.where(ok, np.sqrt(np.maximum(v, 0)) / np.maximum(m, 1e-12), np.nan)
+
+
+def _pop_stats(t, k, groups, n, seconds):
+    ng = int(groups.max()) + 1
+    rate = np.bincount(groups[k], minlength=ng) / np.bincount(groups, minlength=ng) / seconds
+    cv = _isi_cv(t, k, n)
+    mcv = np.array([np.nanmean(cv[groups == g]) for g in range(ng)])
+    return rate, mcv
+
+
+def _compare_modes(fb, desc, n, groups, steps, a, b, dt=0.1, same_stream=True):
+    runs = {}
+    for m in (a, b):
+        e = fb.Engine(desc, m, chunk_steps=10000)
+        try:
+            e.reset(1)
+            runs[m] = _raster(e, steps)
+        finally:
+            e.close()
+    seconds = steps * dt * 1e-3
+    ra, ca = _pop_stats(runs[a][1], runs[a][2], groups, n, seconds)
+    rb, cb = _pop_stats(runs[b][1], runs[b][2], groups, n, seconds)
+    first = next((i for i, (x, y) in enumerate(zip(runs[a][0], runs[b][0])) if not np.array_equal(x, y)), steps)
+    return first, np.abs(ra / rb - 1), np.abs(ca / cb - 1), rb
+
+
+def test_fp32_vs_fp64_connectome_20k(built):
+    from flysim_b200 import netgen, network
+    c = netgen.connectome(n=20000, regions=58, seed=1)
+    na = network.connectome_net(c)
+    groups = np.where(c.excit, 0, 1).astype(np.int64)
+    first, dr, dcv, rates = _compare_modes(built, na.desc, na.n, groups, 100000, "fp32", "fp64")
+    assert first >= 500, "rasters differ at step %d (< 50 ms)" % first
+    assert np.all(rates > 1.0)
+    assert dr.max() < 0.02, dr
+    assert dcv.max() < 0.05, dcv
+
+
+def test_two_population_fp32_vs_fp64_and_compat(built):
+    m = built.Model(os.path.join(GOLDEN, "two_pop", "net.conf"), os.path.join(GOLDEN, "two_pop", "net.pro"))
+    desc = m.desc()
+    groups = np.r_[np.zeros(800, np.int64), np.ones(200, np.int64)]
+    first, dr, dcv, rates = _compare_modes(built, desc, 1000, groups, 100000, "fp32", "fp64")
+    assert first >= 500, "rasters differ at step %d (< 50 ms)" % first
+    assert np.all(rates > 5.0)
+    assert dr.max() < 0.02 and dcv.max() < 0.05, (dr, dcv)
+    # production against the reference-order path (independent random streams)
+    _, dr, dcv, _ = _compare_modes(built, desc, 1000, groups, 100000, "fp32", "compat")
+    assert dr.max() < 0.02 and dcv.max() < 0.05, (dr, dcv)
+
+
+def _conn_net(n=2000, seed=3):
+    from flysim_b200 import netgen, network
+    c = netgen.connectome(n=n, regions=max(2, n // 345), seed=seed)
+    return network.connectome_net(c)
+
+
+def test_results_do_not_depend_on_call_split_or_blocks(built):
+    na = _conn_net()
+    steps = 3000
+    ref = None
+    for bps, splits in ((0, [steps]), (1, [1, 7, 100, 892, 2000]), (2, [1500, 1500])):
+        e = built.Engine(na.desc, "fp32", chunk_steps=256, blocks_per_sm=bps)
+        try:
+            e.reset(5)
+            sp = []
+            for k in splits:
+                sp += e.step(k)[0]
+        finally:
+            e.close()
+        if ref is None:
+            ref = sp
+            assert sum(x.size for x in sp) > 100
+        else:
+            assert all(np.array_equal(x, y) for x, y in zip(ref, sp)), "blocks/SM %d, splits %s" % (bps, splits)
+
+
+def test_seed_and_key_change_the_drive(built):
+    na = _conn_net()
+    out = []
+    for seed, key in ((5, 0), (6, 0), (5, 99)):
+        e = built.Engine(na.desc, "fp32", philox_key=key)
+        try:
+            e.reset(seed)
+            out.append(e.step(500)[0])
+        finally:
+            e.close()
+    same = lambda a, b: all(np.array_equal(x, y) for x, y in zip(a, b))  # noqa: E731
+    assert not same(out[0], out[1]) and not same(out[0], out[2])
