@@ -124,9 +124,10 @@ def algorithmic_bytes(na, spikes: int, steps: int, avg_lin_out: float) -> float:
     return steps * per_step + spikes * (4 + avg_lin_out * 16)
 
 
-def cpu_baseline_port(c, samples: int = 200):
+def cpu_baseline_port(c, samples: int = 2000):
     """The oracle (CPU restatement of the reference step, one thread) on the
-    same network with delays 0, through the .conf route; bounded sample."""
+    same network with delays 0, through the .conf route; bounded sample of
+    2,000 timesteps (about 10 s of CPU work)."""
     import ctypes as C
     import flysim_b200 as fb
     from flysim_b200 import netgen
