@@ -94,6 +94,11 @@ class ModelOpts(C.Structure):
                 ("out_rate", C.c_char_p)]
 
 
+class BatchPlan(C.Structure):
+    _fields_ = [("blocks", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("candidates", C.c_uint32),
+                ("cost_update", C.c_float), ("sample_ms", C.c_double)]
+
+
 class EngineVtbl(C.Structure):
     _fields_ = [("reset", C.c_void_p), ("set_drive", C.c_void_p), ("set_act", C.c_void_p),
                 ("set_injection", C.c_void_p), ("step", C.c_void_p), ("error", C.c_void_p)]
@@ -141,6 +146,16 @@ def lib() -> C.CDLL:
         "fs_model_run_with": (C.c_int, [vp, C.POINTER(EngineVtbl), vp, C.c_char_p, C.c_uint32,
                                         C.POINTER(C.c_double)]),
         "fs_device_engine": (C.POINTER(EngineVtbl), []),
+        "fs_spike_counts": (C.c_int, [vp, _u32]),
+        "fs_batch_create": (C.c_int, [C.c_uint32, C.POINTER(C.POINTER(NetDesc)), C.POINTER(RunOpts), C.POINTER(vp)]),
+        "fs_batch_destroy": (C.c_int, [vp]),
+        "fs_batch_error": (C.c_char_p, [vp]),
+        "fs_batch_reset": (C.c_int, [vp, _u32]),
+        "fs_batch_tune": (C.c_int, [vp, C.c_uint32, C.POINTER(BatchPlan)]),
+        "fs_batch_run": (C.c_int, [vp, C.c_uint32, C.POINTER(C.c_double)]),
+        "fs_batch_info": (C.c_int, [vp, _u32, _u32, _u32, C.POINTER(C.c_int), C.POINTER(C.c_uint64)]),
+        "fs_batch_spike_counts": (C.c_int, [vp, C.c_uint32, _u32]),
+        "fs_batch_spike_totals": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -158,7 +173,9 @@ def exported_symbols() -> Sequence[str]:
                         "fs_get_state",
                         "fs_get_syn_state", "fs_model_load", "fs_model_free", "fs_model_error",
                         "fs_model_desc", "fs_model_info", "fs_model_seed", "fs_model_run",
-                        "fs_model_run_with", "fs_device_engine")]
+                        "fs_model_run_with", "fs_device_engine", "fs_spike_counts", "fs_batch_create",
+                        "fs_batch_destroy", "fs_batch_error", "fs_batch_reset", "fs_batch_tune", "fs_batch_run",
+                        "fs_batch_info", "fs_batch_spike_counts", "fs_batch_spike_totals")]
 
 
 def _check(rc: int, h=None):
@@ -331,6 +348,12 @@ class Engine:
         _check(lib().fs_kernel_time(self._h, C.byref(ms), C.byref(n)), self._h)
         return ms.value, n.value
 
+    def spike_counts(self) -> np.ndarray:
+        """Per-neuron spike counts since the last reset (production modes)."""
+        c = np.zeros(self.n, np.uint32)
+        _check(lib().fs_spike_counts(self._h, c.ctypes.data_as(_u32)), self._h)
+        return c
+
     def state(self):
         V = np.zeros(self.n, np.float32)
         cnt = np.zeros(self.n, np.int32)
@@ -355,6 +378,76 @@ def debug_expf(x: np.ndarray) -> np.ndarray:
     y = np.zeros_like(x)
     _check(lib().fs_debug_expf(x.ctypes.data_as(_f), y.ctypes.data_as(_f), x.size))
     return y
+
+
+class Batch:
+    """Independent production networks advanced by one persistent launch
+    (fs_batch_*): the generalisation of the reference's -rp repeat loop to
+    instances of different size, parameters and seed."""
+
+    def __init__(self, descs, mode: str = "fp32", device: int = 0, chunk_steps: int = 0, philox_key: int = 0,
+                 blocks_per_sm: int = 0):
+        L = lib()
+        self._keep = [getattr(d, "_keep", None) for d in descs]
+        self._descs = [d if isinstance(d, C._Pointer) else C.pointer(d) for d in descs]
+        arr = (C.POINTER(NetDesc) * len(descs))(*self._descs)
+        o = RunOpts(MODES[mode], device, chunk_steps, philox_key, blocks_per_sm)
+        h = C.c_void_p()
+        rc = L.fs_batch_create(len(descs), arr, C.byref(o), C.byref(h))
+        if rc != FS_OK:
+            raise FsError(rc, (L.fs_batch_error(None) or b"").decode(errors="replace"))
+        self._h = h
+        self.count = len(descs)
+        self.n = [int(d.contents.neurons.n) for d in self._descs]
+
+    def _ok(self, rc):
+        if rc != FS_OK:
+            raise FsError(rc, (lib().fs_batch_error(self._h) or b"").decode(errors="replace"))
+
+    def reset(self, seeds=None):
+        if seeds is None:
+            self._ok(lib().fs_batch_reset(self._h, None))
+        else:
+            s = np.ascontiguousarray(seeds, np.uint32)
+            assert s.size == self.count
+            self._ok(lib().fs_batch_reset(self._h, s.ctypes.data_as(_u32)))
+
+    def tune(self, sample_steps: int = 200) -> dict:
+        p = BatchPlan()
+        self._ok(lib().fs_batch_tune(self._h, sample_steps, C.byref(p)))
+        return dict(blocks=p.blocks, blocks_per_sm=p.blocks_per_sm, candidates=p.candidates,
+                    cost_update=p.cost_update, sample_ms=p.sample_ms)
+
+    def run(self, nsteps: int) -> float:
+        ms = C.c_double()
+        self._ok(lib().fs_batch_run(self._h, nsteps, C.byref(ms)))
+        return ms.value
+
+    def info(self) -> dict:
+        a, b, c, g, l_ = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_int(), C.c_uint64()
+        self._ok(lib().fs_batch_info(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(g), C.byref(l_)))
+        return dict(count=a.value, blocks=b.value, blocks_per_sm=c.value, graph=bool(g.value), launches=l_.value)
+
+    def spike_counts(self, i: int) -> np.ndarray:
+        c = np.zeros(self.n[i], np.uint32)
+        self._ok(lib().fs_batch_spike_counts(self._h, i, c.ctypes.data_as(_u32)))
+        return c
+
+    def spike_totals(self) -> np.ndarray:
+        t = np.zeros(self.count, np.uint64)
+        self._ok(lib().fs_batch_spike_totals(self._h, t.ctypes.data_as(C.POINTER(C.c_uint64))))
+        return t
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fs_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 NOALLOC_MAX_K = 262144  # FS_NOALLOC_MAX_K

@@ -776,3 +776,139 @@ extern "C" int fs_debug_expf_noalloc(const float *x, float *y, uint64_t k) {
   CK(cudaStreamSynchronize(st));
   return FS_OK;
 }
+
+// ---- batches of independent production networks -----------------------------
+struct fs_batch {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  fsp::Batch *b = nullptr;
+  fsp::BatchPlan tuned{};
+  std::string err;
+};
+
+namespace {
+int batch_err(fs_batch *b, int code, const std::string &msg) {
+  if (b) b->err = msg;
+  g_err = msg;
+  return code;
+}
+}  // namespace
+
+extern "C" {
+
+int fs_batch_create(uint32_t count, const fs_net_desc *const *descs, const fs_run_opts *opts, fs_batch **out) {
+  if (!out) return set_err(nullptr, FS_ERR_ARG, "fs_batch_create: out is NULL");
+  *out = nullptr;
+  fs_run_opts o{};
+  if (opts) o = *opts;
+  if (o.mode == FS_MODE_COMPAT) o.mode = FS_MODE_FP32;
+  if (o.mode != FS_MODE_FP32 && o.mode != FS_MODE_FP64)
+    return set_err(nullptr, FS_ERR_ARG, "fs_batch_create: batches run FS_MODE_FP32 or FS_MODE_FP64");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_err(nullptr, FS_ERR_NODEVICE, "fs_batch_create: no CUDA device visible");
+  if (o.device < 0 || o.device >= ndev) return set_err(nullptr, FS_ERR_ARG, "fs_batch_create: bad device ordinal");
+  for (uint32_t i = 0; i < count; i++)
+    if (!descs || !descs[i] || !descs[i]->syn || descs[i]->neurons.n == 0)
+      return set_err(nullptr, FS_ERR_ARG, "fs_batch_create: instance " + std::to_string(i) + " has no synapse list");
+  fs_batch *b = new fs_batch();
+  b->device = o.device;
+  cudaError_t e = cudaSetDevice(o.device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    const int rc = set_err(nullptr, FS_ERR_CUDA, std::string("fs_batch_create: ") + cudaGetErrorString(e));
+    delete b;
+    return rc;
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, o.device);
+  std::string err;
+  int rc = fsp::batch_create(&b->b, count, descs, o, (uint32_t)sms, b->st, err);
+  if (rc) {
+    set_err(nullptr, rc, "fs_batch_create: " + err);
+    cudaStreamDestroy(b->st);
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return FS_OK;
+}
+
+int fs_batch_destroy(fs_batch *b) {
+  if (!b) return FS_OK;
+  cudaSetDevice(b->device);
+  if (b->st) cudaStreamSynchronize(b->st);
+  fsp::batch_destroy(b->b);
+  if (b->st) cudaStreamDestroy(b->st);
+  delete b;
+  return FS_OK;
+}
+
+const char *fs_batch_error(const fs_batch *b) { return b ? b->err.c_str() : g_err.c_str(); }
+
+int fs_batch_reset(fs_batch *b, const uint32_t *seeds) {
+  if (!b) return set_err(nullptr, FS_ERR_ARG, "fs_batch_reset: null batch");
+  cudaSetDevice(b->device);
+  int rc = fsp::batch_reset(b->b, seeds, b->st, b->err);
+  return rc ? batch_err(b, rc, b->err) : FS_OK;
+}
+
+int fs_batch_tune(fs_batch *b, uint32_t sample_steps, fs_batch_plan *plan) {
+  if (!b) return set_err(nullptr, FS_ERR_ARG, "fs_batch_tune: null batch");
+  cudaSetDevice(b->device);
+  fsp::BatchPlan p{};
+  int rc = fsp::batch_tune(b->b, sample_steps, b->st, &p, b->err);
+  if (rc) return batch_err(b, rc, b->err);
+  if (plan) {
+    plan->blocks = p.blocks;
+    plan->blocks_per_sm = p.blocks_per_sm;
+    plan->candidates = p.candidates;
+    plan->cost_update = (float)p.cost_update;
+    plan->sample_ms = p.sample_ms;
+  }
+  return FS_OK;
+}
+
+int fs_batch_run(fs_batch *b, uint32_t nsteps, double *device_ms) {
+  if (!b) return set_err(nullptr, FS_ERR_ARG, "fs_batch_run: null batch");
+  cudaSetDevice(b->device);
+  int rc = fsp::batch_run(b->b, nsteps, b->st, device_ms, b->err);
+  return rc ? batch_err(b, rc, b->err) : FS_OK;
+}
+
+int fs_batch_info(fs_batch *b, uint32_t *count, uint32_t *blocks, uint32_t *blocks_per_sm, int *graph,
+                  uint64_t *launches) {
+  if (!b) return set_err(nullptr, FS_ERR_ARG, "fs_batch_info: null batch");
+  fsp::BatchPlan p{};
+  fsp::batch_info(b->b, &p);
+  if (count) *count = fsp::batch_size(b->b);
+  if (blocks) *blocks = p.blocks;
+  if (blocks_per_sm) *blocks_per_sm = p.blocks_per_sm;
+  if (graph) *graph = p.graph;
+  if (launches) *launches = p.launches;
+  return FS_OK;
+}
+
+int fs_batch_spike_counts(fs_batch *b, uint32_t inst, uint32_t *counts) {
+  if (!b || !counts) return set_err(nullptr, FS_ERR_ARG, "fs_batch_spike_counts: null argument");
+  cudaSetDevice(b->device);
+  int rc = fsp::batch_spike_counts(b->b, inst, counts, b->st, b->err);
+  return rc ? batch_err(b, rc, b->err) : FS_OK;
+}
+
+int fs_batch_spike_totals(fs_batch *b, uint64_t *totals) {
+  if (!b || !totals) return set_err(nullptr, FS_ERR_ARG, "fs_batch_spike_totals: null argument");
+  cudaSetDevice(b->device);
+  int rc = fsp::batch_spike_totals(b->b, totals, b->st, b->err);
+  return rc ? batch_err(b, rc, b->err) : FS_OK;
+}
+
+int fs_spike_counts(fs_handle *h, uint32_t *counts) {
+  if (!h || !counts) return set_err(nullptr, FS_ERR_ARG, "fs_spike_counts: null argument");
+  if (h->mode == FS_MODE_COMPAT) return set_err(h, FS_ERR_UNSUPPORTED, "fs_spike_counts: production modes only");
+  cudaSetDevice(h->device);
+  int rc = fsp::prod_spike_counts(h->prod, counts, h->st, h->err);
+  return rc ? set_err(h, rc, h->err) : FS_OK;
+}
+
+}  // extern "C"

@@ -95,6 +95,7 @@ struct Params {
   unsigned int *bar;
   int *err;
   unsigned long long *spike_total;  // spikes since reset
+  uint32_t *nspk;                   // per-neuron spike counts since reset (or null)
 };
 
 // ---- Philox-4x32-10 -------------------------------------------------------
@@ -112,18 +113,21 @@ __device__ __forceinline__ void philox(uint32_t c[4], uint32_t k0, uint32_t k1) 
 __device__ __forceinline__ float u24(uint32_t x) { return (float)(x >> 8) * 5.9604644775390625e-08f; }
 
 // ---- bounded grid barrier ---------------------------------------------------
-// bar[0] counts arrivals, bar[32] (its own 128-byte line) is the generation
-// the waiting blocks poll; the last block to arrive resets the count and
-// advances the generation.  Every wait is bounded: after ~2^24 polls the
-// block sets the error word and all blocks leave.
-__device__ __forceinline__ bool grid_sync(unsigned int *bar, int *err) {
+// Over the `count` blocks that share `bar` (the whole grid, or the blocks of
+// one network instance in a batch).  bar[0] counts arrivals, bar[32] (its
+// own 128-byte line) is the generation the waiting blocks poll; the last
+// block to arrive resets the count and advances the generation.  Every wait
+// is bounded: after ~2^24 polls the block sets the error word and all
+// blocks leave.
+__device__ __forceinline__ bool grid_sync(unsigned int *bar, int *err, uint32_t count) {
   __syncthreads();
+  if (count <= 1) return *(volatile int *)err == 0;
   if (threadIdx.x == 0) {
     volatile unsigned int *gen = bar + 32;
     const unsigned int g = *gen;
     __threadfence();
     const unsigned int arrived = atomicAdd(bar, 1u);
-    if (arrived == gridDim.x - 1) {
+    if (arrived == count - 1) {
       atomicExch(bar, 0u);
       __threadfence();
       atomicAdd((unsigned int *)gen, 1u);
@@ -143,12 +147,18 @@ __device__ __forceinline__ bool grid_sync(unsigned int *bar, int *err) {
   return *(volatile int *)err == 0;
 }
 
+// Loads of the NMDA s history may be served by L1 (ld.global.ca): a block
+// reads only slots written in earlier intervals, and every interval ends
+// with the grid barrier above, whose fences (release before the arrival,
+// acquire after the wait, then bar.sync) order those writes before the
+// reads in the PTX memory model; the vector windows of one edge and the
+// edges of different posts that share a presynaptic neuron then hit L1.
 template <class T>
-__device__ __forceinline__ T ldcg_t(const T *p);
+__device__ __forceinline__ T ldhist_t(const T *p);
 template <>
-__device__ __forceinline__ float ldcg_t<float>(const float *p) { return __ldcg(p); }
+__device__ __forceinline__ float ldhist_t<float>(const float *p) { return __ldca(p); }
 template <>
-__device__ __forceinline__ double ldcg_t<double>(const double *p) { return __ldcg(p); }
+__device__ __forceinline__ double ldhist_t<double>(const double *p) { return __ldca(p); }
 
 template <class T>
 __device__ __forceinline__ T exp_t(T x);
@@ -210,7 +220,7 @@ __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint
           const uint32_t i0 = a >> 2;
 #pragma unroll
           for (int i = 0; i < NV; i++)
-            v[u][i] = (ok && (uint32_t)i < nvl) ? __ldcg(row + ((i0 + i) & qmask)) : make_float4(0.f, 0.f, 0.f, 0.f);
+            v[u][i] = (ok && (uint32_t)i < nvl) ? __ldca(row + ((i0 + i) & qmask)) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
 #pragma unroll
         for (int u = 0; u < U; u++) {
@@ -251,7 +261,7 @@ __device__ __forceinline__ void nmda_pull(const Params &P, uint32_t p0, uint32_t
         const uint32_t a = (uint32_t)(tb - 1u - d) & mask;
 #pragma unroll
         for (uint32_t j = 0; j < kLB; j++)
-          if (j < L) acc[j] += w * ldcg_t<T>(row + ((a + j) & mask));
+          if (j < L) acc[j] += w * ldhist_t<T>(row + ((a + j) & mask));
       }
     }
 #pragma unroll
@@ -381,6 +391,7 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
     sp[r] = ((T *)P.st_pre)[(size_t)r * n + p];
   }
   T ex = ((T *)P.ext_x)[p], es = ((T *)P.ext_s)[p], xp = ((T *)P.x_pre)[p], spre = ((T *)P.s_pre)[p];
+  uint32_t nsp = 0;
   // ring slot of the first step
   long long rv[4];
   {
@@ -474,6 +485,7 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
     }
     if (own && P.outV) P.outV[(size_t)s * n + p] = (float)V;
     spk = own && (ns & FS_NS_SPIKE) != 0;
+    nsp += spk ? 1u : 0u;
     // presynaptic state: increment per spike, then plasticity update
     if (pj && own) {
       T inc = (T)1;
@@ -543,7 +555,7 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
     if (m) {
       if (spk && P.bits) atomicOr(P.bits + (size_t)s * P.words + (p >> 5), 1u << (p & 31));
       if (lane == 0) {
-        atomicAdd(P.counts + s, (unsigned)__popc(m));
+        if (P.counts) atomicAdd(P.counts + s, (unsigned)__popc(m));
         atomicAdd(P.spike_total, (unsigned long long)__popc(m));
       }
       bool listed = false;
@@ -583,11 +595,14 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
     ((T *)P.ext_s)[p] = es;
     ((T *)P.x_pre)[p] = xp;
     ((T *)P.s_pre)[p] = spre;
+    if (P.nspk && nsp) P.nspk[p] += nsp;
   }
 }
 
+// The steps of one block: posts [B0, B1) of the network P, whose blocks
+// (nblk of them) meet at a barrier after every interval.
 template <class T>
-__global__ void __launch_bounds__(kThreads) k_prod(const __grid_constant__ Params P) {
+__device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32_t B1, uint32_t nblk) {
   // FP64 tiles are half as wide so the per-tile buffers stay in static
   // shared memory
   constexpr uint32_t kT = TileW<T>::W;
@@ -600,7 +615,6 @@ __global__ void __launch_bounds__(kThreads) k_prod(const __grid_constant__ Param
   __shared__ T l_c[kCap][4];
   const SpikeList<T> lst{&l_n, l_p, l_tm, l_c, kCap};
   const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  const uint32_t B0 = P.block_post[blockIdx.x], B1 = P.block_post[blockIdx.x + 1];
   if (tid == 0) l_n = 0;
   __syncthreads();
   uint32_t s = 0;
@@ -617,13 +631,13 @@ __global__ void __launch_bounds__(kThreads) k_prod(const __grid_constant__ Param
         // warps without neurons in this tile skip the steps
         if ((tid & ~31u) < np) neuron_steps<T>(P, tp0, np, bs, L, gn, hits, gauss, lst);
         __syncthreads();
-        // the batch's spikes, pushed by the whole block
+        // the batch's spikes: one spike per warp, eight in flight per block
         const uint32_t nl = min(l_n, kCap);
-        for (uint32_t k = 0; k < nl; k++) {
+        for (uint32_t k = wid; k < nl; k += kThreads / 32) {
           T cj[4];
 #pragma unroll
           for (int r = 0; r < 4; r++) cj[r] = l_c[k][r];
-          push_spike<T>(P, l_p[k], l_tm[k], cj, tid, kThreads);
+          push_spike<T>(P, l_p[k], l_tm[k], cj, lane, 32);
         }
         __syncthreads();
         if (tid == 0) l_n = 0;
@@ -631,9 +645,42 @@ __global__ void __launch_bounds__(kThreads) k_prod(const __grid_constant__ Param
     }
     s = iv_end;
     if (s < P.nsteps) {
-      if (!grid_sync(P.bar, P.err)) return;
+      if (!grid_sync(P.bar, P.err, nblk)) return;
     }
   }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_prod(const __grid_constant__ Params P) {
+  prod_blocks<T>(P, P.block_post[blockIdx.x], P.block_post[blockIdx.x + 1], gridDim.x);
+}
+
+// ---- batch: many independent networks in one persistent launch -----------
+// Block b works on instance blk[b].inst, posts [b0, b1), and meets only the
+// other blocks of that instance (blk[b].nblk of them) at its barriers, so
+// instances of different sizes and intervals advance independently.
+struct BatchBlock {
+  uint32_t inst, b0, b1, nblk;
+};
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_prod_batch(const Params *__restrict__ Ps,
+                                                         const BatchBlock *__restrict__ blk) {
+  __shared__ __align__(16) Params Psh;
+  const BatchBlock me = blk[blockIdx.x];
+  {
+    const uint32_t *src = (const uint32_t *)(Ps + me.inst);
+    uint32_t *dst = (uint32_t *)&Psh;
+    for (uint32_t i = threadIdx.x; i < sizeof(Params) / 4; i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  prod_blocks<T>(Psh, me.b0, me.b1, me.nblk);
+}
+
+// Advances every instance's step counter after a batch launch (graph node).
+__global__ void k_batch_advance(Params *Ps, uint32_t count, uint32_t nsteps) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) Ps[i].t0 += nsteps;
 }
 
 // ---- host side -------------------------------------------------------------
@@ -660,6 +707,7 @@ struct Prod {
   uint64_t kl = 0;
   uint64_t key = 0;
   std::vector<uint32_t> host_counts;
+  std::vector<uint32_t> in_row_h;  // NMDA in-degree prefix (block partitioning)
 };
 
 namespace {
@@ -903,6 +951,7 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
     for (; b < blocks; b++) block_post[b] = n;
   }
   p->chunks = blocks;
+  p->in_row_h = in_row;
   // ---- device arrays ----
   int rc = 0;
   const size_t T = p->fp64 ? 8 : 4;
@@ -954,6 +1003,7 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
       (rc = dup(p, &P.D, (const float *)nullptr, n, st, err)) || (rc = dup(p, &P.F, (const float *)nullptr, n, st, err)) ||
       (rc = dup(p, &P.Cap, (const float *)nullptr, n, st, err)) || (rc = dup(p, &P.Car, (const float *)nullptr, n, st, err)) ||
       (rc = dup(p, &P.tm_u, (const float *)nullptr, n, st, err)) || (rc = dup(p, &P.tm_x, (const float *)nullptr, n, st, err)) ||
+      (rc = dup(p, &P.nspk, (const uint32_t *)nullptr, n, st, err)) ||
       (rc = dup(p, &P.ring, (const unsigned long long *)nullptr, (size_t)std::max<uint32_t>(1, p->nlin) * P.slots * n, st, err)))
     goto fail;
   // edges
@@ -1029,7 +1079,7 @@ int prod_reset(Prod *p, uint32_t seed, cudaStream_t st, std::string &err) {
   };
   z(P.G, 4 * n * T); z(P.ext_st, 4 * n * T); z(P.ext_x, n * T); z(P.ext_s, n * T);
   z(P.st_pre, 4 * n * T); z(P.x_pre, n * T); z(P.s_pre, n * T); z(P.s_hist, (size_t)P.slots * n * T * (p->fp64 ? 1 : kSH));
-  z(P.Count, n * 4); z(P.NS, n * 4); z(P.Cap, n * 4); z(P.Car, n * 4);
+  z(P.Count, n * 4); z(P.NS, n * 4); z(P.Cap, n * 4); z(P.Car, n * 4); z(P.nspk, n * 4);
   z(P.ring, (size_t)std::max<uint32_t>(1, p->nlin) * P.slots * n * 8);
   z(p->err, 4);
   z(p->spike_total, 8);
@@ -1158,5 +1208,408 @@ void prod_info(const Prod *p, ProdInfo *info) {
   info->lin_receptors = p->nlin;
   info->fp64 = p->fp64 ? 1 : 0;
 }
+
+
+int prod_spike_counts(Prod *p, uint32_t *counts, cudaStream_t st, std::string &err) {
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaMemcpy(counts, p->P.nspk, (size_t)p->n * 4, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    err = cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  return FS_OK;
+}
+
+// ---- batch of independent networks ------------------------------------------
+struct Batch {
+  bool fp64 = false;
+  uint32_t sm = 148, occ = 1;
+  std::vector<Prod *> inst;
+  std::vector<uint32_t> seeds;
+  Params *dP = nullptr;          // [count] parameters as the kernel reads them
+  BatchBlock *dB = nullptr;      // [blocks]
+  uint32_t dB_cap = 0;
+  unsigned int *bars = nullptr;  // [count][64]
+  int *errs = nullptr;           // [count]
+  uint32_t blocks = 0, per_sm = 0;
+  double upd = 24.0;
+  uint32_t chunk = 10000;
+  uint32_t dev_nsteps = 0;       // nsteps the device parameter array holds (0: stale)
+  cudaGraphExec_t exec = nullptr;
+  uint32_t graph_steps = 0;
+  bool graph_ok = true;          // capture works for this launch
+  bool graph_used = false;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  double ms = 0.0;
+  uint64_t launches = 0;
+};
+
+namespace {
+
+template <class X>
+cudaError_t bal(X **p, size_t count) {
+  return cudaMalloc((void **)p, count * sizeof(X));
+}
+
+// cost-balanced split of an instance's posts into k contiguous ranges
+void split_posts(const Prod *p, uint32_t k, double upd, std::vector<uint32_t> &bp) {
+  const uint32_t n = p->n;
+  bp.assign(k + 1, n);
+  bp[0] = 0;
+  const std::vector<uint32_t> &in = p->in_row_h;
+  const double total = (double)p->nmda_edges + upd * n;
+  double acc = 0;
+  uint32_t b = 1;
+  for (uint32_t q = 0; q < n && b < k; q++) {
+    acc += upd + (double)(in[q + 1] - in[q]);
+    while (b < k && acc >= total * b / k) bp[b++] = q + 1;
+  }
+  for (; b < k; b++) bp[b] = n;
+}
+
+int batch_plan(Batch *B, uint32_t per_sm, double upd, std::string &err) {
+  const uint32_t count = (uint32_t)B->inst.size();
+  const uint32_t total = B->sm * per_sm;
+  if (count > total) {
+    err = "batch of " + std::to_string(count) + " instances exceeds the " + std::to_string(total) +
+          " co-resident blocks of one launch";
+    return FS_ERR_CAPACITY;
+  }
+  std::vector<double> c(count);
+  double sum = 0;
+  for (uint32_t i = 0; i < count; i++) sum += (c[i] = upd * B->inst[i]->n + (double)B->inst[i]->nmda_edges);
+  // one block each, the rest by cost (largest remainder), at most n/8 blocks
+  std::vector<uint32_t> k(count, 1);
+  std::vector<std::pair<double, uint32_t>> rem;
+  uint32_t used = count;
+  for (uint32_t i = 0; i < count; i++) {
+    const double want = (double)(total - count) * c[i] / sum;
+    const uint32_t cap = std::max<uint32_t>(1, (B->inst[i]->n + 7) / 8);
+    const uint32_t add = std::min<uint32_t>((uint32_t)want, cap - 1);
+    k[i] += add;
+    used += add;
+    rem.push_back({want - (double)add, i});
+  }
+  std::sort(rem.begin(), rem.end(), [](const std::pair<double, uint32_t> &a, const std::pair<double, uint32_t> &b) {
+    return a.first > b.first || (a.first == b.first && a.second < b.second);
+  });
+  for (size_t r = 0; r < rem.size() && used < total; r++) {
+    const uint32_t i = rem[r].second;
+    if (k[i] < std::max<uint32_t>(1, (B->inst[i]->n + 7) / 8)) { k[i]++; used++; }
+  }
+  std::vector<BatchBlock> plan;
+  std::vector<uint32_t> bp;
+  for (uint32_t i = 0; i < count; i++) {
+    split_posts(B->inst[i], k[i], upd, bp);
+    for (uint32_t j = 0; j < k[i]; j++) plan.push_back(BatchBlock{i, bp[j], bp[j + 1], k[i]});
+  }
+  if (plan.size() > B->dB_cap) {
+    if (B->dB) cudaFree(B->dB);
+    B->dB = nullptr;
+    B->dB_cap = 0;
+    cudaError_t e = bal(&B->dB, plan.size());
+    if (e != cudaSuccess) {
+      err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+      return FS_ERR_NOMEM;
+    }
+    B->dB_cap = (uint32_t)plan.size();
+  }
+  cudaError_t e = cudaMemcpy(B->dB, plan.data(), plan.size() * sizeof(BatchBlock), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    err = std::string("plan upload: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  B->blocks = (uint32_t)plan.size();
+  B->per_sm = per_sm;
+  B->upd = upd;
+  if (B->exec) cudaGraphExecDestroy(B->exec);
+  B->exec = nullptr;
+  B->graph_steps = 0;
+  return FS_OK;
+}
+
+int batch_upload(Batch *B, uint32_t nsteps, cudaStream_t st, std::string &err) {
+  const uint32_t count = (uint32_t)B->inst.size();
+  std::vector<Params> hp(count);
+  for (uint32_t i = 0; i < count; i++) {
+    Params P = B->inst[i]->P;
+    P.t0 = B->inst[i]->t;
+    P.nsteps = nsteps;
+    P.bits = nullptr;
+    P.counts = nullptr;
+    P.outV = nullptr;
+    P.bar = B->bars + 64 * (size_t)i;
+    P.err = B->errs + i;
+    P.spike_total = B->inst[i]->spike_total;
+    hp[i] = P;
+  }
+  cudaError_t e = cudaMemcpyAsync(B->dP, hp.data(), count * sizeof(Params), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("batch parameter upload: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  B->dev_nsteps = nsteps;
+  return FS_OK;
+}
+
+cudaError_t batch_enqueue(Batch *B, uint32_t nsteps, cudaStream_t st) {
+  void *args[] = {&B->dP, &B->dB};
+  cudaError_t e = B->fp64 ? cudaLaunchCooperativeKernel((void *)k_prod_batch<double>, B->blocks, kThreads, args, 0, st)
+                          : cudaLaunchCooperativeKernel((void *)k_prod_batch<float>, B->blocks, kThreads, args, 0, st);
+  if (e != cudaSuccess) return e;
+  const uint32_t count = (uint32_t)B->inst.size();
+  k_batch_advance<<<(count + 255) / 256, 256, 0, st>>>(B->dP, count, nsteps);
+  return cudaGetLastError();
+}
+
+// one launch of nsteps for every instance: a replay of the captured graph
+// when one exists for this step count, else a direct launch
+int batch_launch(Batch *B, uint32_t nsteps, cudaStream_t st, std::string &err) {
+  int rc;
+  if (B->dev_nsteps != nsteps && (rc = batch_upload(B, nsteps, st, err))) return rc;
+  cudaError_t e = cudaSuccess;
+  if (B->graph_ok && B->graph_steps != nsteps) {
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    B->exec = nullptr;
+    B->graph_steps = 0;
+    cudaGraph_t g = nullptr;
+    e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      cudaError_t le = batch_enqueue(B, nsteps, st);
+      e = cudaStreamEndCapture(st, &g);
+      if (le != cudaSuccess) e = le;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&B->exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e == cudaSuccess) {
+      B->graph_steps = nsteps;
+    } else {
+      // this launch form cannot be captured here: launch it directly
+      cudaGetLastError();
+      B->graph_ok = false;
+      if (B->exec) cudaGraphExecDestroy(B->exec);
+      B->exec = nullptr;
+    }
+  }
+  if (B->exec && B->graph_steps == nsteps) {
+    e = cudaGraphLaunch(B->exec, st);
+    B->graph_used = true;
+  } else {
+    e = batch_enqueue(B, nsteps, st);
+  }
+  if (e != cudaSuccess) {
+    err = std::string("batch launch: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  for (Prod *p : B->inst) p->t += nsteps;
+  B->launches++;
+  return FS_OK;
+}
+
+int batch_check(Batch *B, cudaStream_t st, std::string &err) {
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("batch kernel: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  std::vector<int> h(B->inst.size());
+  e = cudaMemcpy(h.data(), B->errs, h.size() * 4, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    err = std::string("error words: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  for (size_t i = 0; i < h.size(); i++)
+    if (h[i]) {
+      err = "instance " + std::to_string(i) + ": barrier wait gave up (device error word set)";
+      return FS_ERR_TIMEOUT;
+    }
+  return FS_OK;
+}
+
+}  // namespace
+
+void batch_destroy(Batch *B) {
+  if (!B) return;
+  for (Prod *p : B->inst) prod_destroy(p);
+  if (B->exec) cudaGraphExecDestroy(B->exec);
+  if (B->dP) cudaFree(B->dP);
+  if (B->dB) cudaFree(B->dB);
+  if (B->bars) cudaFree(B->bars);
+  if (B->errs) cudaFree(B->errs);
+  if (B->e0) cudaEventDestroy(B->e0);
+  if (B->e1) cudaEventDestroy(B->e1);
+  delete B;
+}
+
+int batch_create(Batch **out, uint32_t count, const fs_net_desc *const *descs, const fs_run_opts &o,
+                 uint32_t sm_count, cudaStream_t st, std::string &err) {
+  *out = nullptr;
+  if (!count || !descs) {
+    err = "batch: no instances";
+    return FS_ERR_ARG;
+  }
+  Batch *B = new Batch();
+  B->fp64 = (o.mode == FS_MODE_FP64);
+  B->sm = sm_count;
+  B->chunk = o.chunk_steps ? o.chunk_steps : 10000;
+  int rc = FS_OK;
+  for (uint32_t i = 0; i < count && rc == FS_OK; i++) {
+    Prod *p = nullptr;
+    if (!descs[i]) {
+      err = "batch: null network description " + std::to_string(i);
+      rc = FS_ERR_ARG;
+      break;
+    }
+    rc = prod_create(&p, descs[i], o, sm_count, st, err);
+    if (rc) err = "instance " + std::to_string(i) + ": " + err;
+    else B->inst.push_back(p);
+  }
+  int occ = 0;
+  if (rc == FS_OK) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &occ, B->fp64 ? (const void *)k_prod_batch<double> : (const void *)k_prod_batch<float>, kThreads, 0);
+    B->occ = (uint32_t)std::max(1, occ);
+    cudaError_t e = bal(&B->dP, count);
+    if (e == cudaSuccess) e = bal(&B->bars, (size_t)count * 64);
+    if (e == cudaSuccess) e = bal(&B->errs, count);
+    if (e == cudaSuccess) e = cudaMemset(B->bars, 0, (size_t)count * 64 * 4);
+    if (e == cudaSuccess) e = cudaMemset(B->errs, 0, (size_t)count * 4);
+    if (e == cudaSuccess) e = cudaEventCreate(&B->e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&B->e1);
+    if (e != cudaSuccess) {
+      err = std::string("batch buffers: ") + cudaGetErrorString(e);
+      rc = FS_ERR_NOMEM;
+    }
+  }
+  if (rc == FS_OK) {
+    uint32_t per_sm = std::min<uint32_t>(B->occ, 2);
+    if (o.blocks_per_sm) per_sm = std::min<uint32_t>(B->occ, o.blocks_per_sm);
+    while (per_sm < B->occ && B->sm * per_sm < count) per_sm++;
+    rc = batch_plan(B, per_sm, 24.0, err);
+  }
+  if (rc) {
+    batch_destroy(B);
+    return rc;
+  }
+  B->seeds.assign(count, 1);
+  *out = B;
+  return FS_OK;
+}
+
+int batch_reset(Batch *B, const uint32_t *seeds, cudaStream_t st, std::string &err) {
+  for (size_t i = 0; i < B->inst.size(); i++) {
+    const uint32_t s = seeds ? seeds[i] : B->seeds[i];
+    B->seeds[i] = s;
+    int rc = prod_reset(B->inst[i], s, st, err);
+    if (rc) {
+      err = "instance " + std::to_string(i) + ": " + err;
+      return rc;
+    }
+  }
+  cudaError_t e = cudaMemsetAsync(B->bars, 0, B->inst.size() * 64 * 4, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(B->errs, 0, B->inst.size() * 4, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("batch reset: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  B->dev_nsteps = 0;
+  B->ms = 0.0;
+  return FS_OK;
+}
+
+int batch_run(Batch *B, uint32_t nsteps, cudaStream_t st, double *device_ms, std::string &err) {
+  cudaEventRecord(B->e0, st);
+  uint32_t done = 0;
+  while (done < nsteps) {
+    const uint32_t k = std::min(B->chunk, nsteps - done);
+    int rc = batch_launch(B, k, st, err);
+    if (rc) return rc;
+    done += k;
+  }
+  cudaEventRecord(B->e1, st);
+  int rc = batch_check(B, st, err);
+  if (rc) return rc;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, B->e0, B->e1);
+  B->ms += ms;
+  if (device_ms) *device_ms = ms;
+  return FS_OK;
+}
+
+int batch_tune(Batch *B, uint32_t sample_steps, cudaStream_t st, BatchPlan *out, std::string &err) {
+  if (!sample_steps) sample_steps = 200;
+  double best = -1.0;
+  uint32_t best_ps = B->per_sm;
+  double best_upd = B->upd;
+  const double upds[3] = {8.0, 24.0, 64.0};
+  uint32_t tried = 0;
+  for (uint32_t ps = 1; ps <= std::min<uint32_t>(B->occ, 4); ps++) {
+    if (B->sm * ps < B->inst.size()) continue;
+    for (double u : upds) {
+      int rc = batch_plan(B, ps, u, err);
+      if (rc) return rc;
+      if ((rc = batch_reset(B, nullptr, st, err))) return rc;
+      double ms = 0;
+      if ((rc = batch_run(B, sample_steps, st, nullptr, err))) return rc;   // warm-up (graph capture)
+      if ((rc = batch_run(B, sample_steps, st, &ms, err))) return rc;
+      tried++;
+      if (best < 0 || ms < best) {
+        best = ms;
+        best_ps = ps;
+        best_upd = u;
+      }
+    }
+  }
+  int rc = batch_plan(B, best_ps, best_upd, err);
+  if (rc == FS_OK) rc = batch_reset(B, nullptr, st, err);
+  if (rc) return rc;
+  B->ms = 0.0;
+  if (out) {
+    out->blocks = B->blocks;
+    out->blocks_per_sm = B->per_sm;
+    out->cost_update = best_upd;
+    out->sample_ms = best;
+    out->candidates = tried;
+  }
+  return FS_OK;
+}
+
+void batch_info(const Batch *B, BatchPlan *out) {
+  out->blocks = B->blocks;
+  out->blocks_per_sm = B->per_sm;
+  out->cost_update = B->upd;
+  out->sample_ms = 0.0;
+  out->candidates = 0;
+  out->graph = B->graph_used ? 1 : 0;
+  out->launches = B->launches;
+  out->total_ms = B->ms;
+}
+
+int batch_spike_counts(Batch *B, uint32_t i, uint32_t *counts, cudaStream_t st, std::string &err) {
+  if (i >= B->inst.size()) {
+    err = "batch: instance index out of range";
+    return FS_ERR_ARG;
+  }
+  return prod_spike_counts(B->inst[i], counts, st, err);
+}
+
+int batch_spike_totals(Batch *B, uint64_t *totals, cudaStream_t st, std::string &err) {
+  cudaError_t e = cudaStreamSynchronize(st);
+  for (size_t i = 0; i < B->inst.size() && e == cudaSuccess; i++) {
+    unsigned long long t = 0;
+    e = cudaMemcpy(&t, B->inst[i]->spike_total, 8, cudaMemcpyDeviceToHost);
+    totals[i] = t;
+  }
+  if (e != cudaSuccess) {
+    err = cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  return FS_OK;
+}
+
+uint32_t batch_size(const Batch *B) { return (uint32_t)B->inst.size(); }
+uint32_t batch_neurons(const Batch *B, uint32_t i) { return i < B->inst.size() ? B->inst[i]->n : 0; }
 
 }  // namespace fsp

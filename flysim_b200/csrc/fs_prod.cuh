@@ -30,5 +30,27 @@ struct ProdInfo {
   int fp64;
 };
 void prod_info(const Prod *p, ProdInfo *info);
+int prod_spike_counts(Prod *p, uint32_t *counts, cudaStream_t st, std::string &err);
+
+// Batch: independent production networks advanced by one persistent launch.
+struct Batch;
+struct BatchPlan {
+  uint32_t blocks, blocks_per_sm, candidates;
+  double cost_update, sample_ms;
+  int graph;
+  uint64_t launches;
+  double total_ms;
+};
+int batch_create(Batch **out, uint32_t count, const fs_net_desc *const *descs, const fs_run_opts &o,
+                 uint32_t sm_count, cudaStream_t st, std::string &err);
+void batch_destroy(Batch *b);
+int batch_reset(Batch *b, const uint32_t *seeds, cudaStream_t st, std::string &err);
+int batch_run(Batch *b, uint32_t nsteps, cudaStream_t st, double *device_ms, std::string &err);
+int batch_tune(Batch *b, uint32_t sample_steps, cudaStream_t st, BatchPlan *out, std::string &err);
+void batch_info(const Batch *b, BatchPlan *out);
+int batch_spike_counts(Batch *b, uint32_t inst, uint32_t *counts, cudaStream_t st, std::string &err);
+int batch_spike_totals(Batch *b, uint64_t *totals, cudaStream_t st, std::string &err);
+uint32_t batch_size(const Batch *b);
+uint32_t batch_neurons(const Batch *b, uint32_t inst);
 
 }  // namespace fsp

@@ -298,6 +298,49 @@ int fs_model_run_with(fs_model *m, const fs_engine_vtbl *eng, void *ctx, const c
 /* The device engine's table (ctx = fs_handle*). */
 const fs_engine_vtbl *fs_device_engine(void);
 
+/* Per-neuron spike counts since the last fs_reset (production modes; n
+ * entries).  The per-population rates of a FiringRate output are sums of
+ * these (code/NetSimGnl2_info.cpp:660-700). */
+int fs_spike_counts(fs_handle *h, uint32_t *counts);
+
+/* ---- batches: many independent networks in one persistent launch -------
+ * The generalisation of the reference's repeat loop (-rp, code/main.cpp:
+ * 251-252) to instances that differ in size, parameters and seed, as the
+ * seizure-like E/I-gain scans need.  Every instance is a production-mode
+ * network (FP32 or FP64) with its own state; one cooperative launch advances
+ * all of them, each instance's blocks meeting only at its own barriers, and
+ * the launch is captured once into a CUDA graph and replayed per chunk of
+ * steps.  An instance's results are identical to running it alone with
+ * fs_create / fs_run (same seed and philox_key). */
+typedef struct fs_batch fs_batch;
+typedef struct fs_batch_plan {
+  uint32_t blocks;        /* thread blocks of the launch                     */
+  uint32_t blocks_per_sm; /* resident blocks per SM                          */
+  uint32_t candidates;    /* configurations the tuner timed                  */
+  float cost_update;      /* per-neuron cost weight of the block partition,
+                             in units of one NMDA in-edge                   */
+  double sample_ms;       /* device time of the chosen plan's sample run     */
+} fs_batch_plan;
+/* opts: mode FS_MODE_FP32 (default) or FS_MODE_FP64, device, chunk_steps
+ * (steps per graph replay, default 10000), philox_key, blocks_per_sm. */
+int fs_batch_create(uint32_t count, const fs_net_desc *const *descs, const fs_run_opts *opts, fs_batch **out);
+int fs_batch_destroy(fs_batch *b);
+const char *fs_batch_error(const fs_batch *b); /* b may be NULL */
+/* seeds: one per instance (NULL = the previous seeds, initially 1). */
+int fs_batch_reset(fs_batch *b, const uint32_t *seeds);
+/* Autotuner: times sample_steps (0 = 200) for each candidate block plan
+ * (blocks per SM x partition cost weight), keeps the fastest and resets
+ * every instance (its seed unchanged).  Results never depend on the plan. */
+int fs_batch_tune(fs_batch *b, uint32_t sample_steps, fs_batch_plan *plan);
+/* Advances every instance by nsteps; device_ms = device time of the call. */
+int fs_batch_run(fs_batch *b, uint32_t nsteps, double *device_ms);
+int fs_batch_info(fs_batch *b, uint32_t *count, uint32_t *blocks, uint32_t *blocks_per_sm, int *graph,
+                  uint64_t *launches);
+/* Per-neuron spike counts of instance inst since its reset. */
+int fs_batch_spike_counts(fs_batch *b, uint32_t inst, uint32_t *counts);
+/* Total spikes of every instance since its reset (count entries). */
+int fs_batch_spike_totals(fs_batch *b, uint64_t *totals);
+
 #ifdef __cplusplus
 }
 #endif
