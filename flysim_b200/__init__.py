@@ -156,6 +156,18 @@ def lib() -> C.CDLL:
         "fs_batch_info": (C.c_int, [vp, _u32, _u32, _u32, C.POINTER(C.c_int), C.POINTER(C.c_uint64)]),
         "fs_batch_spike_counts": (C.c_int, [vp, C.c_uint32, _u32]),
         "fs_batch_spike_totals": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
+        "fs_mlp_error": (C.c_char_p, []),
+        "fs_mlp_create": (C.c_int, [_u32, C.c_uint32, C.c_int, C.c_uint64, C.POINTER(vp)]),
+        "fs_mlp_destroy": (C.c_int, [vp]),
+        "fs_mlp_param_count": (C.c_uint64, [vp]),
+        "fs_mlp_get_params": (C.c_int, [vp, _f]),
+        "fs_mlp_set_params": (C.c_int, [vp, _f]),
+        "fs_mlp_forward": (C.c_int, [vp, _f, C.c_uint64, _f, C.POINTER(C.c_double)]),
+        "fs_mlp_grad": (C.c_int, [vp, _f, _f, C.c_uint32, _f, _f]),
+        "fs_mlp_train": (C.c_int, [vp, _f, _f, C.c_uint64, C.c_uint32, C.c_float, C.c_uint64, _f,
+                                   C.POINTER(C.c_double)]),
+        "fs_mlp_gemm": (C.c_int, [C.POINTER(C.c_uint16), C.POINTER(C.c_uint16), C.c_uint32, C.c_uint32, C.c_uint32,
+                                  _f, C.c_int, _f]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -175,7 +187,9 @@ def exported_symbols() -> Sequence[str]:
                         "fs_model_desc", "fs_model_info", "fs_model_seed", "fs_model_run",
                         "fs_model_run_with", "fs_device_engine", "fs_spike_counts", "fs_batch_create",
                         "fs_batch_destroy", "fs_batch_error", "fs_batch_reset", "fs_batch_tune", "fs_batch_run",
-                        "fs_batch_info", "fs_batch_spike_counts", "fs_batch_spike_totals")]
+                        "fs_batch_info", "fs_batch_spike_counts", "fs_batch_spike_totals", "fs_mlp_error",
+                        "fs_mlp_create", "fs_mlp_destroy", "fs_mlp_param_count", "fs_mlp_get_params",
+                        "fs_mlp_set_params", "fs_mlp_forward", "fs_mlp_grad", "fs_mlp_train", "fs_mlp_gemm")]
 
 
 def _check(rc: int, h=None):
@@ -448,6 +462,86 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def _mlp_ok(rc):
+    if rc != FS_OK:
+        raise FsError(rc, (lib().fs_mlp_error() or b"").decode(errors="replace"))
+
+
+class Mlp:
+    """The surrogate MLP (fs_mlp_*): BF16 tensor-core training and inference."""
+
+    def __init__(self, dims, device: int = 0, seed: int = 1):
+        d = np.ascontiguousarray(dims, np.uint32)
+        h = C.c_void_p()
+        _mlp_ok(lib().fs_mlp_create(d.ctypes.data_as(_u32), d.size, device, seed, C.byref(h)))
+        self._h = h
+        self.dims = [int(x) for x in dims]
+
+    def param_count(self) -> int:
+        return int(lib().fs_mlp_param_count(self._h))
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.param_count(), np.float32)
+        _mlp_ok(lib().fs_mlp_get_params(self._h, p.ctypes.data_as(_f)))
+        return p
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.param_count()
+        _mlp_ok(lib().fs_mlp_set_params(self._h, p.ctypes.data_as(_f)))
+
+    def forward(self, x: np.ndarray, with_time: bool = False):
+        x = np.ascontiguousarray(x, np.float32)
+        rows = x.shape[0]
+        y = np.zeros((rows, self.dims[-1]), np.float32)
+        ms = C.c_double()
+        _mlp_ok(lib().fs_mlp_forward(self._h, x.ctypes.data_as(_f), rows, y.ctypes.data_as(_f), C.byref(ms)))
+        return (y, ms.value) if with_time else y
+
+    def grad(self, x: np.ndarray, t: np.ndarray):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        g = np.zeros(self.param_count(), np.float32)
+        loss = C.c_float()
+        _mlp_ok(lib().fs_mlp_grad(self._h, x.ctypes.data_as(_f), t.ctypes.data_as(_f), x.shape[0],
+                                  g.ctypes.data_as(_f), C.byref(loss)))
+        return g, loss.value
+
+    def train(self, x: np.ndarray, t: np.ndarray, epochs: int, lr: float = 1e-3, seed: int = 1):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        losses = np.zeros(epochs, np.float32)
+        ms = C.c_double()
+        _mlp_ok(lib().fs_mlp_train(self._h, x.ctypes.data_as(_f), t.ctypes.data_as(_f), x.shape[0], epochs, lr,
+                                   seed, losses.ctypes.data_as(_f), C.byref(ms)))
+        return losses, ms.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fs_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def mlp_gemm(a_bf16: np.ndarray, b_bf16: np.ndarray, bias=None, relu: bool = False) -> np.ndarray:
+    """fs_mlp_gemm: c = a . b^T on the tensor cores (a, b as uint16 BF16 bits)."""
+    a = np.ascontiguousarray(a_bf16, np.uint16)
+    b = np.ascontiguousarray(b_bf16, np.uint16)
+    m, k = a.shape
+    n = b.shape[0]
+    c = np.zeros((m, n), np.float32)
+    bp = None if bias is None else np.ascontiguousarray(bias, np.float32)
+    _mlp_ok(lib().fs_mlp_gemm(a.ctypes.data_as(C.POINTER(C.c_uint16)), b.ctypes.data_as(C.POINTER(C.c_uint16)),
+                              m, n, k, None if bp is None else bp.ctypes.data_as(_f), int(relu),
+                              c.ctypes.data_as(_f)))
+    return c
 
 
 NOALLOC_MAX_K = 262144  # FS_NOALLOC_MAX_K

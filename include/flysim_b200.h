@@ -341,6 +341,36 @@ int fs_batch_spike_counts(fs_batch *b, uint32_t inst, uint32_t *counts);
 /* Total spikes of every instance since its reset (count entries). */
 int fs_batch_spike_totals(fs_batch *b, uint64_t *totals);
 
+/* ---- mean-field surrogate (no counterpart in the reference) -------------
+ * A multilayer perceptron with ReLU hidden layers, BF16 weights and
+ * activations and FP32 accumulation on the tensor cores (tcgen05), trained
+ * with Adam on rates the batched engine produced.  dims = {inputs, hidden...,
+ * outputs}, every width in [1, 256]; the last output is a hyperactivity
+ * logit and the others regress log(1 + rate).  Loss per batch: mean squared
+ * error over the rate outputs plus binary cross-entropy of the logit.
+ * Parameters in the host-side vectors are, per layer, W [out x in]
+ * row-major followed by b [out].  Errors: fs_mlp_error(). */
+typedef struct fs_mlp fs_mlp;
+const char *fs_mlp_error(void);
+int fs_mlp_create(const uint32_t *dims, uint32_t ndims, int device, uint64_t seed, fs_mlp **out);
+int fs_mlp_destroy(fs_mlp *m);
+uint64_t fs_mlp_param_count(const fs_mlp *m);
+int fs_mlp_get_params(fs_mlp *m, float *params);
+int fs_mlp_set_params(fs_mlp *m, const float *params);
+/* y[rows x outputs] = network(x[rows x inputs]); host arrays. */
+int fs_mlp_forward(fs_mlp *m, const float *x, uint64_t rows, float *y, double *device_ms);
+/* Gradients of the loss over one batch (rows a multiple of 16, <= 256),
+ * targets t[rows x outputs]; no update. */
+int fs_mlp_grad(fs_mlp *m, const float *x, const float *t, uint32_t rows, float *grads, float *loss);
+/* Adam, batches of 256 rows in a fresh shuffle per epoch (rows beyond a
+ * multiple of 256 are left out of that epoch); epoch_loss[epochs] or NULL. */
+int fs_mlp_train(fs_mlp *m, const float *x, const float *t, uint64_t rows, uint32_t epochs, float lr,
+                 uint64_t seed, float *epoch_loss, double *device_ms);
+/* One tensor-core GEMM for checks: c[m x n] = a[m x k] . b[n x k]^T (+ bias,
+ * ReLU), a and b BF16 bit patterns, n and k multiples of 16 up to 256. */
+int fs_mlp_gemm(const uint16_t *a, const uint16_t *b, uint32_t m, uint32_t n, uint32_t k, const float *bias,
+                int relu, float *c);
+
 #ifdef __cplusplus
 }
 #endif
