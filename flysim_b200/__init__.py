@@ -156,6 +156,9 @@ def lib() -> C.CDLL:
         "fs_batch_info": (C.c_int, [vp, _u32, _u32, _u32, C.POINTER(C.c_int), C.POINTER(C.c_uint64)]),
         "fs_batch_spike_counts": (C.c_int, [vp, C.c_uint32, _u32]),
         "fs_batch_spike_totals": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
+        "fs_set_gains": (C.c_int, [vp, _f]),
+        "fs_batch_set_gains": (C.c_int, [vp, C.c_uint32, _f]),
+        "fs_batch_set_drive": (C.c_int, [vp, C.c_uint32, _f]),
         "fs_mlp_error": (C.c_char_p, []),
         "fs_mlp_create": (C.c_int, [_u32, C.c_uint32, C.c_int, C.c_uint64, C.POINTER(vp)]),
         "fs_mlp_destroy": (C.c_int, [vp]),
@@ -187,7 +190,8 @@ def exported_symbols() -> Sequence[str]:
                         "fs_model_desc", "fs_model_info", "fs_model_seed", "fs_model_run",
                         "fs_model_run_with", "fs_device_engine", "fs_spike_counts", "fs_batch_create",
                         "fs_batch_destroy", "fs_batch_error", "fs_batch_reset", "fs_batch_tune", "fs_batch_run",
-                        "fs_batch_info", "fs_batch_spike_counts", "fs_batch_spike_totals", "fs_mlp_error",
+                        "fs_batch_info", "fs_batch_spike_counts", "fs_batch_spike_totals", "fs_set_gains",
+                        "fs_batch_set_gains", "fs_batch_set_drive", "fs_mlp_error",
                         "fs_mlp_create", "fs_mlp_destroy", "fs_mlp_param_count", "fs_mlp_get_params",
                         "fs_mlp_set_params", "fs_mlp_forward", "fs_mlp_grad", "fs_mlp_train", "fs_mlp_gemm")]
 
@@ -362,6 +366,12 @@ class Engine:
         _check(lib().fs_kernel_time(self._h, C.byref(ms), C.byref(n)), self._h)
         return ms.value, n.value
 
+    def set_gains(self, gains):
+        """Synaptic gain per receptor (production modes)."""
+        g = np.ascontiguousarray(gains, np.float32)
+        assert g.size == FS_NREC
+        _check(lib().fs_set_gains(self._h, g.ctypes.data_as(_f)), self._h)
+
     def spike_counts(self) -> np.ndarray:
         """Per-neuron spike counts since the last reset (production modes)."""
         c = np.zeros(self.n, np.uint32)
@@ -446,6 +456,17 @@ class Batch:
         c = np.zeros(self.n[i], np.uint32)
         self._ok(lib().fs_batch_spike_counts(self._h, i, c.ctypes.data_as(_u32)))
         return c
+
+    def set_gains(self, i: int, gains):
+        g = np.ascontiguousarray(gains, np.float32)
+        assert g.size == FS_NREC
+        self._ok(lib().fs_batch_set_gains(self._h, i, g.ctypes.data_as(_f)))
+
+    def set_drive(self, i: int, pb: np.ndarray):
+        """Drive probabilities of instance i, pb[FS_NREC * n] (receptor-major)."""
+        p = np.ascontiguousarray(pb, np.float32)
+        assert p.size == FS_NREC * self.n[i]
+        self._ok(lib().fs_batch_set_drive(self._h, i, p.ctypes.data_as(_f)))
 
     def spike_totals(self) -> np.ndarray:
         t = np.zeros(self.count, np.uint64)

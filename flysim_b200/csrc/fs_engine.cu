@@ -903,6 +903,26 @@ int fs_batch_spike_totals(fs_batch *b, uint64_t *totals) {
   return rc ? batch_err(b, rc, b->err) : FS_OK;
 }
 
+int fs_set_gains(fs_handle *h, const float *gains) {
+  if (!h || !gains) return set_err(nullptr, FS_ERR_ARG, "fs_set_gains: null argument");
+  if (h->mode == FS_MODE_COMPAT) return set_err(h, FS_ERR_UNSUPPORTED, "fs_set_gains: production modes only");
+  fsp::prod_set_gains(h->prod, gains);
+  return FS_OK;
+}
+
+int fs_batch_set_gains(fs_batch *b, uint32_t inst, const float *gains) {
+  if (!b || !gains) return set_err(nullptr, FS_ERR_ARG, "fs_batch_set_gains: null argument");
+  int rc = fsp::batch_set_gains(b->b, inst, gains, b->err);
+  return rc ? batch_err(b, rc, b->err) : FS_OK;
+}
+
+int fs_batch_set_drive(fs_batch *b, uint32_t inst, const float *pb) {
+  if (!b || !pb) return set_err(nullptr, FS_ERR_ARG, "fs_batch_set_drive: null argument");
+  cudaSetDevice(b->device);
+  int rc = fsp::batch_set_drive(b->b, inst, pb, b->st, b->err);
+  return rc ? batch_err(b, rc, b->err) : FS_OK;
+}
+
 int fs_spike_counts(fs_handle *h, uint32_t *counts) {
   if (!h || !counts) return set_err(nullptr, FS_ERR_ARG, "fs_spike_counts: null argument");
   if (h->mode == FS_MODE_COMPAT) return set_err(h, FS_ERR_UNSUPPORTED, "fs_spike_counts: production modes only");

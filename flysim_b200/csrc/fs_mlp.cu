@@ -96,9 +96,11 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
+// Grid: x over 128-row tiles, y over column tiles of g.N / gridDim.y columns.
 __global__ void __launch_bounds__(kThreads) k_gemm_tn(const __grid_constant__ GemmArgs g) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  const int K = g.K, N = g.N, nks = K >> 4;
+  const int K = g.K, N = g.N / (int)gridDim.y, nks = K >> 4;
+  const int n0 = blockIdx.y * N;  // first column of this CTA
   uint8_t *sA = smem;                              // nks slabs of 128 rows x 32 B
   uint8_t *sB = smem + (size_t)nks * kTileM * 32;  // nks slabs of N rows x 32 B
   uint64_t *mbar = (uint64_t *)(sB + (size_t)nks * N * 32);
@@ -117,18 +119,41 @@ __global__ void __launch_bounds__(kThreads) k_gemm_tn(const __grid_constant__ Ge
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(mbar)));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
   }
-  // operands -> shared memory; rows past M read as zero
+  // operands -> shared memory, eight 16-byte loads in flight per thread;
+  // rows past M read as zero
   const int kc8 = K >> 3;
-  for (int idx = tid; idx < kTileM * kc8; idx += kThreads) {
-    const int r = idx % kTileM, kc = idx / kTileM;
-    uint4 v = make_uint4(0u, 0u, 0u, 0u);
-    if (m0 + r < g.M) v = *(const uint4 *)(g.A + (size_t)(m0 + r) * g.lda + kc * 8);
-    *(uint4 *)(sA + (kc >> 1) * (kTileM * 32) + (r >> 3) * 256 + (kc & 1) * 128 + (r & 7) * 16) = v;
-  }
-  for (int idx = tid; idx < N * kc8; idx += kThreads) {
-    const int r = idx % N, kc = idx / N;
-    const uint4 v = *(const uint4 *)(g.B + (size_t)r * g.ldb + kc * 8);
-    *(uint4 *)(sB + (size_t)(kc >> 1) * (N * 32) + (r >> 3) * 256 + (kc & 1) * 128 + (r & 7) * 16) = v;
+  {
+    const int na = kTileM * kc8;
+    for (int i0 = tid; i0 < na; i0 += 8 * kThreads) {
+      uint4 v[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int idx = i0 + u * kThreads, r = idx % kTileM, kc = idx / kTileM;
+        v[u] = (idx < na && m0 + r < g.M) ? *(const uint4 *)(g.A + (size_t)(m0 + r) * g.lda + kc * 8)
+                                           : make_uint4(0u, 0u, 0u, 0u);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int idx = i0 + u * kThreads, r = idx % kTileM, kc = idx / kTileM;
+        if (idx < na)
+          *(uint4 *)(sA + (kc >> 1) * (kTileM * 32) + (r >> 3) * 256 + (kc & 1) * 128 + (r & 7) * 16) = v[u];
+      }
+    }
+    const int nb = N * kc8;
+    for (int i0 = tid; i0 < nb; i0 += 8 * kThreads) {
+      uint4 v[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int idx = i0 + u * kThreads, r = idx % N, kc = idx / N;
+        v[u] = idx < nb ? *(const uint4 *)(g.B + (size_t)(n0 + r) * g.ldb + kc * 8) : make_uint4(0u, 0u, 0u, 0u);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int idx = i0 + u * kThreads, r = idx % N, kc = idx / N;
+        if (idx < nb)
+          *(uint4 *)(sB + (size_t)(kc >> 1) * (N * 32) + (r >> 3) * 256 + (kc & 1) * 128 + (r & 7) * 16) = v[u];
+      }
+    }
   }
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   __syncthreads();
@@ -176,7 +201,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm_tn(const __grid_constant__ Ge
       if (!live) continue;
 #pragma unroll
       for (int j = 0; j < 16; j++) {
-        const int c = c0 + j;
+        const int c = n0 + c0 + j;
         float x = __uint_as_float(v[j]);
         if (g.bias) x += g.bias[c];
         if (g.relu) x = fmaxf(x, 0.0f);
@@ -209,7 +234,11 @@ int gemm(const GemmArgs &g, cudaStream_t st, std::string &err) {
     cudaFuncSetAttribute(k_gemm_tn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem(256, 256));
     gemm_attr_set = true;
   }
-  k_gemm_tn<<<(g.M + kTileM - 1) / kTileM, kThreads, gemm_smem(g.N, g.K), st>>>(g);
+  // column tiles of 64 (or all of N when it is not a multiple of 64) so that
+  // small-M GEMMs still spread over several SMs
+  const int ny = (g.N % 64 == 0) ? g.N / 64 : 1;
+  const dim3 grid((g.M + kTileM - 1) / kTileM, ny);
+  k_gemm_tn<<<grid, kThreads, gemm_smem(g.N / ny, g.K), st>>>(g);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     err = std::string("gemm launch: ") + cudaGetErrorString(e);

@@ -96,6 +96,7 @@ struct Params {
   int *err;
   unsigned long long *spike_total;  // spikes since reset
   uint32_t *nspk;                   // per-neuron spike counts since reset (or null)
+  float rg[5];                      // synaptic gain per receptor (scales every weight; 1 = as built)
 };
 
 // ---- Philox-4x32-10 -------------------------------------------------------
@@ -186,50 +187,74 @@ __device__ __forceinline__ float comp4(const float4 &q, int k) {
   return k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w;
 }
 
+// The next post's row bounds and first edge codes are fetched while the
+// current post's history windows are in flight, so a post costs about one
+// L2 round trip; per lane the edges are summed in the same order as a
+// plain walk (chunks of 32 x U edges, lane-strided), so the result does not
+// depend on the prefetching.
 __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint32_t np, uint64_t tb, uint32_t L,
                                               float (*gn)[kTile], uint32_t wid, uint32_t lane) {
   constexpr int U = 4;                 // edges per lane per round
   constexpr int NV = kLB / 4;          // vectors per edge window
+  constexpr uint32_t CH = 32u * U;     // edges per warp round
   const float4 *sh = (const float4 *)P.s_hist;
   const uint32_t S4 = P.slots >> 2, qmask = S4 - 1, mask = P.mask;
   const uint32_t nvl = (L + 3u) >> 2;  // vectors needed for L steps
   const uint32_t nw = kThreads / 32;
-  for (uint32_t q = wid; q < np; q += nw) {
+  uint32_t code[U];
+  float w[U];
+  auto fetch = [&](uint32_t base, uint32_t end) {
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const uint32_t eu = base + lane + 32u * u;
+      code[u] = eu < end ? __ldg(P.in_code + eu) : 0u;
+      w[u] = eu < end ? __ldg(P.in_w + eu) : 0.0f;
+    }
+  };
+  uint32_t q = wid, b0 = 0, b1 = 0;
+  if (P.in_row && q < np) {
+    b0 = __ldg(P.in_row + p0 + q);
+    b1 = __ldg(P.in_row + p0 + q + 1);
+    fetch(b0, b1);
+  }
+  for (; q < np; q += nw) {
+    const uint32_t qn = q + nw;
+    uint32_t n0 = 0, n1 = 0;
+    if (P.in_row && qn < np) {
+      n0 = __ldg(P.in_row + p0 + qn);
+      n1 = __ldg(P.in_row + p0 + qn + 1);
+    }
     float acc[kLB];
 #pragma unroll
     for (uint32_t j = 0; j < kLB; j++) acc[j] = 0.0f;
-    if (P.in_row) {
-      const uint32_t p = p0 + q;
-      const uint32_t e0 = __ldg(P.in_row + p), e1 = __ldg(P.in_row + p + 1);
-      for (uint32_t e = e0 + lane; e < e1; e += 32u * U) {
-        uint32_t code[U];
-        float w[U];
+    const uint32_t nch = (b1 - b0 + CH - 1) / CH;
+    for (uint32_t c = 0; c < nch; c++) {
+      const uint32_t e = b0 + c * CH + lane;
+      float4 v[U][NV];
 #pragma unroll
-        for (int u = 0; u < U; u++) {
-          const uint32_t eu = e + 32u * u;
-          code[u] = eu < e1 ? __ldg(P.in_code + eu) : 0u;
-          w[u] = eu < e1 ? __ldg(P.in_w + eu) : 0.0f;
-        }
-        float4 v[U][NV];
+      for (int u = 0; u < U; u++) {
+        const bool ok = e + 32u * u < b1;
+        const uint32_t pre = code[u] & 0xffffffu, d = code[u] >> 24;
+        const uint32_t a = (uint32_t)(tb - 1u - d) & mask;
+        const float4 *row = sh + ((size_t)pre * kSH + (a & 3u)) * S4;
+        const uint32_t i0 = a >> 2;
 #pragma unroll
-        for (int u = 0; u < U; u++) {
-          const bool ok = e + 32u * u < e1;
-          const uint32_t pre = code[u] & 0xffffffu, d = code[u] >> 24;
-          const uint32_t a = (uint32_t)(tb - 1u - d) & mask;
-          const float4 *row = sh + ((size_t)pre * kSH + (a & 3u)) * S4;
-          const uint32_t i0 = a >> 2;
+        for (int i = 0; i < NV; i++)
+          v[u][i] = (ok && (uint32_t)i < nvl) ? __ldca(row + ((i0 + i) & qmask)) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      float wc[U];
 #pragma unroll
-          for (int i = 0; i < NV; i++)
-            v[u][i] = (ok && (uint32_t)i < nvl) ? __ldca(row + ((i0 + i) & qmask)) : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
+      for (int u = 0; u < U; u++) wc[u] = w[u];
+      if (c + 1 < nch) fetch(b0 + (c + 1) * CH, b1);
+      else if (qn < np) fetch(n0, n1);
 #pragma unroll
-        for (int u = 0; u < U; u++) {
+      for (int u = 0; u < U; u++) {
 #pragma unroll
-          for (int j = 0; j < (int)kLB; j++)
-            if ((uint32_t)j < L) acc[j] += w[u] * comp4(v[u][j >> 2], j & 3);
-        }
+        for (int j = 0; j < (int)kLB; j++)
+          if ((uint32_t)j < L) acc[j] += wc[u] * comp4(v[u][j >> 2], j & 3);
       }
     }
+    if (nch == 0 && qn < np) fetch(n0, n1);
 #pragma unroll
     for (uint32_t j = 0; j < kLB; j++) {
       if (j < L) {
@@ -237,6 +262,8 @@ __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint
         if (lane == j) gn[j][q] = v;
       }
     }
+    b0 = n0;
+    b1 = n1;
   }
 }
 
@@ -296,7 +323,7 @@ __device__ __forceinline__ void push_spike(const Params &P, uint32_t q, uint32_t
     for (int u = 0; u < 4; u++) {
       if (e + u * stride < oe) {
         const uint32_t post = code[u] & 0x3fffffu, r = (code[u] >> 22) & 3u, d = code[u] >> 24;
-        const T cv = (r == 0) ? cj[0] : (r == 1) ? cj[1] : (r == 2) ? cj[2] : cj[3];
+        const T cv = ((r == 0) ? cj[0] : (r == 1) ? cj[1] : (r == 2) ? cj[2] : cj[3]) * (T)P.rg[r];
         const long long fx = __double2ll_rn((double)((T)w[u] * cv) * kFix);
         const int ri = P.lin_of_rec[r];
         atomicAdd(P.ring + ((size_t)ri * n + post) * S + ((tm + d) & mask), (unsigned long long)fx);
@@ -423,7 +450,7 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
       }
     }
     const uint32_t qs = tid < np ? tid : 0;
-    g[FS_NMDA] = gn[j][qs];
+    g[FS_NMDA] = gn[j][qs] * (T)P.rg[FS_NMDA];
     // external drive (BgInit): the Bernoulli outcomes of this step were drawn
     // in the pull phase (bit r: receptor r hit)
     const uint32_t hit = hits[j][qs];
@@ -841,6 +868,7 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
   p->chunk_steps = o.chunk_steps ? o.chunk_steps : 1000;
   Params &P = p->P;
   P.n = n;
+  for (int r = 0; r < 5; r++) P.rg[r] = 1.0f;
   const size_t nr = (size_t)FS_NREC * n;
   const fs_syn_list &S = *d->syn;
   // ---- receptor kinetics seen by each presynaptic neuron ----
@@ -1610,6 +1638,38 @@ int batch_spike_totals(Batch *B, uint64_t *totals, cudaStream_t st, std::string 
 }
 
 uint32_t batch_size(const Batch *B) { return (uint32_t)B->inst.size(); }
+
+void prod_set_gains(Prod *p, const float *g) {
+  for (int r = 0; r < 5; r++) p->P.rg[r] = g[r];
+}
+
+int prod_set_pb(Prod *p, const float *pb, cudaStream_t st, std::string &err) {
+  cudaError_t e = cudaMemcpyAsync((void *)p->P.pb, pb, (size_t)FS_NREC * p->n * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("drive upload: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  return FS_OK;
+}
+
+int batch_set_gains(Batch *B, uint32_t i, const float *g, std::string &err) {
+  if (i >= B->inst.size()) {
+    err = "batch: instance index out of range";
+    return FS_ERR_ARG;
+  }
+  prod_set_gains(B->inst[i], g);
+  B->dev_nsteps = 0;  // the device copy of the parameters is stale
+  return FS_OK;
+}
+
+int batch_set_drive(Batch *B, uint32_t i, const float *pb, cudaStream_t st, std::string &err) {
+  if (i >= B->inst.size()) {
+    err = "batch: instance index out of range";
+    return FS_ERR_ARG;
+  }
+  return prod_set_pb(B->inst[i], pb, st, err);
+}
 uint32_t batch_neurons(const Batch *B, uint32_t i) { return i < B->inst.size() ? B->inst[i]->n : 0; }
 
 }  // namespace fsp

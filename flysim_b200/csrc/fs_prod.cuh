@@ -52,5 +52,9 @@ int batch_spike_counts(Batch *b, uint32_t inst, uint32_t *counts, cudaStream_t s
 int batch_spike_totals(Batch *b, uint64_t *totals, cudaStream_t st, std::string &err);
 uint32_t batch_size(const Batch *b);
 uint32_t batch_neurons(const Batch *b, uint32_t inst);
+void prod_set_gains(Prod *p, const float *gains);
+int prod_set_pb(Prod *p, const float *pb, cudaStream_t st, std::string &err);
+int batch_set_gains(Batch *b, uint32_t inst, const float *gains, std::string &err);
+int batch_set_drive(Batch *b, uint32_t inst, const float *pb, cudaStream_t st, std::string &err);
 
 }  // namespace fsp

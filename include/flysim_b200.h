@@ -340,6 +340,16 @@ int fs_batch_info(fs_batch *b, uint32_t *count, uint32_t *blocks, uint32_t *bloc
 int fs_batch_spike_counts(fs_batch *b, uint32_t inst, uint32_t *counts);
 /* Total spikes of every instance since its reset (count entries). */
 int fs_batch_spike_totals(fs_batch *b, uint64_t *totals);
+/* Synaptic gains per receptor (FS_AMPA .. FS_NMDA; 1 = the weights as
+ * built): every recurrent weight of receptor r is scaled by gains[r], the
+ * analogue of the reference's per-population efficacy factors that its
+ * seizure scans vary (experiment/seizure/readme:1-6).  Production modes;
+ * takes effect at the next run. */
+int fs_set_gains(fs_handle *h, const float *gains);
+int fs_batch_set_gains(fs_batch *b, uint32_t inst, const float *gains);
+/* Drive probabilities of every neuron of instance inst, pb[FS_NREC * n]
+ * (receptor-major, as fs_neurons.pb). */
+int fs_batch_set_drive(fs_batch *b, uint32_t inst, const float *pb);
 
 /* ---- mean-field surrogate (no counterpart in the reference) -------------
  * A multilayer perceptron with ReLU hidden layers, BF16 weights and

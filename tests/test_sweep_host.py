@@ -36,3 +36,19 @@ def test_region_rates():
     r = sweep.region_rates(counts, region, 2.0)
     assert r.shape == (sweep.REGIONS,)
     assert r[0] == 1.5 and r[1] == 1.5 and r[57] == 5.0 and r[5] == 0.0
+
+
+def test_surrogate_parameterisation():
+    from flysim_b200 import surrogate as S
+    g = S.region_group()
+    assert g.shape == (58,) and g.min() == 0 and g.max() == 29
+    assert np.all(np.bincount(g)[:28] == 2) and np.all(np.bincount(g)[28:] == 1)
+    p = S.sample_params(1000, np.random.default_rng(1))
+    x = S.encode(p)
+    assert x.shape == (1000, 32) and x.min() >= -1.0 and x.max() <= 1.0
+    rates = np.abs(np.random.default_rng(2).normal(20, 30, (5, 58)))
+    t = S.targets(rates)
+    assert t.shape == (5, 59)
+    assert np.allclose(S.decode_rates(t), rates, rtol=1e-5)
+    assert np.all(t[:, -1] == (rates.mean(1) > S.HYPER_HZ))
+    assert S.rate_error(rates, rates).max() == 0.0
