@@ -658,13 +658,24 @@ __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32
         // warps without neurons in this tile skip the steps
         if ((tid & ~31u) < np) neuron_steps<T>(P, tp0, np, bs, L, gn, hits, gauss, lst);
         __syncthreads();
-        // the batch's spikes: one spike per warp, eight in flight per block
+        // the batch's spikes: with fewer spikes than warps the whole block
+        // walks each spike's out-edges (a hub's hundreds of edges in one or
+        // two rounds); with more, one spike per warp, eight in flight
         const uint32_t nl = min(l_n, kCap);
-        for (uint32_t k = wid; k < nl; k += kThreads / 32) {
-          T cj[4];
+        if (nl < kThreads / 32) {
+          for (uint32_t k = 0; k < nl; k++) {
+            T cj[4];
 #pragma unroll
-          for (int r = 0; r < 4; r++) cj[r] = l_c[k][r];
-          push_spike<T>(P, l_p[k], l_tm[k], cj, lane, 32);
+            for (int r = 0; r < 4; r++) cj[r] = l_c[k][r];
+            push_spike<T>(P, l_p[k], l_tm[k], cj, tid, kThreads);
+          }
+        } else {
+          for (uint32_t k = wid; k < nl; k += kThreads / 32) {
+            T cj[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) cj[r] = l_c[k][r];
+            push_spike<T>(P, l_p[k], l_tm[k], cj, lane, 32);
+          }
         }
         __syncthreads();
         if (tid == 0) l_n = 0;
