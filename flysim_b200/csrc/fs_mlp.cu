@@ -96,15 +96,25 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
+constexpr int kKC = 64;   // K columns per staging chunk (4 MMAs)
+constexpr int kCW = 64;   // output columns per epilogue chunk
+constexpr int kSP = kCW + 4;  // staging row pitch (floats)
+
 // Grid: x over 128-row tiles, y over column tiles of g.N / gridDim.y columns.
+// The operands are staged K chunk by K chunk; the MMAs of a chunk are issued
+// as soon as it is in shared memory, so they overlap the next chunk's loads.
+// The epilogue goes through shared memory (reusing the operand space once
+// the accumulator is complete) so that every global store is coalesced.
 __global__ void __launch_bounds__(kThreads) k_gemm_tn(const __grid_constant__ GemmArgs g) {
   extern __shared__ __align__(1024) uint8_t smem[];
   const int K = g.K, N = g.N / (int)gridDim.y, nks = K >> 4;
   const int n0 = blockIdx.y * N;  // first column of this CTA
   uint8_t *sA = smem;                              // nks slabs of 128 rows x 32 B
   uint8_t *sB = smem + (size_t)nks * kTileM * 32;  // nks slabs of N rows x 32 B
-  uint64_t *mbar = (uint64_t *)(sB + (size_t)nks * N * 32);
+  const size_t opnd = (size_t)nks * (kTileM + N) * 32, stage = (size_t)kTileM * kSP * 4;
+  uint64_t *mbar = (uint64_t *)(smem + (opnd > stage ? opnd : stage));
   uint32_t *tslot = (uint32_t *)(mbar + 1);
+  float *stg = (float *)smem;                      // epilogue staging [128][kSP]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * kTileM;
   uint32_t ncols = 32;
@@ -119,57 +129,56 @@ __global__ void __launch_bounds__(kThreads) k_gemm_tn(const __grid_constant__ Ge
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(mbar)));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
   }
-  // operands -> shared memory, eight 16-byte loads in flight per thread;
-  // rows past M read as zero
-  const int kc8 = K >> 3;
-  {
-    const int na = kTileM * kc8;
+  const uint32_t id = idesc_bf16(kTileM, (uint32_t)N);
+  for (int k0 = 0; k0 < K; k0 += kKC) {
+    const int kc0 = k0 >> 3, kcn = min(kKC, K - k0) >> 3;  // 8-wide K columns of this chunk
+    const int na = kTileM * kcn, nb = N * kcn;
     for (int i0 = tid; i0 < na; i0 += 8 * kThreads) {
       uint4 v[8];
 #pragma unroll
       for (int u = 0; u < 8; u++) {
-        const int idx = i0 + u * kThreads, r = idx % kTileM, kc = idx / kTileM;
+        const int idx = i0 + u * kThreads, r = idx % kTileM, kc = kc0 + idx / kTileM;
         v[u] = (idx < na && m0 + r < g.M) ? *(const uint4 *)(g.A + (size_t)(m0 + r) * g.lda + kc * 8)
                                            : make_uint4(0u, 0u, 0u, 0u);
       }
 #pragma unroll
       for (int u = 0; u < 8; u++) {
-        const int idx = i0 + u * kThreads, r = idx % kTileM, kc = idx / kTileM;
+        const int idx = i0 + u * kThreads, r = idx % kTileM, kc = kc0 + idx / kTileM;
         if (idx < na)
           *(uint4 *)(sA + (kc >> 1) * (kTileM * 32) + (r >> 3) * 256 + (kc & 1) * 128 + (r & 7) * 16) = v[u];
       }
     }
-    const int nb = N * kc8;
     for (int i0 = tid; i0 < nb; i0 += 8 * kThreads) {
       uint4 v[8];
 #pragma unroll
       for (int u = 0; u < 8; u++) {
-        const int idx = i0 + u * kThreads, r = idx % N, kc = idx / N;
+        const int idx = i0 + u * kThreads, r = idx % N, kc = kc0 + idx / N;
         v[u] = idx < nb ? *(const uint4 *)(g.B + (size_t)(n0 + r) * g.ldb + kc * 8) : make_uint4(0u, 0u, 0u, 0u);
       }
 #pragma unroll
       for (int u = 0; u < 8; u++) {
-        const int idx = i0 + u * kThreads, r = idx % N, kc = idx / N;
+        const int idx = i0 + u * kThreads, r = idx % N, kc = kc0 + idx / N;
         if (idx < nb)
           *(uint4 *)(sB + (size_t)(kc >> 1) * (N * 32) + (r >> 3) * 256 + (kc & 1) * 128 + (r & 7) * 16) = v[u];
       }
     }
-  }
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-  const uint32_t tmem = *tslot;
-  if (tid == 0) {
-    const uint32_t id = idesc_bf16(kTileM, (uint32_t)N);
-    for (int s = 0; s < nks; s++) {
-      const uint64_t ad = sdesc(smem_u32(sA + (size_t)s * kTileM * 32), 128, 256);
-      const uint64_t bd = sdesc(smem_u32(sB + (size_t)s * N * 32), 128, 256);
-      mma_bf16(tmem, ad, bd, id, s > 0 ? 1u : 0u);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (tid == 0) {
+      const uint32_t tmem = *tslot;
+      for (int sl = k0 >> 4; sl < ((k0 + kcn * 8) >> 4); sl++) {
+        const uint64_t ad = sdesc(smem_u32(sA + (size_t)sl * kTileM * 32), 128, 256);
+        const uint64_t bd = sdesc(smem_u32(sB + (size_t)sl * N * 32), 128, 256);
+        mma_bf16(tmem, ad, bd, id, sl > 0 ? 1u : 0u);
+      }
     }
+  }
+  const uint32_t tmem = *tslot;
+  if (tid == 0)
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
                      smem_u32(mbar))
                  : "memory");
-  }
   // wait for the accumulator (bounded)
   bool ok = false;
   {
@@ -191,26 +200,64 @@ __global__ void __launch_bounds__(kThreads) k_gemm_tn(const __grid_constant__ Ge
   }
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (!ok) {
-    if (g.err) atomicExch(g.err, 3);
+    if (g.err && tid == 0) atomicExch(g.err, 3);
   } else {
-    const int row = m0 + warp * 32 + lane;
-    const bool live = row < g.M;
-    for (int c0 = 0; c0 < N; c0 += 16) {
-      uint32_t v[16];
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-      if (!live) continue;
+    const int rl = warp * 32 + lane;  // this thread's accumulator row
+    for (int cc = 0; cc < N; cc += kCW) {
+      const int cw = min(kCW, N - cc);
+      // TMEM -> registers -> (bias, ReLU) -> staging
+      for (int c0 = 0; c0 < cw; c0 += 16) {
+        uint32_t v[16];
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cc + c0), v);
 #pragma unroll
-      for (int j = 0; j < 16; j++) {
-        const int c = n0 + c0 + j;
-        float x = __uint_as_float(v[j]);
-        if (g.bias) x += g.bias[c];
-        if (g.relu) x = fmaxf(x, 0.0f);
-        if (g.mask && !(__bfloat162float(g.mask[(size_t)row * g.ldm + c]) > 0.0f)) x = 0.0f;
-        if (g.Cf) g.Cf[(size_t)row * g.ldcf + c] = x;
-        const bf16 xb = __float2bfloat16_rn(x);
-        if (g.Cb) g.Cb[(size_t)row * g.ldcb + c] = xb;
-        if (g.Ct) g.Ct[(size_t)c * g.ldct + row] = xb;
+        for (int j = 0; j < 16; j++) {
+          float x = __uint_as_float(v[j]);
+          if (g.bias) x += g.bias[n0 + cc + c0 + j];
+          if (g.relu) x = fmaxf(x, 0.0f);
+          stg[rl * kSP + c0 + j] = x;
+        }
       }
+      __syncthreads();
+      const int rows = min(kTileM, g.M - m0);
+      // row-major outputs: 8 consecutive columns per thread, coalesced
+      const int c8 = cw >> 3;
+      for (int i = tid; i < rows * c8; i += kThreads) {
+        const int r = i / c8, c = (i - r * c8) * 8;
+        float x[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) x[j] = stg[r * kSP + c + j];
+        const size_t gc = (size_t)n0 + cc + c;
+        if (g.mask) {
+          const uint4 mv = *(const uint4 *)(g.mask + (size_t)(m0 + r) * g.ldm + gc);
+          const bf16 *mb = (const bf16 *)&mv;
+#pragma unroll
+          for (int j = 0; j < 8; j++)
+            if (!(__bfloat162float(mb[j]) > 0.0f)) x[j] = 0.0f;
+#pragma unroll
+          for (int j = 0; j < 8; j++) stg[r * kSP + c + j] = x[j];  // masked values for the transposed store
+        }
+        if (g.Cf) {
+          float4 *dst = (float4 *)(g.Cf + (size_t)(m0 + r) * g.ldcf + gc);
+          dst[0] = make_float4(x[0], x[1], x[2], x[3]);
+          dst[1] = make_float4(x[4], x[5], x[6], x[7]);
+        }
+        if (g.Cb) {
+          uint4 o;
+          bf16 *ob = (bf16 *)&o;
+#pragma unroll
+          for (int j = 0; j < 8; j++) ob[j] = __float2bfloat16_rn(x[j]);
+          *(uint4 *)(g.Cb + (size_t)(m0 + r) * g.ldcb + gc) = o;
+        }
+      }
+      if (g.Ct) {
+        __syncthreads();
+        // transposed: consecutive threads take consecutive rows of one column
+        for (int i = tid; i < rows * cw; i += kThreads) {
+          const int c = i / rows, r = i - c * rows;
+          g.Ct[((size_t)n0 + cc + c) * g.ldct + m0 + r] = __float2bfloat16_rn(stg[r * kSP + c]);
+        }
+      }
+      __syncthreads();
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -218,25 +265,31 @@ __global__ void __launch_bounds__(kThreads) k_gemm_tn(const __grid_constant__ Ge
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(ncols));
 }
 
-size_t gemm_smem(int N, int K) { return (size_t)(K / 16) * (kTileM + N) * 32 + 16; }
+size_t gemm_smem(int N, int K) {
+  const size_t opnd = (size_t)(K / 16) * (kTileM + N) * 32, stage = (size_t)kTileM * kSP * 4;
+  return (opnd > stage ? opnd : stage) + 16;
+}
 
 bool gemm_attr_set = false;
 
 // Checks the shape rules and launches one GEMM.
 int gemm(const GemmArgs &g, cudaStream_t st, std::string &err) {
   if (g.N < 16 || g.N > 256 || g.N % 16 || g.K < 16 || g.K > 256 || g.K % 16 || g.M < 1 || g.lda % 8 ||
-      g.ldb % 8 || ((uintptr_t)g.A & 15) || ((uintptr_t)g.B & 15)) {
-    err = "gemm: N and K must be multiples of 16 in [16, 256], leading dimensions multiples of 8, "
-          "operands 16-byte aligned";
+      g.ldb % 8 || ((uintptr_t)g.A & 15) || ((uintptr_t)g.B & 15) ||
+      (g.Cf && (g.ldcf % 4 || ((uintptr_t)g.Cf & 15))) || (g.Cb && (g.ldcb % 8 || ((uintptr_t)g.Cb & 15))) ||
+      (g.mask && (g.ldm % 8 || ((uintptr_t)g.mask & 15)))) {
+    err = "gemm: N and K must be multiples of 16 in [16, 256], leading dimensions multiples of 8 (4 for "
+          "FP32 output), operands and outputs 16-byte aligned";
     return FS_ERR_ARG;
   }
   if (!gemm_attr_set) {
     cudaFuncSetAttribute(k_gemm_tn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem(256, 256));
     gemm_attr_set = true;
   }
-  // column tiles of 64 (or all of N when it is not a multiple of 64) so that
-  // small-M GEMMs still spread over several SMs
-  const int ny = (g.N % 64 == 0) ? g.N / 64 : 1;
+  // column tiles of 64 when there are few row tiles (training batches), so
+  // that small-M GEMMs still spread over the SMs; one column tile otherwise
+  const int tiles = (g.M + kTileM - 1) / kTileM;
+  const int ny = (g.N % 64 == 0 && tiles < 296) ? g.N / 64 : 1;
   const dim3 grid((g.M + kTileM - 1) / kTileM, ny);
   k_gemm_tn<<<grid, kThreads, gemm_smem(g.N / ny, g.K), st>>>(g);
   cudaError_t e = cudaGetLastError();
