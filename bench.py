@@ -105,13 +105,27 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def build_network(rank: int):
+# --workload: the 20k-neuron connectome (the default, the headline) or the
+# scaled network (1,000,000 neurons, ~100 M connections, Tsodyks-Markram
+# plasticity on excitatory synapses; its working set is far beyond L2)
+WORKLOADS = {
+    "connectome20k": dict(n=N_NEURONS, mean_degree=120.0, tm=False),
+    "scaled1m": dict(n=1_000_000, mean_degree=100.0, tm=True),
+    "scaled250k": dict(n=250_000, mean_degree=100.0, tm=True),  # the same network, sized for ncu captures
+}
+
+
+def build_network(rank: int, workload: str = "connectome20k"):
     from flysim_b200 import netgen, network
-    c = netgen.connectome(n=N_NEURONS, regions=REGIONS, seed=SEED + rank)
-    return c, network.connectome_net(c, dt=DT, with_delays=True)
+    w = WORKLOADS[workload]
+    if workload == "connectome20k":
+        c = netgen.connectome(n=w["n"], regions=REGIONS, seed=SEED + rank)
+    else:
+        c = netgen.connectome_fast(n=w["n"], regions=REGIONS, mean_degree=w["mean_degree"], seed=SEED + rank)
+    return c, network.connectome_net(c, dt=DT, with_delays=True, tm=w["tm"])
 
 
-def algorithmic_bytes(na, spikes: int, steps: int, avg_lin_out: float) -> float:
+def algorithmic_bytes(na, spikes: int, steps: int, avg_lin_out: float, tm: bool = False) -> float:
     """Bytes a launch must move at minimum: per neuron-step 60 B of state
     (V, LIF state, 2 conductance slots, NMDA post sum, ext gate: 24 B read,
     20 B written; presynaptic NMDA x/s: 16 B); N/8 B of spike flags; 12 B per
@@ -121,6 +135,8 @@ def algorithmic_bytes(na, spikes: int, steps: int, avg_lin_out: float) -> float:
     n = na.n
     nmda_edges = int(np.count_nonzero(na.syn["rec"] == 4))
     per_step = n * 60 + n / 8.0 + nmda_edges * 12
+    if tm:  # Tsodyks-Markram u, x of every excitatory neuron, read and written
+        per_step += 16 * int(np.count_nonzero(na.tm["enabled"]))
     return steps * per_step + spikes * (4 + avg_lin_out * 16)
 
 
@@ -229,6 +245,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="connectome20k", choices=sorted(WORKLOADS))
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="run this many timesteps once and exit (for ncu captures)")
     args = ap.parse_args()
@@ -245,7 +262,8 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
 
-    c, na = build_network(rank)
+    c, na = build_network(rank, args.workload)
+    tm = WORKLOADS[args.workload]["tm"]
     eng = fb.Engine(na.desc, args.mode, device=local, chunk_steps=STEPS_PER_BENCH_STEP)
     eng.reset(SEED + rank)
     if args.profile_steps:
@@ -293,11 +311,11 @@ def main():
     avg_lin_out = float(np.count_nonzero(lin)) / na.n
     k_ms = float(np.mean(kern_ms))
     spikes_per_launch = spikes / max(1, args.steps)
-    alg = algorithmic_bytes(na, spikes_per_launch, STEPS_PER_BENCH_STEP, avg_lin_out)
+    alg = algorithmic_bytes(na, spikes_per_launch, STEPS_PER_BENCH_STEP, avg_lin_out, tm)
     peak, peak_kind = load_peaks()
     achieved = alg / (k_ms * 1e-3) / 1e9
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "prod_fp32_connectome20k_traffic.json")
+    tp = os.path.join(ROOT, "profiles", "prod_fp32_%s_traffic.json" % args.workload)
     if os.path.exists(tp):
         tj = json.load(open(tp))
         traffic = tj.get("dram_bytes_per_timestep", 0) * STEPS_PER_BENCH_STEP
@@ -320,7 +338,8 @@ def main():
             # region by region (uploaded host -> device inside fs_step)
             for lo, hi in region_bounds:
                 eng.set_drive(int(lo), int(hi - lo), 0, float(pb_host[lo]))
-            spk, _ = eng.step(STEPS_PER_BENCH_STEP, spike_cap=STEPS_PER_BENCH_STEP * 64)
+            cap = int(2 * spikes / max(1, args.steps)) + STEPS_PER_BENCH_STEP * 64
+            spk, _ = eng.step(STEPS_PER_BENCH_STEP, spike_cap=cap)
             t1 = time.perf_counter()
             e2e_wall.append(t1 - t0)
             d2h = 4 * STEPS_PER_BENCH_STEP + 4 * sum(int(x.size) for x in spk) + 4
@@ -335,23 +354,28 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_baseline_port(c)
+            cpu = cpu_baseline_port(c) if args.workload == "connectome20k" else None
         except Exception as ex:  # reported, not fatal
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "port", "sample": "failed: %s" % ex}
 
     if rank == 0:
+        scaled = args.workload != "connectome20k"
+        ws = int((na.n_syn * 8 + na.n * 200) / 1e6)
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": METRIC if not scaled else
+            "simulated seconds per wall second (%d-neuron scaled network)" % na.n, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.mode == "fp32" else "f64",
             "data": "synthetic",
             "config": {"workload": "connectome-shaped network: %d LIF neurons, %d regions, %d connections "
-                                   "(%d synapse entries), delays 1-5 ms, drive 1-4 kHz, dt 0.1 ms, %s mode; "
+                                   "(%d synapse entries), delays 1-5 ms, drive 1-4 kHz, dt 0.1 ms, %s mode%s; "
                                    "one step = 1 s simulated (10,000 timesteps)"
-                                   % (na.n, REGIONS, c.n_connections, na.n_syn, args.mode),
+                                   % (na.n, REGIONS, c.n_connections, na.n_syn, args.mode,
+                                      ", Tsodyks-Markram plasticity on excitatory synapses" if tm else ""),
                        "parallelism": "replicas" if world > 1 else "single GPU",
-                       "l2": "flushed (256 MB write) before every timed step; the ~%d MB working set is "
-                             "L2-resident within a step" % int((na.n_syn * 8 + na.n * 200) / 1e6)},
+                       "l2": ("flushed (256 MB write) before every timed step; the ~%d MB working set is "
+                              "L2-resident within a step" % ws) if ws < 100 else
+                             ("inputs larger than L2: ~%d MB working set" % ws)},
             "syn_events_per_s": syn_events_per_s,
             "spikes_per_step": spikes / args.steps,
             "mean_rate_hz": spikes / args.steps / na.n,

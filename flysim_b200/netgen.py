@@ -144,10 +144,19 @@ def connectome_fast(n: int = 20000, regions: int = 58, mean_degree: float = 120.
         s, a = int(sizes[r]), int(starts[r])
         if s < 2:
             continue
+        kk = k_in[a:a + s]
+        if s > 2048:
+            # large regions: targets drawn with replacement (self excluded)
+            # and deduplicated below; at ~100 draws from thousands the loss
+            # is a fraction of a percent
+            src = np.repeat(np.arange(s), kk)
+            u = rng.integers(0, s - 1, src.size)
+            pre_l.append(src + a)
+            post_l.append(u + (u >= src) + a)
+            continue
         keys = rng.random((s, s))
         np.fill_diagonal(keys, 2.0)  # never self
         order = np.argsort(keys, axis=1)
-        kk = k_in[a:a + s]
         take = np.arange(s)[None, :] < kk[:, None]
         src = np.repeat(np.arange(s), kk)
         pre_l.append(src + a)
