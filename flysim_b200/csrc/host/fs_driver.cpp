@@ -14,6 +14,8 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <functional>
+#include <thread>
 #include <iostream>
 #include <algorithm>
 #include "fs_host.hpp"
@@ -105,22 +107,64 @@ int run_protocol(Model &m, const fs_engine_vtbl *eng, void *ctx, const std::stri
     }
   }
   const uint32_t gv_n = (uint32_t)gv_all.size();
-  std::vector<float> gv_st, gv_xt;
-  if (gv_n) {
-    gv_st.resize((size_t)chunk_steps * gv_n);
-    gv_xt.resize((size_t)chunk_steps * gv_n);
+  // Spike and FiringRate outputs over many populations: per-neuron maps so
+  // that a step costs O(spikes) instead of a search per listed population.
+  // Used when the list is ascending and has no repeats (then walking the
+  // sorted spikes emits the lines in the list's order); other lists take the
+  // general loop.
+  std::vector<uint32_t> pop_of(n, 0xffffffffu);
+  for (uint32_t pp = 0; pp < np; pp++)
+    for (uint32_t k = net.nidx[pp]; k < net.nidx[pp] + m.pops[pp].N; k++) pop_of[k] = pp;
+  std::vector<std::vector<int64_t>> spike_map(m.outs.size());  // neuron -> printed index, -1 = not listed
+  std::vector<std::vector<int32_t>> rate_pos(m.outs.size());   // population -> list position, -1
+  for (size_t i = 0; i < m.outs.size(); i++) {
+    const OutCtl &o = m.outs[i];
+    if (o.TypeID != OUT_SPIKE && o.TypeID != OUT_FRATE) continue;
+    bool ascending = true;
+    for (size_t j = 1; j < o.ParList.size(); j++) ascending &= o.ParList[j] > o.ParList[j - 1];
+    bool in_range = true;
+    for (uint32_t pp : o.ParList) in_range &= pp < np;
+    if (!ascending || !in_range) continue;
+    if (o.TypeID == OUT_SPIKE) {
+      std::vector<int64_t> &mp = spike_map[i];
+      mp.assign(n, -1);
+      unsigned long long cnt = 0;
+      for (uint32_t pp : o.ParList) {
+        const uint32_t b = net.nidx[pp];
+        for (uint32_t k = b; k < b + m.pops[pp].N; k++)
+          mp[k] = (o.Status & OF_ALIGN) ? (int64_t)(cnt + (k - b)) : (int64_t)k;
+        cnt += m.pops[pp].N;
+      }
+    } else {
+      std::vector<int32_t> &rp = rate_pos[i];
+      rp.assign(np, -1);
+      for (size_t j = 0; j < o.ParList.size(); j++) rp[o.ParList[j]] = (int32_t)j;
+    }
   }
   const int rp = std::max(1, m.opts.repeats);
   double total_run = 0.0;
-  // per-step output buffers
-  std::vector<uint32_t> counts(chunk_steps);
-  std::vector<uint32_t> spikes;
-  std::vector<float> Vbuf, Ibuf;
-  std::vector<uint32_t> NSbuf;
-  if (need_V) Vbuf.resize((size_t)chunk_steps * n);
-  if (need_Irep) Ibuf.resize((size_t)chunk_steps * FS_NREC * n);
-  if (need_ns) NSbuf.resize((size_t)chunk_steps * n);
-  spikes.resize((size_t)chunk_steps * n);
+  // Output pipeline: two buffer sets; while a formatter thread writes the
+  // files of chunk k from one set, the engine computes chunk k+1 into the
+  // other.  Chunks are formatted strictly in order (the next formatter starts
+  // after the previous one joined), so the files are those of a serial run.
+  struct ChunkBuf {
+    std::vector<uint32_t> counts, spikes, NS;
+    std::vector<float> V, I, gst, gxt;
+    unsigned long long first = 0;
+    uint32_t steps = 0;
+  };
+  ChunkBuf bufs[2];
+  for (ChunkBuf &b : bufs) {
+    b.counts.resize(chunk_steps);
+    b.spikes.resize((size_t)chunk_steps * n);
+    if (need_V) b.V.resize((size_t)chunk_steps * n);
+    if (need_Irep) b.I.resize((size_t)chunk_steps * FS_NREC * n);
+    if (need_ns) b.NS.resize((size_t)chunk_steps * n);
+    if (gv_n) {
+      b.gst.resize((size_t)chunk_steps * gv_n);
+      b.gxt.resize((size_t)chunk_steps * gv_n);
+    }
+  }
 
   for (int rep = 1; rep <= rp; rep++) {
     const Event &last = m.events.back();
@@ -209,6 +253,18 @@ int run_protocol(Model &m, const fs_engine_vtbl *eng, void *ctx, const std::stri
             break;
           }
           case OUT_SPIKE: {
+            if (!spike_map[i].empty()) {
+              const std::vector<int64_t> &mp = spike_map[i];
+              for (uint32_t q = 0; q < nsp; q++) {
+                const int64_t v = mp[sp[q]];
+                if (v < 0) continue;
+                put_g(s, tsec);
+                s.push_back(' ');
+                put_u(s, (unsigned long long)v);
+                s.push_back('\n');
+              }
+              break;
+            }
             unsigned long long cnt = 0;
             for (uint32_t pp : o.ParList) {
               const uint32_t b = net.nidx[pp], e = b + m.pops[pp].N;
@@ -227,12 +283,20 @@ int run_protocol(Model &m, const fs_engine_vtbl *eng, void *ctx, const std::stri
           case OUT_FRATE: {
             const size_t P = o.ParList.size();
             std::vector<uint32_t> &w = o.SpiRWin;
-            for (size_t j = 0; j < P; j++) {
-              const uint32_t pp = o.ParList[j];
-              const uint32_t b = net.nidx[pp], e = b + m.pops[pp].N;
-              const uint32_t *lo = std::lower_bound(sp, sp + nsp, b);
-              const uint32_t *hi = std::lower_bound(lo, sp + nsp, e);
-              w[P * o.RWin + j] += (uint32_t)(hi - lo);
+            if (!rate_pos[i].empty()) {
+              for (uint32_t q = 0; q < nsp; q++) {
+                const uint32_t pp = pop_of[sp[q]];
+                const int32_t j = pp < np ? rate_pos[i][pp] : -1;
+                if (j >= 0) w[P * o.RWin + j] += 1;
+              }
+            } else {
+              for (size_t j = 0; j < P; j++) {
+                const uint32_t pp = o.ParList[j];
+                const uint32_t b = net.nidx[pp], e = b + m.pops[pp].N;
+                const uint32_t *lo = std::lower_bound(sp, sp + nsp, b);
+                const uint32_t *hi = std::lower_bound(lo, sp + nsp, e);
+                w[P * o.RWin + j] += (uint32_t)(hi - lo);
+              }
             }
             if (step % one_ms == 0) {
               const unsigned long long s1ms = step / one_ms;
@@ -332,35 +396,53 @@ int run_protocol(Model &m, const fs_engine_vtbl *eng, void *ctx, const std::stri
     auto t1 = std::chrono::high_resolution_clock::now();
     unsigned long long i = 0, batch_first = 0;
     uint32_t pending = 0;
+    int cur = 0;
+    std::thread formatter;
+    auto join = [&]() {
+      if (formatter.joinable()) formatter.join();
+    };
+    auto format_chunk = [&](ChunkBuf *b) {
+      uint64_t off = 0;
+      for (uint32_t s = 0; s < b->steps; s++) {
+        file_out(b->first + s, b->spikes.data() + off, b->counts[s],
+                 need_V ? b->V.data() + (size_t)s * n : nullptr,
+                 need_Irep ? b->I.data() + (size_t)s * FS_NREC * n : nullptr,
+                 need_ns ? b->NS.data() + (size_t)s * n : nullptr,
+                 gv_n ? b->gst.data() + (size_t)s * gv_n : nullptr,
+                 gv_n ? b->gxt.data() + (size_t)s * gv_n : nullptr);
+        off += b->counts[s];
+      }
+    };
     auto flush = [&]() -> int {
       if (pending == 0) return FS_OK;
+      ChunkBuf &b = bufs[cur];  // its previous formatter (two chunks ago) has joined
       fs_step_out so{};
-      so.spike_count = counts.data();
-      so.spike_idx = spikes.data();
-      so.spike_cap = spikes.size();
-      so.V = need_V ? Vbuf.data() : nullptr;
-      so.Irep = need_Irep ? Ibuf.data() : nullptr;
-      so.nstate = need_ns ? NSbuf.data() : nullptr;
+      so.spike_count = b.counts.data();
+      so.spike_idx = b.spikes.data();
+      so.spike_cap = b.spikes.size();
+      so.V = need_V ? b.V.data() : nullptr;
+      so.Irep = need_Irep ? b.I.data() : nullptr;
+      so.nstate = need_ns ? b.NS.data() : nullptr;
       so.gv_sel = gv_n ? gv_all.data() : nullptr;
       so.gv_n = gv_n;
-      so.gv_st = gv_n ? gv_st.data() : nullptr;
-      so.gv_xt = gv_n ? gv_xt.data() : nullptr;
+      so.gv_st = gv_n ? b.gst.data() : nullptr;
+      so.gv_xt = gv_n ? b.gxt.data() : nullptr;
       int r = eng->step(ctx, pending, &so);
+      join();  // the previous chunk's files are complete
       if (r) return r;
-      uint64_t off = 0;
-      for (uint32_t s = 0; s < pending; s++) {
-        file_out(batch_first + s, spikes.data() + off, counts[s],
-                 need_V ? Vbuf.data() + (size_t)s * n : nullptr,
-                 need_Irep ? Ibuf.data() + (size_t)s * FS_NREC * n : nullptr,
-                 need_ns ? NSbuf.data() + (size_t)s * n : nullptr,
-                 gv_n ? gv_st.data() + (size_t)s * gv_n : nullptr,
-                 gv_n ? gv_xt.data() + (size_t)s * gv_n : nullptr);
-        off += counts[s];
-      }
+      b.first = batch_first;
+      b.steps = pending;
+      formatter = std::thread(format_chunk, &b);
+      cur ^= 1;
       batch_first += pending;
       pending = 0;
       return FS_OK;
     };
+    // every return below joins the formatter first
+    struct Joiner {
+      std::function<void()> f;
+      ~Joiner() { f(); }
+    } joiner{join};
     for (; (i < endtime) || nolmt; i++) {
       int erc = 0;
       if (events_at(i, false, erc)) {
@@ -380,6 +462,7 @@ int run_protocol(Model &m, const fs_engine_vtbl *eng, void *ctx, const std::stri
       int r = flush();
       if (r) return fail(r);
     }
+    join();
     auto t2 = std::chrono::high_resolution_clock::now();
     const double secs = std::chrono::duration_cast<std::chrono::nanoseconds>(t2 - t1).count() * 1e-9;
     total_run += secs;
