@@ -125,6 +125,24 @@ def build_network(rank: int, workload: str = "connectome20k"):
     return c, network.connectome_net(c, dt=DT, with_delays=True, tm=w["tm"])
 
 
+def max_over_ranks(x: float, world: int, device: str = "cuda") -> float:
+    """The slowest rank's figure: replicas report the whole job's time as the
+    maximum over ranks (one collective, no data-path traffic)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world: int, sim_s_per_rank: float, max_ms: float) -> float:
+    """Whole-job throughput of `world` independent replicas: simulated
+    seconds of all ranks over the slowest rank's time."""
+    return world * sim_s_per_rank / (max_ms * 1e-3)
+
+
 def algorithmic_bytes(na, spikes: int, steps: int, avg_lin_out: float, tm: bool = False) -> float:
     """Bytes a launch must move at minimum: per neuron-step 60 B of state
     (V, LIF state, 2 conductance slots, NMDA post sum, ext gate: 24 B read,
@@ -294,13 +312,9 @@ def main():
         barrier()
     clk = clocks.stop()
     s1 = eng.stats()
-    total_ms = float(np.sum(dev_ms))
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(float(np.sum(dev_ms)), world)
     sim_s = args.steps * STEPS_PER_BENCH_STEP * DT * 1e-3
-    value = world * sim_s / (total_ms * 1e-3)
+    value = replica_value(world, sim_s, total_ms)
     spikes = s1["spikes"] - s0["spikes"]
     launches = s1["launches"] - s0["launches"]
     # synaptic events: spikes x outgoing connections of the spiking neurons
@@ -343,11 +357,7 @@ def main():
             t1 = time.perf_counter()
             e2e_wall.append(t1 - t0)
             d2h = 4 * STEPS_PER_BENCH_STEP + 4 * sum(int(x.size) for x in spk) + 4
-        e2e_s = float(np.median(e2e_wall))
-        if world > 1:
-            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = max_over_ranks(float(np.median(e2e_wall)), world)
         e2e = {"value": world * STEPS_PER_BENCH_STEP * DT * 1e-3 / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 

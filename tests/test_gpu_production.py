@@ -195,3 +195,32 @@ def test_seed_and_key_change_the_drive(built):
             e.close()
     same = lambda a, b: all(np.array_equal(x, y) for x, y in zip(a, b))  # noqa: E731
     assert not same(out[0], out[1]) and not same(out[0], out[2])
+
+
+def test_cli_production_modes_match_compat_statistics(built, tmp_path):
+    """The drop-in command line in FS_MODE_FP32 / FP64 on a reference-format
+    network (E=800 / I=200, 2 s): the same output files (line counts of the
+    rate files), population spike counts within 3 % of the reference-order
+    compat run."""
+    import subprocess
+    from flysim_b200 import netgen
+    netgen.write_two_pop(str(tmp_path / "net.conf"))
+    netgen.write_pro(str(tmp_path / "net.pro"), 2000.0, seeds=(3,), outputs=(
+        {"name": "Spikes.dat", "type": "Spike", "pop": "AllPopulation"},))
+    exe = os.path.join(ROOT, "flysim_b200", "_build", "flysim")
+    counts = {}
+    for mode in ("compat", "fp32", "fp64"):
+        d = tmp_path / mode
+        d.mkdir()
+        for f in ("net.conf", "net.pro"):
+            os.symlink(str(tmp_path / f), str(d / f))
+        r = subprocess.run([exe, "-conf", "net.conf", "-pro", "net.pro", "-mode", mode], cwd=str(d),
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr
+        sp = np.loadtxt(str(d / "Spikes.dat"), ndmin=2)
+        k = sp[:, 1].astype(np.int64)
+        counts[mode] = np.array([np.count_nonzero(k < 800), np.count_nonzero(k >= 800)], np.float64)
+    assert np.all(counts["compat"] > 1000), counts
+    for mode in ("fp32", "fp64"):
+        rel = np.abs(counts[mode] / counts["compat"] - 1)
+        assert rel.max() < 0.03, (mode, counts)
