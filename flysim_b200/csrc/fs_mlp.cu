@@ -26,6 +26,7 @@
 #include <random>
 #include <string>
 #include <vector>
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include "flysim_b200.h"
@@ -96,27 +97,58 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
-constexpr int kKC = 64;   // K columns per staging chunk (4 MMAs)
+constexpr int kKC = 64;   // K columns per load chunk (4 MMAs, one mbarrier)
 constexpr int kCW = 64;   // output columns per epilogue chunk
 constexpr int kSP = kCW + 4;  // staging row pitch (floats)
+constexpr int kMaxChunks = 256 / kKC;
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          dst),
+      "l"(map), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (uint32_t it = 0; it < kSpin; it++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
 
 // Grid: x over 128-row tiles, y over column tiles of g.N / gridDim.y columns.
-// The operands are staged K chunk by K chunk; the MMAs of a chunk are issued
-// as soon as it is in shared memory, so they overlap the next chunk's loads.
-// The epilogue goes through shared memory (reusing the operand space once
-// the accumulator is complete) so that every global store is coalesced.
-__global__ void __launch_bounds__(kThreads) k_gemm_tn(const __grid_constant__ GemmArgs g) {
+// Operands arrive by TMA (cp.async.bulk.tensor, no swizzle): each 8-wide K
+// column of a tile is one box of rows x 16 bytes, which is exactly a stack
+// of K-major core matrices (8 rows x 16 bytes, 128 bytes apart), so one
+// thread issues every box of the tile up front, K chunk by K chunk on its
+// own mbarrier, and starts each chunk's MMAs as soon as it lands.  Rows past
+// M are the TMA's zero fill.  The epilogue goes through shared memory
+// (reusing the operand space once the accumulator is complete) so that
+// every global store is coalesced.
+__global__ void __launch_bounds__(kThreads) k_gemm_tn(const __grid_constant__ GemmArgs g,
+                                                      const __grid_constant__ CUtensorMap ta,
+                                                      const __grid_constant__ CUtensorMap tb) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  const int K = g.K, N = g.N / (int)gridDim.y, nks = K >> 4;
+  const int K = g.K, N = g.N / (int)gridDim.y, nkb = K >> 3;  // 8-wide K columns
   const int n0 = blockIdx.y * N;  // first column of this CTA
-  uint8_t *sA = smem;                              // nks slabs of 128 rows x 32 B
-  uint8_t *sB = smem + (size_t)nks * kTileM * 32;  // nks slabs of N rows x 32 B
-  const size_t opnd = (size_t)nks * (kTileM + N) * 32, stage = (size_t)kTileM * kSP * 4;
-  uint64_t *mbar = (uint64_t *)(smem + (opnd > stage ? opnd : stage));
-  uint32_t *tslot = (uint32_t *)(mbar + 1);
+  uint8_t *sA = smem;                              // nkb boxes of 128 rows x 16 B
+  uint8_t *sB = smem + (size_t)nkb * kTileM * 16;  // nkb boxes of N rows x 16 B
+  const size_t opnd = (size_t)nkb * (kTileM + N) * 16, stage = (size_t)kTileM * kSP * 4;
+  uint64_t *mbar = (uint64_t *)(smem + (opnd > stage ? opnd : stage));  // [0] MMA, [1..] K chunks
+  uint32_t *tslot = (uint32_t *)(mbar + 1 + kMaxChunks);
   float *stg = (float *)smem;                      // epilogue staging [128][kSP]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * kTileM;
+  const int nch = (K + kKC - 1) / kKC;
   uint32_t ncols = 32;
   while (ncols < (uint32_t)N) ncols <<= 1;
 
@@ -126,78 +158,46 @@ __global__ void __launch_bounds__(kThreads) k_gemm_tn(const __grid_constant__ Ge
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(mbar)));
+    for (int c = 0; c <= nch; c++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(mbar + c)));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
-  }
-  const uint32_t id = idesc_bf16(kTileM, (uint32_t)N);
-  for (int k0 = 0; k0 < K; k0 += kKC) {
-    const int kc0 = k0 >> 3, kcn = min(kKC, K - k0) >> 3;  // 8-wide K columns of this chunk
-    const int na = kTileM * kcn, nb = N * kcn;
-    for (int i0 = tid; i0 < na; i0 += 8 * kThreads) {
-      uint4 v[8];
-#pragma unroll
-      for (int u = 0; u < 8; u++) {
-        const int idx = i0 + u * kThreads, r = idx % kTileM, kc = kc0 + idx / kTileM;
-        v[u] = (idx < na && m0 + r < g.M) ? *(const uint4 *)(g.A + (size_t)(m0 + r) * g.lda + kc * 8)
-                                           : make_uint4(0u, 0u, 0u, 0u);
-      }
-#pragma unroll
-      for (int u = 0; u < 8; u++) {
-        const int idx = i0 + u * kThreads, r = idx % kTileM, kc = kc0 + idx / kTileM;
-        if (idx < na)
-          *(uint4 *)(sA + (kc >> 1) * (kTileM * 32) + (r >> 3) * 256 + (kc & 1) * 128 + (r & 7) * 16) = v[u];
-      }
-    }
-    for (int i0 = tid; i0 < nb; i0 += 8 * kThreads) {
-      uint4 v[8];
-#pragma unroll
-      for (int u = 0; u < 8; u++) {
-        const int idx = i0 + u * kThreads, r = idx % N, kc = kc0 + idx / N;
-        v[u] = idx < nb ? *(const uint4 *)(g.B + (size_t)(n0 + r) * g.ldb + kc * 8) : make_uint4(0u, 0u, 0u, 0u);
-      }
-#pragma unroll
-      for (int u = 0; u < 8; u++) {
-        const int idx = i0 + u * kThreads, r = idx % N, kc = kc0 + idx / N;
-        if (idx < nb)
-          *(uint4 *)(sB + (size_t)(kc >> 1) * (N * 32) + (r >> 3) * 256 + (kc & 1) * 128 + (r & 7) * 16) = v[u];
-      }
-    }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    if (tid == 0) {
-      const uint32_t tmem = *tslot;
-      for (int sl = k0 >> 4; sl < ((k0 + kcn * 8) >> 4); sl++) {
-        const uint64_t ad = sdesc(smem_u32(sA + (size_t)sl * kTileM * 32), 128, 256);
-        const uint64_t bd = sdesc(smem_u32(sB + (size_t)sl * N * 32), 128, 256);
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tslot;
+  bool loads_ok = true;
+  if (tid == 0) {
+    // every box of the tile, chunk by chunk
+    for (int c = 0; c < nch; c++) {
+      const int kb0 = c * (kKC / 8), kb1 = min(nkb, kb0 + kKC / 8);
+      const uint32_t bytes = (uint32_t)(kb1 - kb0) * (uint32_t)(kTileM + N) * 16u;
+      const uint32_t bar = smem_u32(mbar + 1 + c);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+      for (int kb = kb0; kb < kb1; kb++) {
+        tma_load_2d(smem_u32(sA + (size_t)kb * kTileM * 16), &ta, kb * 8, m0, bar);
+        tma_load_2d(smem_u32(sB + (size_t)kb * N * 16), &tb, kb * 8, n0, bar);
+      }
+    }
+    // MMAs as the chunks land: slab s (16 wide) = boxes 2s (LBO away: 2s+1)
+    const uint32_t id = idesc_bf16(kTileM, (uint32_t)N);
+    for (int c = 0; c < nch && loads_ok; c++) {
+      loads_ok = mbar_wait(smem_u32(mbar + 1 + c), 0);
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const int s0 = c * (kKC / 16), s1 = min(K >> 4, s0 + kKC / 16);
+      for (int sl = s0; sl < s1 && loads_ok; sl++) {
+        const uint64_t ad = sdesc(smem_u32(sA + (size_t)(2 * sl) * kTileM * 16), kTileM * 16, 128);
+        const uint64_t bd = sdesc(smem_u32(sB + (size_t)(2 * sl) * N * 16), (uint32_t)N * 16, 128);
         mma_bf16(tmem, ad, bd, id, sl > 0 ? 1u : 0u);
       }
     }
+    if (!loads_ok && g.err) atomicExch(g.err, 4);
   }
-  const uint32_t tmem = *tslot;
   if (tid == 0)
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
                      smem_u32(mbar))
                  : "memory");
-  // wait for the accumulator (bounded)
-  bool ok = false;
-  {
-    const uint32_t mb = smem_u32(mbar);
-    for (uint32_t it = 0; it < kSpin; it++) {
-      uint32_t done;
-      asm volatile(
-          "{\n\t.reg .pred p;\n\t"
-          "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
-          "selp.u32 %0, 1, 0, p;\n\t}\n"
-          : "=r"(done)
-          : "r"(mb)
-          : "memory");
-      if (done) {
-        ok = true;
-        break;
-      }
-    }
-  }
+  // wait for the accumulator (bounded); the commit covers every MMA issued
+  const bool ok = mbar_wait(smem_u32(mbar), 0);
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (!ok) {
     if (g.err && tid == 0) atomicExch(g.err, 3);
@@ -266,8 +266,40 @@ __global__ void __launch_bounds__(kThreads) k_gemm_tn(const __grid_constant__ Ge
 }
 
 size_t gemm_smem(int N, int K) {
-  const size_t opnd = (size_t)(K / 16) * (kTileM + N) * 32, stage = (size_t)kTileM * kSP * 4;
-  return (opnd > stage ? opnd : stage) + 16;
+  const size_t opnd = (size_t)(K / 8) * (kTileM + N) * 16, stage = (size_t)kTileM * kSP * 4;
+  return (opnd > stage ? opnd : stage) + 8 * (1 + kMaxChunks) + 16;
+}
+
+// 2-D tensor map of a row-major BF16 matrix (rows x cols, leading dimension
+// ld elements) read in boxes of box_rows rows x 8 columns (16 bytes)
+typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encode_fn = nullptr;
+
+int make_map(CUtensorMap *map, const bf16 *ptr, int rows, int cols, int ld, int box_rows, std::string &err) {
+  if (!encode_fn) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn ||
+        q != cudaDriverEntryPointSuccess) {
+      err = "gemm: cuTensorMapEncodeTiled is not available";
+      return FS_ERR_CUDA;
+    }
+    encode_fn = (EncodeTiled)fn;
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {8u, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1u, 1u};
+  const CUresult r = encode_fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)ptr, dims, strides, box, estr,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    err = "gemm: tensor map encoding failed (" + std::to_string((int)r) + ")";
+    return FS_ERR_ARG;
+  }
+  return FS_OK;
 }
 
 bool gemm_attr_set = false;
@@ -291,7 +323,11 @@ int gemm(const GemmArgs &g, cudaStream_t st, std::string &err) {
   const int tiles = (g.M + kTileM - 1) / kTileM;
   const int ny = (g.N % 64 == 0 && tiles < 296) ? g.N / 64 : 1;
   const dim3 grid((g.M + kTileM - 1) / kTileM, ny);
-  k_gemm_tn<<<grid, kThreads, gemm_smem(g.N / ny, g.K), st>>>(g);
+  CUtensorMap ta, tb;
+  int rc = make_map(&ta, g.A, g.M, g.K, g.lda, kTileM, err);
+  if (!rc) rc = make_map(&tb, g.B, g.N, g.K, g.ldb, g.N / ny, err);
+  if (rc) return rc;
+  k_gemm_tn<<<grid, kThreads, gemm_smem(g.N / ny, g.K), st>>>(g, ta, tb);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     err = std::string("gemm launch: ") + cudaGetErrorString(e);
