@@ -327,21 +327,32 @@ class Engine:
     def set_injection(self, first: int, count: int, mean: float, std: float):
         _check(lib().fs_set_injection(self._h, first, count, mean, std), self._h)
 
-    def step(self, nsteps: int, want_V: bool = False, spike_cap: Optional[int] = None):
-        """Runs nsteps; returns (list of per-step spike index arrays, V or None)."""
+    def step(self, nsteps: int, want_V: bool = False, spike_cap: Optional[int] = None, want_Irep: bool = False,
+             want_nstate: bool = False):
+        """Runs nsteps; returns (list of per-step spike index arrays, V or
+        None), or with want_Irep / want_nstate (spikes, V, Irep [steps, 5, n]
+        or None, LIF state words [steps, n] or None)."""
         counts = np.zeros(nsteps, np.uint32)
         cap = spike_cap if spike_cap is not None else max(1024, nsteps * self.n)
         idx = np.zeros(cap, np.uint32)
         V = np.zeros((nsteps, self.n), np.float32) if want_V else None
+        I = np.zeros((nsteps, FS_NREC, self.n), np.float32) if want_Irep else None
+        NS = np.zeros((nsteps, self.n), np.uint32) if want_nstate else None
         so = StepOut()
         so.spike_count = counts.ctypes.data_as(_u32)
         so.spike_idx = idx.ctypes.data_as(_u32)
         so.spike_cap = cap
         if V is not None:
             so.V = V.ctypes.data_as(_f)
+        if I is not None:
+            so.Irep = I.ctypes.data_as(_f)
+        if NS is not None:
+            so.nstate = NS.ctypes.data_as(_u32)
         _check(lib().fs_step(self._h, nsteps, C.byref(so)), self._h)
         offs = np.concatenate([[0], np.cumsum(counts.astype(np.int64))])
         spikes = [idx[offs[i]:offs[i + 1]].copy() for i in range(nsteps)]
+        if want_Irep or want_nstate:
+            return spikes, V, I, NS
         return spikes, V
 
     def run(self, nsteps: int):

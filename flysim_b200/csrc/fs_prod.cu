@@ -96,6 +96,9 @@ struct Params {
   int *err;
   unsigned long long *spike_total;  // spikes since reset
   uint32_t *nspk;                   // per-neuron spike counts since reset (or null)
+  float *Irep;                      // [5][n] receptor currents of each neuron's last integrated step
+  float *outI;                      // [steps][5][n] Irep per step (or null)
+  uint32_t *outNS;                  // [steps][n] LIF state word per step (or null)
   float rg[5];                      // synaptic gain per receptor (scales every weight; 1 = as built)
 };
 
@@ -494,6 +497,13 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
         ns &= ~(FS_NS_MEMDV_OVF | FS_NS_MEMDV_UDF);
       }
       V = df * v + ef * I;
+      if (P.outI && own) {  // kept only while requested (code/EqsGnl2.cpp:196-206)
+        P.Irep[p] = (float)Ir0;
+        P.Irep[(size_t)n + p] = (float)Ir1;
+        P.Irep[(size_t)FS_NMDA * n + p] = (float)Ir2;
+        P.Irep[(size_t)FS_ACH * n + p] = (float)Ir3;
+        P.Irep[(size_t)FS_GCL * n + p] = (float)Ir4;
+      }
       if (V > vth) {
         ns |= FS_NS_FIRE;
         fire_now = true;
@@ -511,6 +521,10 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
       }
     }
     if (own && P.outV) P.outV[(size_t)s * n + p] = (float)V;
+    if (own && P.outNS) P.outNS[(size_t)s * n + p] = ns;
+    if (own && P.outI)
+#pragma unroll
+      for (int r = 0; r < 5; r++) P.outI[(size_t)s * 5 * n + (size_t)r * n + p] = P.Irep[(size_t)r * n + p];
     spk = own && (ns & FS_NS_SPIKE) != 0;
     nsp += spk ? 1u : 0u;
     // presynaptic state: increment per spike, then plasticity update
@@ -688,8 +702,9 @@ __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32
   }
 }
 
+// FP32: two blocks per SM (128 registers); FP64 runs one block per SM
 template <class T>
-__global__ void __launch_bounds__(kThreads) k_prod(const __grid_constant__ Params P) {
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) k_prod(const __grid_constant__ Params P) {
   prod_blocks<T>(P, P.block_post[blockIdx.x], P.block_post[blockIdx.x + 1], gridDim.x);
 }
 
@@ -735,8 +750,9 @@ struct Prod {
   uint32_t chunk_steps = 1000;
   // per-launch buffers
   uint32_t *counts = nullptr, *bits = nullptr, *offsets = nullptr, *idx = nullptr;
-  float *outV = nullptr;
-  uint64_t cap_steps = 0, outv_steps = 0;
+  float *outV = nullptr, *outI = nullptr;
+  uint32_t *outNS = nullptr;
+  uint64_t cap_steps = 0, outv_steps = 0, outi_steps = 0, outns_steps = 0;
   unsigned int *bar = nullptr;
   int *err = nullptr;
   unsigned long long *spike_total = nullptr;
@@ -777,7 +793,7 @@ int dup(Prod *p, X **ptr, const X *src, size_t count, cudaStream_t st, std::stri
   return FS_OK;
 }
 
-int ensure_buffers(Prod *p, uint32_t steps, bool wantV, std::string &err) {
+int ensure_buffers(Prod *p, uint32_t steps, bool wantV, bool wantI, bool wantNS, std::string &err) {
   int rc;
   if (steps > p->cap_steps) {
     const uint32_t words = (p->n + 31) / 32;
@@ -790,12 +806,20 @@ int ensure_buffers(Prod *p, uint32_t steps, bool wantV, std::string &err) {
     if ((rc = dal(p, &p->outV, (size_t)steps * p->n, err))) return rc;
     p->outv_steps = steps;
   }
+  if (wantI && steps > p->outi_steps) {
+    if ((rc = dal(p, &p->outI, (size_t)steps * 5 * p->n, err))) return rc;
+    p->outi_steps = steps;
+  }
+  if (wantNS && steps > p->outns_steps) {
+    if ((rc = dal(p, &p->outNS, (size_t)steps * p->n, err))) return rc;
+    p->outns_steps = steps;
+  }
   return FS_OK;
 }
 
 int launch(Prod *p, uint32_t nsteps, bool want_bits, bool wantV, cudaStream_t st, uint64_t *launches,
-           std::string &err) {
-  int rc = ensure_buffers(p, nsteps, wantV, err);
+           std::string &err, bool wantI = false, bool wantNS = false) {
+  int rc = ensure_buffers(p, nsteps, wantV, wantI, wantNS, err);
   if (rc) return rc;
   const uint32_t words = (p->n + 31) / 32;
   cudaError_t e = cudaMemsetAsync(p->counts, 0, (size_t)nsteps * 4, st);
@@ -812,6 +836,8 @@ int launch(Prod *p, uint32_t nsteps, bool want_bits, bool wantV, cudaStream_t st
   P.words = words;
   P.counts = p->counts;
   P.outV = wantV ? p->outV : nullptr;
+  P.outI = wantI ? p->outI : nullptr;
+  P.outNS = wantNS ? p->outNS : nullptr;
   P.bar = p->bar;
   P.err = p->err;
   P.spike_total = p->spike_total;
@@ -1043,6 +1069,7 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
       (rc = dup(p, &P.Cap, (const float *)nullptr, n, st, err)) || (rc = dup(p, &P.Car, (const float *)nullptr, n, st, err)) ||
       (rc = dup(p, &P.tm_u, (const float *)nullptr, n, st, err)) || (rc = dup(p, &P.tm_x, (const float *)nullptr, n, st, err)) ||
       (rc = dup(p, &P.nspk, (const uint32_t *)nullptr, n, st, err)) ||
+      (rc = dup(p, &P.Irep, (const float *)nullptr, (size_t)5 * n, st, err)) ||
       (rc = dup(p, &P.ring, (const unsigned long long *)nullptr, (size_t)std::max<uint32_t>(1, p->nlin) * P.slots * n, st, err)))
     goto fail;
   // edges
@@ -1118,7 +1145,7 @@ int prod_reset(Prod *p, uint32_t seed, cudaStream_t st, std::string &err) {
   };
   z(P.G, 4 * n * T); z(P.ext_st, 4 * n * T); z(P.ext_x, n * T); z(P.ext_s, n * T);
   z(P.st_pre, 4 * n * T); z(P.x_pre, n * T); z(P.s_pre, n * T); z(P.s_hist, (size_t)P.slots * n * T * (p->fp64 ? 1 : kSH));
-  z(P.Count, n * 4); z(P.NS, n * 4); z(P.Cap, n * 4); z(P.Car, n * 4); z(P.nspk, n * 4);
+  z(P.Count, n * 4); z(P.NS, n * 4); z(P.Cap, n * 4); z(P.Car, n * 4); z(P.nspk, n * 4); z(P.Irep, (size_t)5 * n * 4);
   z(P.ring, (size_t)std::max<uint32_t>(1, p->nlin) * P.slots * n * 8);
   z(p->err, 4);
   z(p->spike_total, 8);
@@ -1148,8 +1175,12 @@ int prod_step(Prod *p, uint32_t nsteps, fs_step_out *out, uint64_t *written, cud
   uint32_t done = 0;
   while (done < nsteps) {
     const uint32_t b = std::min(chunk, nsteps - done);
-    const bool wantV = out && out->V;
-    int rc = launch(p, b, true, wantV, st, launches, err);
+    const bool wantV = out && out->V, wantI = out && out->Irep, wantNS = out && out->nstate;
+    if (out && out->gv_n) {
+      err = "production modes aggregate the synapse gates: GatingVariable output needs FS_MODE_COMPAT";
+      return FS_ERR_UNSUPPORTED;
+    }
+    int rc = launch(p, b, true, wantV, st, launches, err, wantI, wantNS);
     if (rc) return rc;
     cudaError_t e = fsd::spikes_compact(p->bits, b, words, p->counts, p->offsets, p->idx, st, launches);
     if (e != cudaSuccess) { err = cudaGetErrorString(e); return FS_ERR_CUDA; }
@@ -1172,9 +1203,13 @@ int prod_step(Prod *p, uint32_t nsteps, fs_step_out *out, uint64_t *written, cud
       e = cudaMemcpy(out->V + (size_t)done * n, p->outV, (size_t)b * n * 4, cudaMemcpyDeviceToHost);
       if (e != cudaSuccess) { err = cudaGetErrorString(e); return FS_ERR_CUDA; }
     }
-    if (out && (out->Irep || out->nstate || out->gv_n)) {
-      err = "production modes return spikes and V only";
-      return FS_ERR_UNSUPPORTED;
+    if (wantI) {
+      e = cudaMemcpy(out->Irep + (size_t)done * 5 * n, p->outI, (size_t)b * 5 * n * 4, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) { err = cudaGetErrorString(e); return FS_ERR_CUDA; }
+    }
+    if (wantNS) {
+      e = cudaMemcpy(out->nstate + (size_t)done * n, p->outNS, (size_t)b * n * 4, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) { err = cudaGetErrorString(e); return FS_ERR_CUDA; }
     }
     *written += total;
     if (spikes_total) *spikes_total += total;

@@ -25,10 +25,14 @@ import numpy as np
 AMPA, GABA, ACH, GCL, NMDA = range(5)
 ACT_INJ, ACT_NMDA = 128, 4
 NS_FIRE, NS_SPIKE = 1, 2
+NS_OVF, NS_UDF = 16, 32
 
 
-def simulate(na, steps: int):
-    """Returns (spikes: list of index arrays per step, V: [steps, n] float64)."""
+def simulate(na, steps: int, extra: bool = False):
+    """Returns (spikes: list of index arrays per step, V: [steps, n] float64)
+    and, with `extra`, also the receptor currents Irep [steps, 5, n] (kept
+    from the last integrated step while a neuron fires,
+    code/EqsGnl2.cpp:196-206) and the LIF state word [steps, n]."""
     f, s = na.fields, na.syn
     n = na.n
     assert not np.any(f["pb"]), "external drive is random: not covered"
@@ -81,6 +85,9 @@ def simulate(na, steps: int):
     spre = np.zeros(n)
     nm = rec == NMDA
     spikes, Vout = [], np.zeros((steps, n))
+    Irep = np.zeros((5, n))
+    Iout = np.zeros((steps, 5, n)) if extra else None
+    NSout = np.zeros((steps, n), np.int64) if extra else None
     for t in range(steps):
         if t >= 1:
             G = dfs[:4] * G + arrive[t - 1]
@@ -95,7 +102,11 @@ def simulate(na, steps: int):
         Ir[NMDA] = g[NMDA] * (vrev[NMDA] - v) / (1.0 + mg * np.exp(-0.062 * v) / 3.57)
         I = Ir.sum(0) + inj * 1e3 + leak
         I = 1e-3 * I / cm
+        ovf, udf = I > dvm, I < -dvm
+        ns = np.where(fire_now, ns, np.where(ovf, (ns | NS_OVF) & ~NS_UDF,
+                                             np.where(udf, (ns & ~NS_OVF) | NS_UDF, ns & ~(NS_OVF | NS_UDF))))
         I = np.clip(I, -dvm, dvm)
+        Irep = np.where(fire_now, Irep, Ir)
         Vi = df * v + ef * I
         crossed = ~fire_now & (Vi > vth)
         V = np.where(fire_now, V, Vi)
@@ -108,6 +119,9 @@ def simulate(na, steps: int):
         cnt = np.where(ref, cnt + 1, np.where(done, 0, cnt))
         ns = np.where(done, ns & ~NS_FIRE, ns)
         Vout[t] = V
+        if extra:
+            Iout[t] = Irep
+            NSout[t] = ns
         spk = (ns & NS_SPIKE) != 0
         spikes.append(np.nonzero(spk)[0].astype(np.uint32))
         inc = np.ones(n)
@@ -128,4 +142,6 @@ def simulate(na, steps: int):
         if spk.any():
             for e in np.nonzero(spk[pre] & ~nm)[0]:
                 arrive[t + dl[e], rec[e], post[e]] += w[e] * cinc[rec[e], pre[e]]
+    if extra:
+        return spikes, Vout, Iout, NSout
     return spikes, Vout

@@ -59,13 +59,17 @@ SMALL = {
 def test_small_network_matches_restatement(built, shape, tm, mode, tol):
     na = _small_net(built, *SMALL[shape], tm=tm)
     steps = 3000
-    ref_sp, ref_V = prod_model.simulate(na, steps)
+    ref_sp, ref_V, ref_I, ref_NS = prod_model.simulate(na, steps, extra=True)
     e = built.Engine(na.desc, mode)
     try:
         e.reset(1)
-        sp, V = e.step(steps, want_V=True)
+        sp, V, I, NS = e.step(steps, want_V=True, want_Irep=True, want_nstate=True)
     finally:
         e.close()
+    # receptor currents (IsynSep output) and the LIF state word (dV overflow output)
+    np.testing.assert_array_equal(NS, ref_NS)
+    scale = np.abs(ref_I).max()
+    assert np.abs(I.astype(np.float64) - ref_I).max() <= 1e-3 * scale, np.abs(I - ref_I).max() / scale
     assert sum(x.size for x in ref_sp) > 20
     for t in range(steps):
         np.testing.assert_array_equal(sp[t], ref_sp[t], err_msg="spikes differ at step %d" % t)
