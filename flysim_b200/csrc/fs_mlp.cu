@@ -265,6 +265,156 @@ __global__ void __launch_bounds__(kThreads) k_gemm_tn(const __grid_constant__ Ge
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(ncols));
 }
 
+// ---- persistent GEMM for many row tiles --------------------------------------
+// One CTA per SM walks row tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...
+// W (the B operand) stays in shared memory; warp 4 (one lane) loads each
+// tile's A by TMA into a single buffer and issues its MMAs into one of two
+// TMEM accumulators, while warps 0-3 drain the other accumulator through the
+// epilogue; so the next tile's loads and MMAs overlap the current epilogue.
+constexpr int kPThreads = 160;
+
+__device__ __forceinline__ bool epi_all(bool v) {  // uniform decision of the 128 epilogue threads
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, 1, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(out)
+      : "r"((uint32_t)v)
+      : "memory");
+  return out != 0;
+}
+
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
+
+__global__ void __launch_bounds__(kPThreads) k_gemm_persist(const __grid_constant__ GemmArgs g,
+                                                            const __grid_constant__ CUtensorMap ta,
+                                                            const __grid_constant__ CUtensorMap tb) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const int K = g.K, N = g.N, nkb = K >> 3;
+  uint8_t *sB = smem;                                   // W: nkb boxes of N rows x 16 B
+  uint8_t *sA = smem + (size_t)nkb * N * 16;            // A: nkb boxes of 128 rows x 16 B
+  float *stg = (float *)(sA + (size_t)nkb * kTileM * 16);  // epilogue staging [128][kSP]
+  uint64_t *bars = (uint64_t *)(stg + kTileM * kSP);    // w, a, full[2], empty[2]
+  uint32_t *tslot = (uint32_t *)(bars + 6);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tiles = (g.M + kTileM - 1) / kTileM;
+  uint32_t ncols = 32;
+  while (ncols < (uint32_t)(2 * N)) ncols <<= 1;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(tslot)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    for (int b = 0; b < 4; b++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bars + b)));
+    for (int b = 4; b < 6; b++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(smem_u32(bars + b)));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tslot;
+  const uint32_t bw = smem_u32(bars), ba = smem_u32(bars + 1);
+  if (warp == 4) {
+    if (lane == 0) {
+      bool ok = true;
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bw),
+                   "r"((uint32_t)(N * K * 2))
+                   : "memory");
+      for (int kb = 0; kb < nkb; kb++) tma_load_2d(smem_u32(sB + (size_t)kb * N * 16), &tb, kb * 8, 0, bw);
+      const uint32_t id = idesc_bf16(kTileM, (uint32_t)N);
+      int i = 0;
+      for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, i++) {
+        const int buf = i & 1;
+        // the A buffer is free once the previous tile's MMAs completed
+        if (i > 0) ok = mbar_wait(smem_u32(bars + 2 + ((i - 1) & 1)), ((i - 1) >> 1) & 1);
+        if (!ok) break;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(ba),
+                     "r"((uint32_t)(kTileM * K * 2))
+                     : "memory");
+        for (int kb = 0; kb < nkb; kb++)
+          tma_load_2d(smem_u32(sA + (size_t)kb * kTileM * 16), &ta, kb * 8, t * kTileM, ba);
+        // this accumulator is free once its tile from two rounds ago was drained
+        if (i >= 2) ok = mbar_wait(smem_u32(bars + 4 + buf), ((i - 2) >> 1) & 1);
+        if (ok) ok = mbar_wait(ba, i & 1);
+        if (ok && i == 0) ok = mbar_wait(bw, 0);
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        for (int sl = 0; sl < (K >> 4); sl++) {
+          const uint64_t ad = sdesc(smem_u32(sA + (size_t)(2 * sl) * kTileM * 16), kTileM * 16, 128);
+          const uint64_t bd = sdesc(smem_u32(sB + (size_t)(2 * sl) * N * 16), (uint32_t)N * 16, 128);
+          mma_bf16(tmem + (uint32_t)(buf * N), ad, bd, id, sl > 0 ? 1u : 0u);
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                         smem_u32(bars + 2 + buf))
+                     : "memory");
+      }
+      if (!ok && g.err) atomicExch(g.err, 5);
+    }
+  } else {
+    // epilogue warps 0-3: thread tid owns accumulator row tid
+    int i = 0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x, i++) {
+      const int buf = i & 1;
+      const bool ok = epi_all(mbar_wait(smem_u32(bars + 2 + buf), (i >> 1) & 1));
+      if (!ok) {
+        if (tid == 0 && g.err) atomicExch(g.err, 3);
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const int m0 = t * kTileM, rows = min(kTileM, g.M - m0);
+      for (int cc = 0; cc < N; cc += kCW) {
+        const int cw = min(kCW, N - cc);
+        for (int c0 = 0; c0 < cw; c0 += 16) {
+          uint32_t v[16];
+          tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * N + cc + c0), v);
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            float x = __uint_as_float(v[j]);
+            if (g.bias) x += g.bias[cc + c0 + j];
+            if (g.relu) x = fmaxf(x, 0.0f);
+            stg[tid * kSP + c0 + j] = x;
+          }
+        }
+        epi_sync();
+        const int c8 = cw >> 3;
+        for (int k = tid; k < rows * c8; k += 128) {
+          const int r = k / c8, c = (k - r * c8) * 8;
+          float x[8];
+#pragma unroll
+          for (int j = 0; j < 8; j++) x[j] = stg[r * kSP + c + j];
+          const size_t gc = (size_t)cc + c;
+          if (g.Cf) {
+            float4 *dst = (float4 *)(g.Cf + (size_t)(m0 + r) * g.ldcf + gc);
+            dst[0] = make_float4(x[0], x[1], x[2], x[3]);
+            dst[1] = make_float4(x[4], x[5], x[6], x[7]);
+          }
+          if (g.Cb) {
+            uint4 o;
+            bf16 *ob = (bf16 *)&o;
+#pragma unroll
+            for (int j = 0; j < 8; j++) ob[j] = __float2bfloat16_rn(x[j]);
+            *(uint4 *)(g.Cb + (size_t)(m0 + r) * g.ldcb + gc) = o;
+          }
+        }
+        epi_sync();
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bars + 4 + buf)) : "memory");
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(ncols));
+}
+
+size_t persist_smem(int N, int K) {
+  return (size_t)(K / 8) * (N + kTileM) * 16 + (size_t)kTileM * kSP * 4 + 6 * 8 + 16;
+}
+
 size_t gemm_smem(int N, int K) {
   const size_t opnd = (size_t)(K / 8) * (kTileM + N) * 16, stage = (size_t)kTileM * kSP * 4;
   return (opnd > stage ? opnd : stage) + 8 * (1 + kMaxChunks) + 16;
@@ -321,6 +471,28 @@ int gemm(const GemmArgs &g, cudaStream_t st, std::string &err) {
   // column tiles of 64 when there are few row tiles (training batches), so
   // that small-M GEMMs still spread over the SMs; one column tile otherwise
   const int tiles = (g.M + kTileM - 1) / kTileM;
+  static int sms = 0;
+  if (!sms && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0) != cudaSuccess) sms = 148;
+  // many row tiles, plain outputs: the persistent kernel (W resident, the
+  // next tile's loads and MMAs overlapping the current epilogue)
+  if (!g.mask && !g.Ct && tiles >= 2 * sms && persist_smem(g.N, g.K) <= 232448) {
+    static bool pattr = false;
+    if (!pattr) {
+      cudaFuncSetAttribute(k_gemm_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
+      pattr = true;
+    }
+    CUtensorMap ta, tb;
+    int rc = make_map(&ta, g.A, g.M, g.K, g.lda, kTileM, err);
+    if (!rc) rc = make_map(&tb, g.B, g.N, g.K, g.ldb, g.N, err);
+    if (rc) return rc;
+    k_gemm_persist<<<std::min(tiles, sms), kPThreads, persist_smem(g.N, g.K), st>>>(g, ta, tb);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      err = std::string("gemm launch: ") + cudaGetErrorString(e);
+      return FS_ERR_CUDA;
+    }
+    return FS_OK;
+  }
   const int ny = (g.N % 64 == 0 && tiles < 296) ? g.N / 64 : 1;
   const dim3 grid((g.M + kTileM - 1) / kTileM, ny);
   CUtensorMap ta, tb;

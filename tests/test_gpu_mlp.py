@@ -104,3 +104,22 @@ def test_training_reduces_loss(built):
         assert acc > 0.85, acc
     finally:
         net.close()
+
+
+def test_large_inference_matches_oracle(built):
+    # 40,000 rows = 313 row tiles: the persistent kernel (W resident, two TMEM
+    # accumulators alternating, ragged last tile)
+    rng = np.random.default_rng(4)
+    net = built.Mlp(DIMS, seed=8)
+    try:
+        x, _ = _data(rng, 40000)
+        y = net.forward(x)
+        ref, _ = mo.forward(net.get_params(), DIMS, x.astype(np.float64))
+        rel = np.linalg.norm(y - ref) / np.linalg.norm(ref)
+        assert rel < 1e-2, rel
+        # rows across the tile boundaries agree with a small (non-persistent) call
+        for lo in (0, 127, 38656, 39936):
+            ys = net.forward(x[lo:lo + 64])
+            np.testing.assert_array_equal(ys, y[lo:lo + 64])
+    finally:
+        net.close()
