@@ -270,6 +270,67 @@ __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint
   }
 }
 
+// Single-step batches (networks whose minimum delay is 0 or 1 step pull
+// every step): each edge needs one value, so a warp takes four posts at
+// once with scalar loads, four times the loads in flight of the general
+// path.  Per post and lane the edges are summed in the same order as there
+// (lane-strided rounds of 32 x 4), then the same butterfly.
+__device__ __forceinline__ void nmda_pull1_f32(const Params &P, uint32_t p0, uint32_t np, uint64_t tb,
+                                               float (*gn)[kTile], uint32_t wid, uint32_t lane) {
+  constexpr int PG = 4;             // posts per warp at once
+  constexpr int U = 4;              // edges per lane per post and round
+  constexpr uint32_t CH = 32u * U;  // edges of a post per round
+  const float *sh = (const float *)P.s_hist;
+  const uint32_t S = P.slots, mask = P.mask;
+  const uint32_t nw = kThreads / 32;
+  if (!P.in_row) {
+    for (uint32_t q = wid * 32 + lane; q < np; q += nw * 32) gn[0][q] = 0.0f;
+    return;
+  }
+  for (uint32_t q0 = wid * PG; q0 < np; q0 += nw * PG) {
+    uint32_t bb[PG + 1];
+#pragma unroll
+    for (int k = 0; k <= PG; k++) bb[k] = __ldg(P.in_row + p0 + min(q0 + k, np));
+    uint32_t nch = 0;
+#pragma unroll
+    for (int k = 0; k < PG; k++) nch = max(nch, (bb[k + 1] - bb[k] + CH - 1) / CH);
+    float acc[PG];
+#pragma unroll
+    for (int k = 0; k < PG; k++) acc[k] = 0.0f;
+    for (uint32_t c = 0; c < nch; c++) {
+      uint32_t code[PG][U];
+      float w[PG][U], v[PG][U];
+#pragma unroll
+      for (int k = 0; k < PG; k++)
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const uint32_t e = bb[k] + c * CH + lane + 32u * u;
+          const bool ok = e < bb[k + 1];
+          code[k][u] = ok ? __ldg(P.in_code + e) : 0u;
+          w[k][u] = ok ? __ldg(P.in_w + e) : 0.0f;
+        }
+#pragma unroll
+      for (int k = 0; k < PG; k++)
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const uint32_t e = bb[k] + c * CH + lane + 32u * u;
+          const uint32_t pre = code[k][u] & 0xffffffu, d = code[k][u] >> 24;
+          // row 0 of the shifted copies holds slot i at element i
+          v[k][u] = e < bb[k + 1] ? __ldca(sh + (size_t)pre * kSH * S + ((uint32_t)(tb - 1u - d) & mask)) : 0.0f;
+        }
+#pragma unroll
+      for (int k = 0; k < PG; k++)
+#pragma unroll
+        for (int u = 0; u < U; u++) acc[k] += w[k][u] * v[k][u];
+    }
+#pragma unroll
+    for (int k = 0; k < PG; k++) {
+      const float sum = warp_sum<float>(acc[k]);
+      if (lane == 0 && q0 + k < np) gn[0][q0 + k] = sum;
+    }
+  }
+}
+
 template <class T>
 __device__ __forceinline__ void nmda_pull(const Params &P, uint32_t p0, uint32_t np, uint64_t tb, uint32_t L,
                                           T (*gn)[TileW<T>::W], uint32_t wid, uint32_t lane) {
@@ -665,7 +726,10 @@ __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32
       const uint32_t L = min(kLB, iv_end - bs);
       for (uint32_t tp0 = B0; tp0 < B1; tp0 += kT) {
         const uint32_t np = min(kT, B1 - tp0);
-        if constexpr (sizeof(T) == 4) nmda_pull_f32(P, tp0, np, P.t0 + bs, L, (float (*)[kTile])gn, wid, lane);
+        if constexpr (sizeof(T) == 4) {
+          if (L == 1) nmda_pull1_f32(P, tp0, np, P.t0 + bs, (float (*)[kTile])gn, wid, lane);
+          else nmda_pull_f32(P, tp0, np, P.t0 + bs, L, (float (*)[kTile])gn, wid, lane);
+        }
         else nmda_pull<T>(P, tp0, np, P.t0 + bs, L, gn, wid, lane);
         draw_inputs<T>(P, tp0, np, P.t0 + bs, L, hits, gauss);
         __syncthreads();
