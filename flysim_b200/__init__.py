@@ -137,6 +137,9 @@ def lib() -> C.CDLL:
         "fs_get_state": (C.c_int, [vp, _f, _i32, _u32]),
         "fs_get_syn_state": (C.c_int, [vp, _f, _f]),
         "fs_model_load": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(ModelOpts), C.POINTER(vp)]),
+        "fs_model_load_cached": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(ModelOpts), C.c_char_p,
+                                          C.POINTER(vp), C.POINTER(C.c_int)]),
+        "fs_model_confs_info": (C.c_int, [vp, C.c_char_p]),
         "fs_model_free": (C.c_int, [vp]),
         "fs_model_error": (C.c_char_p, []),
         "fs_model_desc": (C.c_int, [vp, C.POINTER(C.POINTER(NetDesc))]),
@@ -186,7 +189,8 @@ def exported_symbols() -> Sequence[str]:
                         "fs_run_timed",
                         "fs_sync", "fs_stats", "fs_kernel_time", "fs_debug_expf", "fs_debug_expf_noalloc",
                         "fs_get_state",
-                        "fs_get_syn_state", "fs_model_load", "fs_model_free", "fs_model_error",
+                        "fs_get_syn_state", "fs_model_load", "fs_model_load_cached", "fs_model_confs_info",
+                        "fs_model_free", "fs_model_error",
                         "fs_model_desc", "fs_model_info", "fs_model_seed", "fs_model_run",
                         "fs_model_run_with", "fs_device_engine", "fs_spike_counts", "fs_batch_create",
                         "fs_batch_destroy", "fs_batch_error", "fs_batch_reset", "fs_batch_tune", "fs_batch_run",
@@ -211,11 +215,19 @@ def device_count() -> int:
 
 # ---------------------------------------------------------------------------
 class Model:
-    """A parsed and built network (Parser + SetPp of the reference)."""
+    """A parsed and built network (Parser + SetPp of the reference).
+
+    cache: path of a binary network cache; the model is read from it when it
+    was written for the same .conf/.pro bytes and options, else parsed, built
+    and stored there.  cache_status is then "hit", "stored" or "unwritable"
+    ("off" without a cache)."""
+
+    CACHE_STATUS = {0: "off", 1: "hit", 2: "stored", 3: "unwritable"}
 
     def __init__(self, conf: str, pro: str, dt: float = 0.1, stp: bool = False, std: bool = False,
                  ltp: bool = False, repeats: int = 1, threads: int = 1, user_seed: Optional[int] = None,
-                 out_mem: Optional[str] = None, out_spike: Optional[str] = None, out_rate: Optional[str] = None):
+                 out_mem: Optional[str] = None, out_spike: Optional[str] = None, out_rate: Optional[str] = None,
+                 cache: Optional[str] = None):
         L = lib()
         o = ModelOpts()
         o.dt = dt
@@ -228,11 +240,14 @@ class Model:
         o.out_spike = out_spike.encode() if out_spike else None
         o.out_rate = out_rate.encode() if out_rate else None
         h = C.c_void_p()
-        rc = L.fs_model_load(conf.encode(), pro.encode(), C.byref(o), C.byref(h))
+        st = C.c_int(0)
+        rc = L.fs_model_load_cached(conf.encode(), pro.encode(), C.byref(o), cache.encode() if cache else None,
+                                    C.byref(h), C.byref(st))
         if rc != FS_OK:
             raise FsError(rc, L.fs_model_error().decode(errors="replace"))
         self._h = h
         self.dt = dt
+        self.cache_status = self.CACHE_STATUS.get(st.value, str(st.value))
 
     def close(self):
         if getattr(self, "_h", None):
@@ -259,6 +274,12 @@ class Model:
         s = C.c_uint64()
         _check(lib().fs_model_info(self._h, C.byref(a), C.byref(b), C.byref(s), C.byref(d), C.byref(e)))
         return dict(neurons=a.value, populations=b.value, synapses=s.value, events=d.value, outputs=e.value)
+
+    def confs_info(self, path: str) -> None:
+        """Writes ConfsInfo.log (Parser::ConfsInfo, code/parser.cpp:1488-1631)."""
+        rc = lib().fs_model_confs_info(self._h, path.encode())
+        if rc != FS_OK:
+            raise FsError(rc, lib().fs_model_error().decode(errors="replace"))
 
     def seed(self, repeat: int = 1) -> int:
         v = C.c_uint32()

@@ -2,7 +2,9 @@
 // as the reference CLI (code/main.cpp:26-256): reads network.conf and
 // network.pro, writes the output files named in the .pro (and ConfsInfo.log).
 // Extra options: -mode compat|fp32|fp64 (default compat: the reference's
-// raster bit for bit), -gpu N (CUDA device), -chunk N (steps per launch batch).
+// raster bit for bit), -gpu N (CUDA device), -chunk N (steps per launch batch),
+// -cache FILE (binary network cache: a rerun on unchanged files skips parsing
+// and building).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -26,12 +28,13 @@ static void usage() {
       "-STP / -STD / -LTP    # short-term / depression-only / long-term plasticity\n"
       "-nmodel GNL2          # accepted and ignored (GNL2 is the only model)\n"
       "-mode compat|fp32|fp64 # numeric mode (default compat)\n"
-      "-gpu 0                # CUDA device\n");
+      "-gpu 0                # CUDA device\n"
+      "-cache net.cache      # binary network cache (reused while .conf/.pro/options are unchanged)\n");
 }
 
 int main(int argc, char **argv) {
   std::string conf = "network.conf", pro = "network.pro";
-  std::string om, os, orr;
+  std::string om, os, orr, cache;
   fs_model_opts mo{};
   mo.dt = 0.1f;
   mo.threads = 1;
@@ -61,6 +64,7 @@ int main(int argc, char **argv) {
     else if (a == "-LTP") mo.flags |= FS_ACT_LTP;
     else if (a == "-gpu") ro.device = std::atoi(val());
     else if (a == "-chunk") ro.chunk_steps = (uint32_t)std::atoi(val());
+    else if (a == "-cache") cache = val();
     else if (a == "-mode") {
       std::string v = val();
       if (v == "compat") ro.mode = FS_MODE_COMPAT;
@@ -77,11 +81,16 @@ int main(int argc, char **argv) {
   if (!os.empty()) mo.out_spike = os.c_str();
   if (!orr.empty()) mo.out_rate = orr.c_str();
   fs_model *m = nullptr;
-  int rc = fs_model_load(conf.c_str(), pro.c_str(), &mo, &m);
+  int cache_status = FS_CACHE_OFF;
+  int rc = fs_model_load_cached(conf.c_str(), pro.c_str(), &mo, cache.c_str(), &m, &cache_status);
   if (rc) {
     std::fprintf(stderr, "flysim: %s\n", fs_model_error());
     return 1;
   }
+  if (cache_status == FS_CACHE_HIT) std::printf("network read from cache %s\n", cache.c_str());
+  else if (cache_status == FS_CACHE_UNWRITABLE) std::fprintf(stderr, "flysim: %s\n", fs_model_error());
+  // main.cpp:247 writes ConfsInfo.log after parsing, before the network is set up
+  if (fs_model_confs_info(m, "ConfsInfo.log")) std::fprintf(stderr, "flysim: %s\n", fs_model_error());
   uint32_t nn = 0;
   uint64_t ns = 0;
   fs_model_info(m, &nn, nullptr, &ns, nullptr, nullptr);

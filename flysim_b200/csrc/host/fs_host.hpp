@@ -132,8 +132,13 @@ void parse_conf(Model &m, const std::string &path, int &state);
 void parse_macros(Model &m, const std::string &path, int &state);
 void parse_pro(Model &m, const std::string &path, int &state);
 void add_command_outputs(Model &m);
-void write_confs_info(const Model &m, const std::string &path);
+bool write_confs_info(const Model &m, const std::string &path);
 void build_network(Model &m);
+
+// Binary network cache (fs_cache.cpp).
+bool cache_key(const char *conf, const char *pro, const fs_model_opts &o, uint64_t &key);
+bool cache_read(const std::string &path, uint64_t key, Model &m);
+bool cache_write(const std::string &path, uint64_t key, Model &m, std::string &err);
 
 // Protocol driver: NetSimGnl2::Run/DoEvt/FileOut over any engine.
 int run_protocol(Model &m, const fs_engine_vtbl *eng, void *ctx, const std::string &out_dir,

@@ -20,6 +20,12 @@ const char *fs_model_error(void) { return g_model_err.c_str(); }
 // main.cpp:216-249 order: CSta, parse(conf), Comm, DefMacro, parse(pro), SetPp.
 int fs_model_load(const char *conf_path, const char *pro_path, const fs_model_opts *opts,
                   fs_model **out) {
+  return fs_model_load_cached(conf_path, pro_path, opts, nullptr, out, nullptr);
+}
+
+int fs_model_load_cached(const char *conf_path, const char *pro_path, const fs_model_opts *opts,
+                         const char *cache_path, fs_model **out, int *cache_status) {
+  if (cache_status) *cache_status = FS_CACHE_OFF;
   if (!conf_path || !pro_path || !out) {
     g_model_err = "fs_model_load: null argument";
     return FS_ERR_ARG;
@@ -36,37 +42,69 @@ int fs_model_load(const char *conf_path, const char *pro_path, const fs_model_op
   if (!(o.dt > 0.0f)) o.dt = 0.1f;
   if (o.threads < 1) o.threads = 1;
   if (o.repeats < 1) o.repeats = 1;
-  m.opts = o;
-  m.dt = o.dt;
+  uint64_t key = 0;
+  bool use_cache = cache_path && *cache_path && fsh::cache_key(conf_path, pro_path, o, key);
+  if (use_cache && fsh::cache_read(cache_path, key, m)) {
+    m.opts.out_mem = m.opts.out_spike = m.opts.out_rate = nullptr;
+    if (cache_status) *cache_status = FS_CACHE_HIT;
+    *out = fm;
+    return FS_OK;
+  }
+  if (use_cache) {  // a miss may have left part of a damaged file in m
+    delete fm;
+    fm = new (std::nothrow) fs_model();
+    if (!fm) return FS_ERR_NOMEM;
+  }
+  fsh::Model &mm = fm->m;
+  mm.opts = o;
+  mm.dt = o.dt;
   // GetNewSim's ActCtr and the CLI flags (code/main.cpp:220-231, :263)
-  m.act_ctr = FS_ACT_AMPA | FS_ACT_GABA | FS_ACT_NMDA | FS_ACT_ACH | FS_ACT_GCL | FS_ACT_GAP | FS_ACT_LIF;
-  if (o.user_seed_set) m.act_ctr |= FS_ACT_STD;  // UDFRDSEED_ACT == STD_ACT
-  else m.act_ctr &= ~FS_ACT_STD;
-  m.act_ctr |= (o.flags & (FS_ACT_STP | FS_ACT_STD | FS_ACT_LTP));
-  if (o.out_mem) { m.comm_mem = true; m.out_mem = o.out_mem; }
-  if (o.out_spike) { m.comm_spike = true; m.out_spike = o.out_spike; }
-  if (o.out_rate) { m.comm_rate = true; m.out_rate = o.out_rate; }
+  mm.act_ctr = FS_ACT_AMPA | FS_ACT_GABA | FS_ACT_NMDA | FS_ACT_ACH | FS_ACT_GCL | FS_ACT_GAP | FS_ACT_LIF;
+  if (o.user_seed_set) mm.act_ctr |= FS_ACT_STD;  // UDFRDSEED_ACT == STD_ACT
+  else mm.act_ctr &= ~FS_ACT_STD;
+  mm.act_ctr |= (o.flags & (FS_ACT_STP | FS_ACT_STD | FS_ACT_LTP));
+  if (o.out_mem) { mm.comm_mem = true; mm.out_mem = o.out_mem; }
+  if (o.out_spike) { mm.comm_spike = true; mm.out_spike = o.out_spike; }
+  if (o.out_rate) { mm.comm_rate = true; mm.out_rate = o.out_rate; }
   try {
     int state = 0;
-    fsh::parse_conf_counts(m, conf_path, state);
-    fsh::parse_conf(m, conf_path, state);
-    fsh::add_command_outputs(m);
-    fsh::parse_macros(m, pro_path, state);
-    fsh::parse_pro(m, pro_path, state);
-    fsh::build_network(m);
+    fsh::parse_conf_counts(mm, conf_path, state);
+    fsh::parse_conf(mm, conf_path, state);
+    fsh::add_command_outputs(mm);
+    fsh::parse_macros(mm, pro_path, state);
+    fsh::parse_pro(mm, pro_path, state);
+    fsh::build_network(mm);
   } catch (const std::exception &e) {
     g_model_err = e.what();
     delete fm;
     return FS_ERR_PARSE;
   }
   // keep views valid for the model's life; options strings are not kept
-  m.opts.out_mem = m.opts.out_spike = m.opts.out_rate = nullptr;
+  mm.opts.out_mem = mm.opts.out_spike = mm.opts.out_rate = nullptr;
+  if (use_cache) {
+    std::string err;
+    bool stored = fsh::cache_write(cache_path, key, mm, err);
+    if (!stored) g_model_err = err;
+    if (cache_status) *cache_status = stored ? FS_CACHE_STORED : FS_CACHE_UNWRITABLE;
+  } else if (cache_path && *cache_path) {
+    if (cache_status) *cache_status = FS_CACHE_UNWRITABLE;
+    g_model_err = "network cache: cannot read the .conf or .pro for the cache key";
+  }
   *out = fm;
   return FS_OK;
 }
 
 int fs_model_free(fs_model *m) {
   delete m;
+  return FS_OK;
+}
+
+int fs_model_confs_info(fs_model *m, const char *path) {
+  if (!m || !path) return FS_ERR_ARG;
+  if (!fsh::write_confs_info(m->m, path)) {
+    g_model_err = std::string("cannot write ") + path;
+    return FS_ERR_IO;
+  }
   return FS_OK;
 }
 

@@ -583,9 +583,9 @@ static const char *rep_name(uint8_t kw, bool with_gap) {
 
 // Parser::ConfsInfo (code/parser.cpp:1488-1631): ConfsInfo.log.  The
 // Hodgkin-Huxley block prints the reference's defaults (HH is not simulated).
-void write_confs_info(const Model &m, const std::string &path) {
+bool write_confs_info(const Model &m, const std::string &path) {
   std::ofstream o(path.c_str());
-  if (!o) return;
+  if (!o) return false;
   o << "configuration information:----------------------------------------\n";
   for (uint32_t i = 0; i < m.pops.size(); i++) {
     const Pop &p = m.pops[i];
@@ -617,6 +617,7 @@ void write_confs_info(const Model &m, const std::string &path) {
     }
     o << "------------------------------------------------------------------" << std::endl;
   }
+  return bool(o);
 }
 
 }  // namespace fsh

@@ -269,8 +269,23 @@ typedef struct fs_model_opts {
 } fs_model_opts;
 
 int fs_model_load(const char *conf_path, const char *pro_path, const fs_model_opts *opts, fs_model **out);
+/* fs_model_load through a binary network cache at cache_path (no
+ * counterpart in the reference, which parses and builds from text on every
+ * run, code/main.cpp:216-249).  The cache is keyed by the bytes of both files
+ * and by opts: when the key matches, the model is read back without parsing
+ * or building; otherwise the files are parsed and built and the cache is
+ * (re)written.  A cache that cannot be written does not fail the load.
+ * cache_status (may be NULL) receives one of FS_CACHE_*.  cache_path NULL or
+ * "" behaves as fs_model_load. */
+enum { FS_CACHE_OFF = 0, FS_CACHE_HIT = 1, FS_CACHE_STORED = 2, FS_CACHE_UNWRITABLE = 3 };
+int fs_model_load_cached(const char *conf_path, const char *pro_path, const fs_model_opts *opts,
+                         const char *cache_path, fs_model **out, int *cache_status);
 int fs_model_free(fs_model *m);
 const char *fs_model_error(void);
+/* Writes ConfsInfo.log for the parsed model (Parser::ConfsInfo,
+ * code/parser.cpp:1488-1631); the reference CLI writes it on every run
+ * (code/main.cpp:247). */
+int fs_model_confs_info(fs_model *m, const char *path);
 /* View of the built network (valid until fs_model_free). */
 int fs_model_desc(fs_model *m, const fs_net_desc **desc);
 int fs_model_info(fs_model *m, uint32_t *n_neurons, uint32_t *n_pops, uint64_t *n_syn_entries,

@@ -59,8 +59,19 @@ def model_for(fb, case, **kw):
 
 
 def golden_outputs(case):
+    """The output files of a case (its inputs and the log digests excluded)."""
     d = os.path.join(GOLDEN, case)
-    return sorted(f for f in os.listdir(d) if f not in ("net.conf", "net.pro", "cmd.json"))
+    return sorted(f for f in os.listdir(d) if f not in ("net.conf", "net.pro", "cmd.json", "logs.json"))
+
+
+def golden_log_digest(case, name):
+    return json.load(open(os.path.join(GOLDEN, case, "logs.json")))[name]
+
+
+def file_digest(path):
+    import hashlib
+    data = open(path, "rb").read()
+    return {"bytes": len(data), "sha256": hashlib.sha256(data).hexdigest()}
 
 
 def compare_outputs(case, out_dir):

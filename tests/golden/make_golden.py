@@ -5,17 +5,21 @@ The reference is built from its own sources by oracle/Makefile.ref into
 oracle/_ref/flysim_ref (this needs the reference tree, so it runs only where
 the sources are; the fixtures are committed).  Each case directory holds
 net.conf, net.pro, cmd (the reference's extra command-line flags) and the
-reference's output files.
+reference's output files; the two log files it writes on every run
+(ConfsInfo.log, network.log) are recorded as size and SHA-256 in logs.json.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py              # all cases from scratch
+    python tests/golden/make_golden.py --logs-only  # logs.json of the committed cases
 """
 from __future__ import annotations
 
+import hashlib
 import json
 import os
 import shutil
 import subprocess
 import sys
+import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
@@ -121,9 +125,44 @@ def cases():
     return c
 
 
+LOGS = ("ConfsInfo.log", "network.log")
+
+
+def record_logs(d):
+    """Replaces the reference's log files in d by their digests (logs.json)."""
+    rec = {}
+    for f in LOGS:
+        p = os.path.join(d, f)
+        data = open(p, "rb").read()
+        rec[f] = {"bytes": len(data), "sha256": hashlib.sha256(data).hexdigest()}
+        os.remove(p)
+    with open(os.path.join(d, "logs.json"), "w") as f:
+        json.dump(rec, f, indent=1, sort_keys=True)
+
+
+def logs_only():
+    for name in sorted(os.listdir(HERE)):
+        d = os.path.join(HERE, name)
+        if not os.path.isfile(os.path.join(d, "cmd.json")):
+            continue
+        flags = json.load(open(os.path.join(d, "cmd.json")))
+        with tempfile.TemporaryDirectory() as t:
+            for f in ("net.conf", "net.pro"):
+                shutil.copy(os.path.join(d, f), t)
+            r = subprocess.run([REF, "-conf", "net.conf", "-pro", "net.pro"] + flags, cwd=t,
+                               capture_output=True, text=True)
+            if r.returncode != 0:
+                sys.exit("reference failed on %s: %s" % (name, r.stderr[-400:]))
+            record_logs(t)
+            shutil.copy(os.path.join(t, "logs.json"), d)
+        print(name, open(os.path.join(d, "logs.json")).read().replace("\n", " "))
+
+
 def main():
     if not os.path.exists(REF):
         sys.exit("reference binary missing: build it with  make -f oracle/Makefile.ref")
+    if "--logs-only" in sys.argv:
+        return logs_only()
     for name, cs in cases().items():
         d = os.path.join(HERE, name)
         shutil.rmtree(d, ignore_errors=True)
@@ -136,11 +175,8 @@ def main():
                            capture_output=True, text=True)
         if r.returncode != 0:
             sys.exit("reference failed on %s: %s" % (name, r.stderr[-400:]))
-        for junk in ("network.log", "ConfsInfo.log"):
-            p = os.path.join(d, junk)
-            if os.path.exists(p):
-                os.remove(p)
-        outs = sorted(f for f in os.listdir(d) if f not in ("net.conf", "net.pro", "cmd.json"))
+        record_logs(d)
+        outs = sorted(f for f in os.listdir(d) if f not in ("net.conf", "net.pro", "cmd.json", "logs.json"))
         print(name, outs)
 
 
