@@ -140,6 +140,7 @@ def lib() -> C.CDLL:
         "fs_model_load_cached": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(ModelOpts), C.c_char_p,
                                           C.POINTER(vp), C.POINTER(C.c_int)]),
         "fs_model_confs_info": (C.c_int, [vp, C.c_char_p]),
+        "fs_model_network_log": (C.c_int, [vp, C.c_char_p]),
         "fs_model_free": (C.c_int, [vp]),
         "fs_model_error": (C.c_char_p, []),
         "fs_model_desc": (C.c_int, [vp, C.POINTER(C.POINTER(NetDesc))]),
@@ -189,7 +190,7 @@ def exported_symbols() -> Sequence[str]:
                         "fs_run_timed",
                         "fs_sync", "fs_stats", "fs_kernel_time", "fs_debug_expf", "fs_debug_expf_noalloc",
                         "fs_get_state",
-                        "fs_get_syn_state", "fs_model_load", "fs_model_load_cached", "fs_model_confs_info",
+                        "fs_get_syn_state", "fs_model_load", "fs_model_load_cached", "fs_model_confs_info", "fs_model_network_log",
                         "fs_model_free", "fs_model_error",
                         "fs_model_desc", "fs_model_info", "fs_model_seed", "fs_model_run",
                         "fs_model_run_with", "fs_device_engine", "fs_spike_counts", "fs_batch_create",
@@ -278,6 +279,12 @@ class Model:
     def confs_info(self, path: str) -> None:
         """Writes ConfsInfo.log (Parser::ConfsInfo, code/parser.cpp:1488-1631)."""
         rc = lib().fs_model_confs_info(self._h, path.encode())
+        if rc != FS_OK:
+            raise FsError(rc, lib().fs_model_error().decode(errors="replace"))
+
+    def network_log(self, path: str) -> None:
+        """Writes network.log (NetSimGnl2::logDataWrite, code/NetSimGnl2_info.cpp:93-546)."""
+        rc = lib().fs_model_network_log(self._h, path.encode())
         if rc != FS_OK:
             raise FsError(rc, lib().fs_model_error().decode(errors="replace"))
 

@@ -28,7 +28,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 HOST_SRC = ["host/fs_parse.cpp", "host/fs_build.cpp", "host/fs_driver.cpp", "host/fs_model_api.cpp",
-            "host/fs_tables.cpp", "host/fs_cache.cpp"]
+            "host/fs_tables.cpp", "host/fs_cache.cpp", "host/fs_netlog.cpp"]
 CU_SRC = {"fs_engine.cu": [], "fs_prod.cu": [], "fs_compat.cu": ["-fmad=false"], "fs_mlp.cu": []}
 HDRS = ["fs_device.cuh", "fs_prod.cuh", "host/fs_host.hpp"]
 

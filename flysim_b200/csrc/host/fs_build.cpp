@@ -296,6 +296,9 @@ void build_network(Model &m) {
       cnt[seg_post[s] + 1] += seg[r][s].second - seg[r][s].first + 1;
     for (uint32_t i = 0; i < n; i++) cnt[i + 1] += cnt[i];
     ra.gather_rowptr = cnt;
+    ra.seg_post = seg_post;
+    ra.seg_len.resize(seg[r].size());
+    for (size_t s = 0; s < seg[r].size(); s++) ra.seg_len[s] = seg[r][s].second - seg[r][s].first + 1;
     ra.gather_gate.assign(cnt[n], 0);
     std::vector<uint32_t> fillp(cnt.begin(), cnt.end() - 1);
     for (size_t s = 0; s < seg[r].size(); s++) {
@@ -372,6 +375,15 @@ void build_network(Model &m) {
   }
   std::sort(sgap.begin(), sgap.end(), [](const SynRec &a, const SynRec &b) { return a.post < b.post; });
   total += sgap.size();
+  net.gap1_pre.resize(sgap.size());
+  net.gap1_post.resize(sgap.size());
+  net.gap1_g.resize(sgap.size());
+  for (size_t e = 0; e < sgap.size(); e++) {
+    net.gap1_pre[e] = sgap[e].pre;
+    net.gap1_post[e] = sgap[e].post;
+    net.gap1_g[e] = sgap[e].g;
+  }
+  net.gap_ngroup.clear();
   net.total_synapses = total;
 
   // ---- gap-junction terms per neuron, in accumulation order ----
@@ -387,6 +399,8 @@ void build_network(Model &m) {
     if (any) {
       terms.assign(n, {});
       for (const SynIdx &e : tgap) terms[e.post].push_back({gap_gate_pre[e.pre], gap_gate_g[e.pre]});
+      net.gap_ngroup.resize(n);
+      for (uint32_t i = 0; i < n; i++) net.gap_ngroup[i] = (uint32_t)terms[i].size();
       for (const SynRec &e : sgap) terms[e.post].push_back({e.pre, e.g});
       std::vector<std::vector<uint32_t>> by_pre(n);
       for (uint32_t e = 0; e < sgap.size(); e++) {

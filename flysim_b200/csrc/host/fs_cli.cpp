@@ -1,10 +1,11 @@
 // flysim — command line of the B200 drop-in.  Same options and file contract
 // as the reference CLI (code/main.cpp:26-256): reads network.conf and
-// network.pro, writes the output files named in the .pro (and ConfsInfo.log).
+// network.pro, writes the output files named in the .pro, ConfsInfo.log and
+// network.log.
 // Extra options: -mode compat|fp32|fp64 (default compat: the reference's
 // raster bit for bit), -gpu N (CUDA device), -chunk N (steps per launch batch),
 // -cache FILE (binary network cache: a rerun on unchanged files skips parsing
-// and building).
+// and building), -nolog (skip network.log, a text copy of every synapse).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -29,7 +30,8 @@ static void usage() {
       "-nmodel GNL2          # accepted and ignored (GNL2 is the only model)\n"
       "-mode compat|fp32|fp64 # numeric mode (default compat)\n"
       "-gpu 0                # CUDA device\n"
-      "-cache net.cache      # binary network cache (reused while .conf/.pro/options are unchanged)\n");
+      "-cache net.cache      # binary network cache (reused while .conf/.pro/options are unchanged)\n"
+      "-nolog                # do not write network.log\n");
 }
 
 int main(int argc, char **argv) {
@@ -41,7 +43,7 @@ int main(int argc, char **argv) {
   mo.repeats = 1;
   fs_run_opts ro{};
   ro.mode = FS_MODE_COMPAT;
-  bool help = false;
+  bool help = false, netlog = true;
   for (int i = 1; i < argc && !help; i++) {
     std::string a = argv[i];
     auto val = [&](void) -> const char * {
@@ -65,6 +67,7 @@ int main(int argc, char **argv) {
     else if (a == "-gpu") ro.device = std::atoi(val());
     else if (a == "-chunk") ro.chunk_steps = (uint32_t)std::atoi(val());
     else if (a == "-cache") cache = val();
+    else if (a == "-nolog") netlog = false;
     else if (a == "-mode") {
       std::string v = val();
       if (v == "compat") ro.mode = FS_MODE_COMPAT;
@@ -96,6 +99,8 @@ int main(int argc, char **argv) {
   fs_model_info(m, &nn, nullptr, &ns, nullptr, nullptr);
   std::printf("time step:%g, total neurons=%u, total synapses=%llu\n", (double)mo.dt, nn,
               (unsigned long long)ns);
+  // RunInit (code/NetSimGnl2.cpp:143-157) writes network.log before the first repeat
+  if (netlog && fs_model_network_log(m, "network.log")) std::fprintf(stderr, "flysim: %s\n", fs_model_error());
   double secs = 0.0;
   rc = fs_model_run(m, &ro, "", &secs);
   if (rc) {

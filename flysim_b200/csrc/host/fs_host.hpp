@@ -5,6 +5,8 @@
 #include <string>
 #include <vector>
 #include <random>
+#include <sstream>
+#include <thread>
 #include "flysim_b200.h"
 
 namespace fsh {
@@ -92,9 +94,18 @@ struct Network {
     std::vector<uint32_t> rec_pre, rec_post;
     std::vector<float> rec_g;
     std::vector<uint32_t> rec_rowptr;
+    // group segments in the reference's order (posts ascending; for GluCl the
+    // post read through the Ach map): segment s holds seg_len[s] gather
+    // entries of post seg_post[s].  Only network.log reads these.
+    std::vector<uint32_t> seg_post, seg_len;
   } rec[FS_NREC];
   std::vector<uint32_t> gap_rowptr, gap_other;
   std::vector<float> gap_g;
+  // for network.log: single-target gap records sorted by post (PreID is the
+  // population index) and, per post, how many group gap terms open its
+  // gap_other row
+  std::vector<uint32_t> gap1_pre, gap1_post, gap_ngroup;
+  std::vector<float> gap1_g;
 
   // flat synapse list for the production modes
   std::vector<uint32_t> syn_pre, syn_post;
@@ -133,7 +144,33 @@ void parse_macros(Model &m, const std::string &path, int &state);
 void parse_pro(Model &m, const std::string &path, int &state);
 void add_command_outputs(Model &m);
 bool write_confs_info(const Model &m, const std::string &path);
+bool write_network_log(const Model &m, const std::string &path);
 void build_network(Model &m);
+
+// Formats items [0, count) in blocks of `block` on the host cores and writes
+// the blocks to o in item order; fmt(a, b, os) formats items [a, b).  Used by
+// the text logs, whose number formatting dominates their cost.
+template <class F>
+void write_ordered(std::ostream &o, size_t count, size_t block, F fmt) {
+  unsigned hw = std::thread::hardware_concurrency();
+  const unsigned T = hw < 1 ? 1 : (hw > 16 ? 16 : hw);
+  std::vector<std::string> out(T);
+  for (size_t base = 0; base < count; base += (size_t)T * block) {
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < T; t++) {
+      const size_t a = base + (size_t)t * block;
+      if (a >= count) break;
+      const size_t b = a + block < count ? a + block : count;
+      th.emplace_back([&out, &fmt, t, a, b] {
+        std::ostringstream s;
+        fmt(a, b, s);
+        out[t] = s.str();
+      });
+    }
+    for (auto &x : th) x.join();
+    for (size_t t = 0; t < th.size(); t++) o << out[t];
+  }
+}
 
 // Binary network cache (fs_cache.cpp).
 bool cache_key(const char *conf, const char *pro, const fs_model_opts &o, uint64_t &key);

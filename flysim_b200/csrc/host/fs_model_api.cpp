@@ -101,7 +101,30 @@ int fs_model_free(fs_model *m) {
 
 int fs_model_confs_info(fs_model *m, const char *path) {
   if (!m || !path) return FS_ERR_ARG;
-  if (!fsh::write_confs_info(m->m, path)) {
+  bool ok = false;
+  try {
+    ok = fsh::write_confs_info(m->m, path);
+  } catch (const std::exception &e) {
+    g_model_err = e.what();
+    return FS_ERR_IO;
+  }
+  if (!ok) {
+    g_model_err = std::string("cannot write ") + path;
+    return FS_ERR_IO;
+  }
+  return FS_OK;
+}
+
+int fs_model_network_log(fs_model *m, const char *path) {
+  if (!m || !path) return FS_ERR_ARG;
+  bool ok = false;
+  try {
+    ok = fsh::write_network_log(m->m, path);
+  } catch (const std::exception &e) {
+    g_model_err = e.what();
+    return FS_ERR_IO;
+  }
+  if (!ok) {
     g_model_err = std::string("cannot write ") + path;
     return FS_ERR_IO;
   }

@@ -15,6 +15,7 @@
 #include <climits>
 #include <cfloat>
 #include <fstream>
+#include <memory>
 #include <sstream>
 #include <unordered_map>
 #include <algorithm>
@@ -584,39 +585,45 @@ static const char *rep_name(uint8_t kw, bool with_gap) {
 // Parser::ConfsInfo (code/parser.cpp:1488-1631): ConfsInfo.log.  The
 // Hodgkin-Huxley block prints the reference's defaults (HH is not simulated).
 bool write_confs_info(const Model &m, const std::string &path) {
-  std::ofstream o(path.c_str());
+  std::unique_ptr<char[]> buf(new char[1 << 22]);
+  std::ofstream o;
+  o.rdbuf()->pubsetbuf(buf.get(), 1 << 22);
+  o.open(path.c_str());
   if (!o) return false;
   o << "configuration information:----------------------------------------\n";
-  for (uint32_t i = 0; i < m.pops.size(); i++) {
-    const Pop &p = m.pops[i];
-    o << "population:" << i << "\n"
-      << "NeuPopuName:" << p.name << ", N=" << p.N << " Taum=" << p.Taum << " Vth=" << p.Vth
-      << " El=" << p.El << " g=" << p.gl << " Cm=" << p.Cm << " Vreset=" << p.Vreset << "\n";
-    o << "Ek=0 gk=0 Ena=0 gna=0\n"
-      << "AnA=0.01 AnB=-60 AnC=10 AnD=-1\n"
-      << "BnA=0.125 BnB=-70 BnC=80 BnD=0\n"
-      << "AmA=0.1 AmB=-45 AmC=10 AmD=-1\n"
-      << "BmA=4 BmB=-70 BmC=18 BmD=0\n"
-      << "AhA=0.07 AhB=-70 AhC=20 AhD=0\n"
-      << "BhA=1 BhB=-40 BhC=10 BhD=1\n";
-    o << "pv=" << p.pv << " tD=" << p.tD << " aF=" << p.aF << " tF=" << p.tF << " aCap=" << p.aCap
-      << " tCap=" << p.tCap << " aCar=" << p.aCar << " tCar=" << p.tCar << "\n";
-    o << "tLP=" << p.tLP << " SpiLPDy=" << p.SpiLPDy << " PosISI=" << p.PosISI
-      << " NegISI=" << p.NegISI << "\n";
-    for (const Receptor &r : p.reps) {
-      o << "NeuRepName:" << rep_name(r.name, false) << ", Tau=" << r.Tau;
-      if (r.name == KW_NMDA) o << ", TauXT=" << r.TauXT;
-      o << " Vrv=" << r.Vrev << " FExt=" << r.FExt << " MnExtEff=" << r.MnExtEff
-        << " MnExtCon=" << r.MnExtCon << "\n";
+  write_ordered(o, m.pops.size(), 256, [&m](size_t a, size_t b, std::ostream &o) {
+    for (size_t i = a; i < b; i++) {
+      const Pop &p = m.pops[i];
+      o << "population:" << i << "\n"
+        << "NeuPopuName:" << p.name << ", N=" << p.N << " Taum=" << p.Taum << " Vth=" << p.Vth
+        << " El=" << p.El << " g=" << p.gl << " Cm=" << p.Cm << " Vreset=" << p.Vreset << "\n";
+      o << "Ek=0 gk=0 Ena=0 gna=0\n"
+        << "AnA=0.01 AnB=-60 AnC=10 AnD=-1\n"
+        << "BnA=0.125 BnB=-70 BnC=80 BnD=0\n"
+        << "AmA=0.1 AmB=-45 AmC=10 AmD=-1\n"
+        << "BmA=4 BmB=-70 BmC=18 BmD=0\n"
+        << "AhA=0.07 AhB=-70 AhC=20 AhD=0\n"
+        << "BhA=1 BhB=-40 BhC=10 BhD=1\n";
+      o << "pv=" << p.pv << " tD=" << p.tD << " aF=" << p.aF << " tF=" << p.tF << " aCap=" << p.aCap
+        << " tCap=" << p.tCap << " aCar=" << p.aCar << " tCar=" << p.tCar << "\n";
+      o << "tLP=" << p.tLP << " SpiLPDy=" << p.SpiLPDy << " PosISI=" << p.PosISI
+        << " NegISI=" << p.NegISI << "\n";
+      for (const Receptor &r : p.reps) {
+        o << "NeuRepName:" << rep_name(r.name, false) << ", Tau=" << r.Tau;
+        if (r.name == KW_NMDA) o << ", TauXT=" << r.TauXT;
+        o << " Vrv=" << r.Vrev << " FExt=" << r.FExt << " MnExtEff=" << r.MnExtEff
+          << " MnExtCon=" << r.MnExtCon << "\n";
+      }
+      o << "\n";
+      for (uint32_t j = p.link_beg; j < p.link_beg + p.link_num; j++) {
+        const Link &l = m.links[j];
+        o << "TarPopuName:" << m.pops[l.tgt].name << " TarReceptor:" << rep_name(l.rep, true)
+          << ", Connectivity=" << l.conn << " MeanEff=" << l.eff << " weight=" << l.weight << "\n";
+      }
+      o << "------------------------------------------------------------------\n";
     }
-    o << "\n";
-    for (uint32_t j = p.link_beg; j < p.link_beg + p.link_num; j++) {
-      const Link &l = m.links[j];
-      o << "TarPopuName:" << m.pops[l.tgt].name << " TarReceptor:" << rep_name(l.rep, true)
-        << ", Connectivity=" << l.conn << " MeanEff=" << l.eff << " weight=" << l.weight << "\n";
-    }
-    o << "------------------------------------------------------------------" << std::endl;
-  }
+  });
+  o.flush();
   return bool(o);
 }
 

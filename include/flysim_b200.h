@@ -286,6 +286,11 @@ const char *fs_model_error(void);
  * code/parser.cpp:1488-1631); the reference CLI writes it on every run
  * (code/main.cpp:247). */
 int fs_model_confs_info(fs_model *m, const char *path);
+/* Writes network.log for the built network (NetSimGnl2::logDataWrite,
+ * code/NetSimGnl2_info.cpp:93-546: per-neuron parameters, every synapse,
+ * events, output columns); the reference writes it before the first repeat
+ * (code/NetSimGnl2.cpp:143-157).  Text of O(neurons + synapses) size. */
+int fs_model_network_log(fs_model *m, const char *path);
 /* View of the built network (valid until fs_model_free). */
 int fs_model_desc(fs_model *m, const fs_net_desc **desc);
 int fs_model_info(fs_model *m, uint32_t *n_neurons, uint32_t *n_pops, uint64_t *n_syn_entries,

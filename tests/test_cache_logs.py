@@ -1,8 +1,10 @@
-"""Binary network cache and the reference's configuration log (CPU only).
+"""Binary network cache and the reference's two log files (CPU only).
 
 * ConfsInfo.log (Parser::ConfsInfo, code/parser.cpp:1488-1631) written from
-  the parsed model is byte-identical to the reference's for every golden case
-  (size and SHA-256 recorded in tests/golden/<case>/logs.json).
+  the parsed model and network.log (NetSimGnl2::logDataWrite,
+  code/NetSimGnl2_info.cpp:93-546) written from the built network are
+  byte-identical to the reference's for every golden case (size and SHA-256
+  recorded in tests/golden/<case>/logs.json).
 * A model read back from the cache drives the oracle to the same output files
   as the reference, byte for byte, and its counts and seeds equal a fresh load.
 * Any change of the .conf, the .pro or a load option misses the cache; a
@@ -22,6 +24,14 @@ def test_confs_info_matches_reference(built, case, tmp_path):
     p = str(tmp_path / "ConfsInfo.log")
     m.confs_info(p)
     assert file_digest(p) == golden_log_digest(case, "ConfsInfo.log")
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_network_log_matches_reference(built, case, tmp_path):
+    m = model_for(built, case)
+    p = str(tmp_path / "network.log")
+    m.network_log(p)
+    assert file_digest(p) == golden_log_digest(case, "network.log")
 
 
 def _copy_case(case, d):
@@ -50,9 +60,10 @@ def test_cached_model_reproduces_reference_outputs(built, oracle, case, tmp_path
     finally:
         oracle.oracle_destroy(ctx)
     assert not compare_outputs(case, str(out))
-    p = str(tmp_path / "ConfsInfo.log")
-    m.confs_info(p)
-    assert file_digest(p) == golden_log_digest(case, "ConfsInfo.log")
+    for f, write in (("ConfsInfo.log", m.confs_info), ("network.log", m.network_log)):
+        p = str(tmp_path / f)
+        write(p)
+        assert file_digest(p) == golden_log_digest(case, f)
 
 
 def test_cache_key_follows_files_and_options(built, tmp_path):

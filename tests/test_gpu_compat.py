@@ -11,7 +11,8 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, ROOT, OracleEngine, compare_outputs, first_diff, golden_cases, model_for
+from conftest import (GOLDEN, ROOT, OracleEngine, compare_outputs, file_digest, first_diff, golden_cases,
+                      golden_log_digest, golden_outputs, model_for)
 
 pytestmark = pytest.mark.gpu
 
@@ -78,3 +79,17 @@ def test_cli_is_a_drop_in(built, tmp_path):
                        text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     assert not compare_outputs(case, str(tmp_path))
+    # the two logs the reference writes on every run
+    for f in ("ConfsInfo.log", "network.log"):
+        assert file_digest(str(tmp_path / f)) == golden_log_digest(case, f), f
+    # through the binary network cache: stored, then read back, same files
+    os.remove(str(tmp_path / "network.log"))
+    for hit in (False, True):
+        for f in golden_outputs(case):
+            os.remove(str(tmp_path / f))
+        r = subprocess.run([exe, "-conf", "net.conf", "-pro", "net.pro", "-cache", "net.cache", "-nolog"],
+                           cwd=str(tmp_path), capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        assert ("network read from cache" in r.stdout) == hit
+        assert not compare_outputs(case, str(tmp_path))
+        assert not os.path.exists(str(tmp_path / "network.log"))
