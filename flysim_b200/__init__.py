@@ -383,6 +383,20 @@ class Engine:
             return spikes, V, I, NS
         return spikes, V
 
+    def step_csr(self, nsteps: int, spike_cap: Optional[int] = None):
+        """Runs nsteps; returns the spikes as the C ABI gives them: per-step
+        counts (uint32 [nsteps]) and the neuron indices of all steps in step
+        order (uint32 [sum(counts)]), with no per-step Python objects."""
+        counts = np.zeros(nsteps, np.uint32)
+        cap = spike_cap if spike_cap is not None else max(1024, nsteps * self.n)
+        idx = np.empty(cap, np.uint32)
+        so = StepOut()
+        so.spike_count = counts.ctypes.data_as(_u32)
+        so.spike_idx = idx.ctypes.data_as(_u32)
+        so.spike_cap = cap
+        _check(lib().fs_step(self._h, nsteps, C.byref(so)), self._h)
+        return counts, idx[:int(counts.sum(dtype=np.int64))]
+
     def run(self, nsteps: int):
         _check(lib().fs_run(self._h, nsteps), self._h)
 

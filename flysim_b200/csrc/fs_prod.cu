@@ -120,32 +120,50 @@ __device__ __forceinline__ float u24(uint32_t x) { return (float)(x >> 8) * 5.96
 // Over the `count` blocks that share `bar` (the whole grid, or the blocks of
 // one network instance in a batch).  bar[0] counts arrivals, bar[32] (its
 // own 128-byte line) is the generation the waiting blocks poll; the last
-// block to arrive resets the count and advances the generation.  Every wait
-// is bounded: after ~2^24 polls the block sets the error word and all
-// blocks leave.
+// block to arrive resets the count and advances the generation.  Ordering
+// (PTX memory model): after bar.sync, thread 0's acq_rel arrival releases
+// the whole block's writes (release is cumulative) and, for the last block,
+// acquires every earlier arrival's; the last block publishes the count reset
+// and all writes with a release add on the generation, which the others
+// observe with relaxed polls followed by one acquire fence; the closing
+// bar.sync hands that on to the block.  Every wait is bounded: after ~2^24
+// polls the block sets the error word and all blocks leave.
+__device__ __forceinline__ unsigned int ld_relaxed_gpu(const unsigned int *p) {
+  unsigned int v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned int atom_add_acq_rel_gpu(unsigned int *p, unsigned int v) {
+  unsigned int old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ void red_release_gpu(unsigned int *p, unsigned int v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_acquire_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
 __device__ __forceinline__ bool grid_sync(unsigned int *bar, int *err, uint32_t count) {
   __syncthreads();
   if (count <= 1) return *(volatile int *)err == 0;
   if (threadIdx.x == 0) {
-    volatile unsigned int *gen = bar + 32;
-    const unsigned int g = *gen;
-    __threadfence();
-    const unsigned int arrived = atomicAdd(bar, 1u);
+    unsigned int *gen = bar + 32;
+    const unsigned int g = ld_relaxed_gpu(gen);
+    const unsigned int arrived = atom_add_acq_rel_gpu(bar, 1u);
     if (arrived == count - 1) {
       atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd((unsigned int *)gen, 1u);
+      red_release_gpu(gen, 1u);
     } else {
       unsigned int spins = 0;
-      while (*gen == g) {
+      while (ld_relaxed_gpu(gen) == g) {
         if (*(volatile int *)err) break;
         if (++spins > (1u << 24)) {
           atomicExch(err, 2);
           break;
         }
       }
+      fence_acquire_gpu();
     }
-    __threadfence();
   }
   __syncthreads();
   return *(volatile int *)err == 0;
@@ -190,26 +208,31 @@ __device__ __forceinline__ float comp4(const float4 &q, int k) {
   return k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w;
 }
 
-// The next post's row bounds and first edge codes are fetched while the
-// current post's history windows are in flight, so a post costs about one
-// L2 round trip; per lane the edges are summed in the same order as a
-// plain walk (chunks of 32 x U edges, lane-strided), so the result does not
-// depend on the prefetching.
+// Lanes work in quads: the four lanes of a quad take the same edge and each
+// loads one of its window's 16-byte vectors (lane k: steps 4k..4k+3), so one
+// warp load instruction covers eight edges whose vectors share a cache line
+// per edge (about 1.25 L1 wavefronts per edge instead of 3 for a lane per
+// edge); each lane keeps U edges in flight.  The next round's edge codes
+// and weights are fetched while the current windows are in flight.  Quad g
+// sums the post's edges g, g + 8, g + 16, ... in that order whatever U is
+// (U only sets how many are in flight), then the eight quads are combined
+// by a butterfly, so the sums depend on neither U nor the block plan.
+template <int U>
 __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint32_t np, uint64_t tb, uint32_t L,
                                               float (*gn)[kTile], uint32_t wid, uint32_t lane) {
-  constexpr int U = 4;                 // edges per lane per round
-  constexpr int NV = kLB / 4;          // vectors per edge window
-  constexpr uint32_t CH = 32u * U;     // edges per warp round
+  constexpr uint32_t CH = 8u * U;      // edges per warp round
   const float4 *sh = (const float4 *)P.s_hist;
   const uint32_t S4 = P.slots >> 2, qmask = S4 - 1, mask = P.mask;
   const uint32_t nvl = (L + 3u) >> 2;  // vectors needed for L steps
   const uint32_t nw = kThreads / 32;
+  const uint32_t k = lane & 3u, g = lane >> 2;
+  const bool kv = k < nvl;
   uint32_t code[U];
   float w[U];
   auto fetch = [&](uint32_t base, uint32_t end) {
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      const uint32_t eu = base + lane + 32u * u;
+      const uint32_t eu = base + g + 8u * u;
       code[u] = eu < end ? __ldg(P.in_code + eu) : 0u;
       w[u] = eu < end ? __ldg(P.in_w + eu) : 0.0f;
     }
@@ -227,23 +250,18 @@ __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint
       n0 = __ldg(P.in_row + p0 + qn);
       n1 = __ldg(P.in_row + p0 + qn + 1);
     }
-    float acc[kLB];
-#pragma unroll
-    for (uint32_t j = 0; j < kLB; j++) acc[j] = 0.0f;
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     const uint32_t nch = (b1 - b0 + CH - 1) / CH;
     for (uint32_t c = 0; c < nch; c++) {
-      const uint32_t e = b0 + c * CH + lane;
-      float4 v[U][NV];
+      const uint32_t e = b0 + c * CH + g;
+      float4 v[U];
 #pragma unroll
       for (int u = 0; u < U; u++) {
-        const bool ok = e + 32u * u < b1;
+        const bool ok = kv && e + 8u * u < b1;
         const uint32_t pre = code[u] & 0xffffffu, d = code[u] >> 24;
         const uint32_t a = (uint32_t)(tb - 1u - d) & mask;
         const float4 *row = sh + ((size_t)pre * kSH + (a & 3u)) * S4;
-        const uint32_t i0 = a >> 2;
-#pragma unroll
-        for (int i = 0; i < NV; i++)
-          v[u][i] = (ok && (uint32_t)i < nvl) ? __ldca(row + ((i0 + i) & qmask)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        v[u] = ok ? __ldca(row + (((a >> 2) + k) & qmask)) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
       float wc[U];
 #pragma unroll
@@ -252,17 +270,22 @@ __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint
       else if (qn < np) fetch(n0, n1);
 #pragma unroll
       for (int u = 0; u < U; u++) {
-#pragma unroll
-        for (int j = 0; j < (int)kLB; j++)
-          if ((uint32_t)j < L) acc[j] += wc[u] * comp4(v[u][j >> 2], j & 3);
+        acc[0] += wc[u] * v[u].x;
+        acc[1] += wc[u] * v[u].y;
+        acc[2] += wc[u] * v[u].z;
+        acc[3] += wc[u] * v[u].w;
       }
     }
     if (nch == 0 && qn < np) fetch(n0, n1);
 #pragma unroll
-    for (uint32_t j = 0; j < kLB; j++) {
-      if (j < L) {
-        const float v = warp_sum<float>(acc[j]);
-        if (lane == j) gn[j][q] = v;
+    for (int o = 4; o < 32; o <<= 1)
+#pragma unroll
+      for (int i = 0; i < 4; i++) acc[i] += __shfl_xor_sync(fsd::kFull, acc[i], o);
+    if (lane < 4) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const uint32_t j = 4u * lane + (uint32_t)i;
+        if (j < L) gn[j][q] = acc[i];
       }
     }
     b0 = n0;
@@ -702,8 +725,9 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
 }
 
 // The steps of one block: posts [B0, B1) of the network P, whose blocks
-// (nblk of them) meet at a barrier after every interval.
-template <class T>
+// (nblk of them) meet at a barrier after every interval.  PU: NMDA edges in
+// flight per lane in the pull (results do not depend on it).
+template <class T, int PU>
 __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32_t B1, uint32_t nblk) {
   // FP64 tiles are half as wide so the per-tile buffers stay in static
   // shared memory
@@ -728,7 +752,7 @@ __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32
         const uint32_t np = min(kT, B1 - tp0);
         if constexpr (sizeof(T) == 4) {
           if (L == 1) nmda_pull1_f32(P, tp0, np, P.t0 + bs, (float (*)[kTile])gn, wid, lane);
-          else nmda_pull_f32(P, tp0, np, P.t0 + bs, L, (float (*)[kTile])gn, wid, lane);
+          else nmda_pull_f32<PU>(P, tp0, np, P.t0 + bs, L, (float (*)[kTile])gn, wid, lane);
         }
         else nmda_pull<T>(P, tp0, np, P.t0 + bs, L, gn, wid, lane);
         draw_inputs<T>(P, tp0, np, P.t0 + bs, L, hits, gauss);
@@ -766,10 +790,13 @@ __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32
   }
 }
 
-// FP32: two blocks per SM (128 registers); FP64 runs one block per SM
+// FP32: two blocks per SM (128 registers); FP64 runs one block per SM.  Four
+// NMDA edges in flight per lane measured fastest for one network (20k
+// connectome: 4.62 us per timestep against 4.71 with eight), eight for
+// batches of small networks.
 template <class T>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) k_prod(const __grid_constant__ Params P) {
-  prod_blocks<T>(P, P.block_post[blockIdx.x], P.block_post[blockIdx.x + 1], gridDim.x);
+  prod_blocks<T, 4>(P, P.block_post[blockIdx.x], P.block_post[blockIdx.x + 1], gridDim.x);
 }
 
 // ---- batch: many independent networks in one persistent launch -----------
@@ -791,7 +818,7 @@ __global__ void __launch_bounds__(kThreads) k_prod_batch(const Params *__restric
     for (uint32_t i = threadIdx.x; i < sizeof(Params) / 4; i += blockDim.x) dst[i] = src[i];
   }
   __syncthreads();
-  prod_blocks<T>(Psh, me.b0, me.b1, me.nblk);
+  prod_blocks<T, 8>(Psh, me.b0, me.b1, me.nblk);
 }
 
 // Advances every instance's step counter after a batch launch (graph node).
