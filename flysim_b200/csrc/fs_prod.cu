@@ -463,10 +463,11 @@ __device__ __forceinline__ void draw_inputs(const Params &P, uint32_t p0, uint32
 
 // ---- L steps of a tile's neurons (thread per neuron), with the pushes ----
 // Per-neuron parameters and state stay in registers for the L steps; the
-// ring slot of the next step is fetched while the current step computes
-// (it is final: every push into it happened before the interval began); a
-// warp pushes the spikes of its own lanes, so a step needs no block barrier.
-template <class T>
+// ring slots of the next PD steps are in flight while the current step
+// computes (they are final: every push into them happened before the
+// interval began); a warp pushes the spikes of its own lanes, so a step
+// needs no block barrier.
+template <class T, int PD>
 __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint32_t np, uint32_t sb, uint32_t L,
                                              T (*gn)[TileW<T>::W], const uint8_t (*hits)[TileW<T>::W],
                                              const T (*gauss)[TileW<T>::W], const SpikeList<T> &lst) {
@@ -506,14 +507,16 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
   }
   T ex = ((T *)P.ext_x)[p], es = ((T *)P.ext_s)[p], xp = ((T *)P.x_pre)[p], spre = ((T *)P.s_pre)[p];
   uint32_t nsp = 0;
-  // ring slot of the first step
-  long long rv[4];
+  // ring slots of the first steps: rv for step 0, rv2 for step 1 (PD == 2)
+  static_assert(PD == 1 || PD == 2, "ring prefetch distance 1 or 2");
+  long long rv[4], rv2[4];
   {
-    const uint32_t tprev = (uint32_t)(P.t0 + sb - 1u) & mask;
+    const uint32_t tprev = (uint32_t)(P.t0 + sb - 1u) & mask, tn = (uint32_t)(P.t0 + sb) & mask;
 #pragma unroll
     for (int r = 0; r < 4; r++) {
       const int ri = P.lin_of_rec[r];
       rv[r] = (ri >= 0 && own) ? (long long)__ldcg(P.ring + ((size_t)ri * n + p) * S + tprev) : 0ll;
+      rv2[r] = (PD == 2 && ri >= 0 && own && L > 1) ? (long long)__ldcg(P.ring + ((size_t)ri * n + p) * S + tn) : 0ll;
     }
   }
   for (uint32_t j = 0; j < L; j++) {
@@ -532,8 +535,13 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
         if (own && rv[r]) __stcg(P.ring + ((size_t)ri * n + p) * S + tprev, 0ull);
         G[r] = dfs[r] * G[r] + (T)rv[r] * (T)kInvFix;  // exact power-of-two scale
         g[r] = G[r];
-        // next step's slot (tm) is final since the interval began
-        rv[r] = (own && j + 1 < L) ? (long long)__ldcg(P.ring + ((size_t)ri * n + p) * S + tm) : 0ll;
+        // the slot of step j + PD (final since the interval began)
+        if constexpr (PD == 2) {
+          rv[r] = rv2[r];
+          rv2[r] = (own && j + 2 < L) ? (long long)__ldcg(P.ring + ((size_t)ri * n + p) * S + ((tm + 1u) & mask)) : 0ll;
+        } else {
+          rv[r] = (own && j + 1 < L) ? (long long)__ldcg(P.ring + ((size_t)ri * n + p) * S + tm) : 0ll;
+        }
       }
     }
     const uint32_t qs = tid < np ? tid : 0;
@@ -726,8 +734,9 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
 
 // The steps of one block: posts [B0, B1) of the network P, whose blocks
 // (nblk of them) meet at a barrier after every interval.  PU: NMDA edges in
-// flight per lane in the pull (results do not depend on it).
-template <class T, int PU>
+// flight per lane in the pull; PD: ring slots in flight per neuron in the
+// steps (results depend on neither).
+template <class T, int PU, int PD>
 __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32_t B1, uint32_t nblk) {
   // FP64 tiles are half as wide so the per-tile buffers stay in static
   // shared memory
@@ -758,7 +767,7 @@ __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32
         draw_inputs<T>(P, tp0, np, P.t0 + bs, L, hits, gauss);
         __syncthreads();
         // warps without neurons in this tile skip the steps
-        if ((tid & ~31u) < np) neuron_steps<T>(P, tp0, np, bs, L, gn, hits, gauss, lst);
+        if ((tid & ~31u) < np) neuron_steps<T, PD>(P, tp0, np, bs, L, gn, hits, gauss, lst);
         __syncthreads();
         // the batch's spikes: with fewer spikes than warps the whole block
         // walks each spike's out-edges (a hub's hundreds of edges in one or
@@ -790,13 +799,14 @@ __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32
   }
 }
 
-// FP32: two blocks per SM (128 registers); FP64 runs one block per SM.  Four
-// NMDA edges in flight per lane measured fastest for one network (20k
-// connectome: 4.62 us per timestep against 4.71 with eight), eight for
-// batches of small networks.
+// FP32: two blocks per SM (128 registers); FP64 runs one block per SM.  For
+// one network four NMDA edges in flight per lane and ring slots two steps
+// ahead measured fastest (20k connectome: 4.05 us per timestep; 4.60 with
+// one step ahead, 4.71 with eight edges); batches of small networks run
+// eight edges and one step ahead (their kernel has fewer registers to spare).
 template <class T>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) k_prod(const __grid_constant__ Params P) {
-  prod_blocks<T, 4>(P, P.block_post[blockIdx.x], P.block_post[blockIdx.x + 1], gridDim.x);
+  prod_blocks<T, 4, 2>(P, P.block_post[blockIdx.x], P.block_post[blockIdx.x + 1], gridDim.x);
 }
 
 // ---- batch: many independent networks in one persistent launch -----------
@@ -818,7 +828,7 @@ __global__ void __launch_bounds__(kThreads) k_prod_batch(const Params *__restric
     for (uint32_t i = threadIdx.x; i < sizeof(Params) / 4; i += blockDim.x) dst[i] = src[i];
   }
   __syncthreads();
-  prod_blocks<T, 8>(Psh, me.b0, me.b1, me.nblk);
+  prod_blocks<T, 8, 1>(Psh, me.b0, me.b1, me.nblk);
 }
 
 // Advances every instance's step counter after a batch launch (graph node).
