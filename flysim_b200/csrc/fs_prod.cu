@@ -294,63 +294,57 @@ __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint
 }
 
 // Single-step batches (networks whose minimum delay is 0 or 1 step pull
-// every step): each edge needs one value, so a warp takes four posts at
-// once with scalar loads, four times the loads in flight of the general
-// path.  Per post and lane the edges are summed in the same order as there
-// (lane-strided rounds of 32 x 4), then the same butterfly.
+// every step, and the last step of a call that ends one step into an
+// interval): each edge needs one value, so a warp takes four posts at once
+// with scalar loads, four times the edges in flight of the window path.
+// Lane (g, k) of the warp (lane = 4g + k) sums post k's edges g, g + 8,
+// g + 16, ... in order and the same xor 4, 8, 16 butterfly combines the
+// eight g, which is exactly the quad path's order for step 0: a step's
+// NMDA sum does not depend on the batch it falls in.
 __device__ __forceinline__ void nmda_pull1_f32(const Params &P, uint32_t p0, uint32_t np, uint64_t tb,
                                                float (*gn)[kTile], uint32_t wid, uint32_t lane) {
   constexpr int PG = 4;             // posts per warp at once
-  constexpr int U = 4;              // edges per lane per post and round
-  constexpr uint32_t CH = 32u * U;  // edges of a post per round
+  constexpr int U = 4;              // edges per lane per round
+  constexpr uint32_t CH = 8u * U;   // edges of a post per round
   const float *sh = (const float *)P.s_hist;
   const uint32_t S = P.slots, mask = P.mask;
   const uint32_t nw = kThreads / 32;
+  const uint32_t k = lane & 3u, g = lane >> 2;
   if (!P.in_row) {
     for (uint32_t q = wid * 32 + lane; q < np; q += nw * 32) gn[0][q] = 0.0f;
     return;
   }
   for (uint32_t q0 = wid * PG; q0 < np; q0 += nw * PG) {
-    uint32_t bb[PG + 1];
+    const uint32_t q = q0 + k;
+    const bool qv = q < np;
+    const uint32_t b0 = qv ? __ldg(P.in_row + p0 + q) : 0u, b1 = qv ? __ldg(P.in_row + p0 + q + 1) : 0u;
+    uint32_t nch = (b1 - b0 + CH - 1) / CH;
 #pragma unroll
-    for (int k = 0; k <= PG; k++) bb[k] = __ldg(P.in_row + p0 + min(q0 + k, np));
-    uint32_t nch = 0;
-#pragma unroll
-    for (int k = 0; k < PG; k++) nch = max(nch, (bb[k + 1] - bb[k] + CH - 1) / CH);
-    float acc[PG];
-#pragma unroll
-    for (int k = 0; k < PG; k++) acc[k] = 0.0f;
+    for (int o = 1; o < PG; o <<= 1) nch = max(nch, __shfl_xor_sync(fsd::kFull, nch, o));
+    float acc = 0.0f;
     for (uint32_t c = 0; c < nch; c++) {
-      uint32_t code[PG][U];
-      float w[PG][U], v[PG][U];
+      uint32_t code[U];
+      float w[U], v[U];
 #pragma unroll
-      for (int k = 0; k < PG; k++)
+      for (int u = 0; u < U; u++) {
+        const uint32_t e = b0 + c * CH + g + 8u * u;
+        const bool ok = e < b1;
+        code[u] = ok ? __ldg(P.in_code + e) : 0u;
+        w[u] = ok ? __ldg(P.in_w + e) : 0.0f;
+      }
 #pragma unroll
-        for (int u = 0; u < U; u++) {
-          const uint32_t e = bb[k] + c * CH + lane + 32u * u;
-          const bool ok = e < bb[k + 1];
-          code[k][u] = ok ? __ldg(P.in_code + e) : 0u;
-          w[k][u] = ok ? __ldg(P.in_w + e) : 0.0f;
-        }
+      for (int u = 0; u < U; u++) {
+        const uint32_t e = b0 + c * CH + g + 8u * u;
+        const uint32_t pre = code[u] & 0xffffffu, d = code[u] >> 24;
+        // row 0 of the shifted copies holds slot i at element i
+        v[u] = e < b1 ? __ldca(sh + (size_t)pre * kSH * S + ((uint32_t)(tb - 1u - d) & mask)) : 0.0f;
+      }
 #pragma unroll
-      for (int k = 0; k < PG; k++)
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-          const uint32_t e = bb[k] + c * CH + lane + 32u * u;
-          const uint32_t pre = code[k][u] & 0xffffffu, d = code[k][u] >> 24;
-          // row 0 of the shifted copies holds slot i at element i
-          v[k][u] = e < bb[k + 1] ? __ldca(sh + (size_t)pre * kSH * S + ((uint32_t)(tb - 1u - d) & mask)) : 0.0f;
-        }
-#pragma unroll
-      for (int k = 0; k < PG; k++)
-#pragma unroll
-        for (int u = 0; u < U; u++) acc[k] += w[k][u] * v[k][u];
+      for (int u = 0; u < U; u++) acc += w[u] * v[u];
     }
 #pragma unroll
-    for (int k = 0; k < PG; k++) {
-      const float sum = warp_sum<float>(acc[k]);
-      if (lane == 0 && q0 + k < np) gn[0][q0 + k] = sum;
-    }
+    for (int o = 4; o < 32; o <<= 1) acc += __shfl_xor_sync(fsd::kFull, acc, o);
+    if (g == 0 && qv) gn[0][q] = acc;
   }
 }
 

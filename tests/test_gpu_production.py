@@ -168,23 +168,28 @@ def _conn_net(n=2000, seed=3):
 
 
 def test_results_do_not_depend_on_call_split_or_blocks(built):
+    # calls of one step mid-run take the single-step NMDA pull, the others
+    # the window pull: a step's sums must not depend on which one it falls in
     na = _conn_net()
     steps = 3000
     ref = None
-    for bps, splits in ((0, [steps]), (1, [1, 7, 100, 892, 2000]), (2, [1500, 1500])):
+    for bps, splits in ((0, [steps]), (1, [1, 7, 100, 892, 2000]), (2, [1500, 1500]),
+                        (0, [503, 1, 1, 1, 14, 1, 479, 1, 999, 1000])):
         e = built.Engine(na.desc, "fp32", chunk_steps=256, blocks_per_sm=bps)
         try:
             e.reset(5)
             sp = []
             for k in splits:
                 sp += e.step(k)[0]
+            V = e.state()[0]
         finally:
             e.close()
         if ref is None:
-            ref = sp
+            ref, Vref = sp, V
             assert sum(x.size for x in sp) > 100
         else:
             assert all(np.array_equal(x, y) for x, y in zip(ref, sp)), "blocks/SM %d, splits %s" % (bps, splits)
+            assert np.array_equal(V.view(np.uint32), Vref.view(np.uint32)), "blocks/SM %d, splits %s" % (bps, splits)
 
 
 def test_seed_and_key_change_the_drive(built):
