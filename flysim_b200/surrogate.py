@@ -171,9 +171,11 @@ def fit(net: Mlp, x: np.ndarray, y: np.ndarray, rates: np.ndarray, epochs: int, 
     population-average response until the network separates the
     hyperactive regime), then annealed on a cosine.  After every round of
     `epochs_per_round` epochs the rate error on the held-out 10 % is
-    measured and the best parameters are kept; after the hold phase training
-    stops once `patience` rounds bring no improvement.  Returns (losses,
-    device ms, best validation error)."""
+    measured and the best parameters are kept; once the learning rate has
+    fallen below a quarter of `lr`, training stops after `patience` rounds
+    without improvement (stopping earlier, while the rate is still high,
+    ends before the anneal that gives most of the accuracy).  Returns
+    (losses, device ms, best validation error)."""
     n = len(x)
     perm = np.random.default_rng(seed + 17).permutation(n)
     nv = max(1, n // 10)
@@ -190,7 +192,7 @@ def fit(net: Mlp, x: np.ndarray, y: np.ndarray, rates: np.ndarray, epochs: int, 
         err = float(rate_error(decode_rates(net.forward(x[vi])), rates[vi]).mean())
         if err < best:
             best, best_p, stall = err, net.get_params(), 0
-        elif k >= hold:
+        elif k >= hold and f < 0.25:
             stall += 1
             if stall >= patience:
                 break
