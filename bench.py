@@ -115,9 +115,13 @@ WORKLOADS = {
 }
 
 
-def build_network(rank: int, workload: str = "connectome20k"):
+def build_network(rank: int, workload: str = "connectome20k", n: int = 0):
+    """The workload's network for one rank (seed + rank); n > 0 builds the
+    same kind of network with n neurons."""
     from flysim_b200 import netgen, network
-    w = WORKLOADS[workload]
+    w = dict(WORKLOADS[workload])
+    if n > 0:
+        w["n"] = n
     if workload == "connectome20k":
         c = netgen.connectome(n=w["n"], regions=REGIONS, seed=SEED + rank)
     else:
