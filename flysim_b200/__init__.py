@@ -135,6 +135,9 @@ def lib() -> C.CDLL:
         "fs_debug_expf": (C.c_int, [_f, _f, C.c_uint64]),
         "fs_debug_expf_noalloc": (C.c_int, [_f, _f, C.c_uint64]),
         "fs_get_state": (C.c_int, [vp, _f, _i32, _u32]),
+        "fs_checkpoint_size": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
+        "fs_checkpoint_save": (C.c_int, [vp, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
+        "fs_checkpoint_load": (C.c_int, [vp, C.c_void_p, C.c_uint64]),
         "fs_get_syn_state": (C.c_int, [vp, _f, _f]),
         "fs_model_load": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(ModelOpts), C.POINTER(vp)]),
         "fs_model_load_cached": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(ModelOpts), C.c_char_p,
@@ -189,7 +192,7 @@ def exported_symbols() -> Sequence[str]:
                         "fs_reset", "fs_set_drive", "fs_set_act", "fs_set_injection", "fs_step", "fs_run",
                         "fs_run_timed",
                         "fs_sync", "fs_stats", "fs_kernel_time", "fs_debug_expf", "fs_debug_expf_noalloc",
-                        "fs_get_state",
+                        "fs_get_state", "fs_checkpoint_size", "fs_checkpoint_save", "fs_checkpoint_load",
                         "fs_get_syn_state", "fs_model_load", "fs_model_load_cached", "fs_model_confs_info", "fs_model_network_log",
                         "fs_model_free", "fs_model_error",
                         "fs_model_desc", "fs_model_info", "fs_model_seed", "fs_model_run",
@@ -438,6 +441,18 @@ class Engine:
         _check(lib().fs_get_state(self._h, V.ctypes.data_as(_f), cnt.ctypes.data_as(_i32),
                                   ns.ctypes.data_as(_u32)), self._h)
         return V, cnt, ns
+
+    def checkpoint(self) -> bytes:
+        """The handle's state after its last step (production modes), for
+        restore() on a handle of the same network and mode."""
+        nb = C.c_uint64()
+        _check(lib().fs_checkpoint_size(self._h, C.byref(nb)), self._h)
+        buf = C.create_string_buffer(nb.value)
+        _check(lib().fs_checkpoint_save(self._h, buf, nb.value, C.byref(nb)), self._h)
+        return buf.raw[:nb.value]
+
+    def restore(self, data: bytes):
+        _check(lib().fs_checkpoint_load(self._h, data, len(data)), self._h)
 
     def syn_state(self):
         g = np.zeros(FS_NREC * self.n, np.float32)

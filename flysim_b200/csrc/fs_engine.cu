@@ -649,6 +649,110 @@ int fs_get_state(fs_handle *h, float *V, int32_t *Count, uint32_t *NState) {
   return FS_OK;
 }
 
+// ---- checkpoints (production modes) ----------------------------------------
+// Layout: CkptHead, the event-set parameters (pb [FS_NREC][n], act [n],
+// inj_mean [n], inj_std [n]), then the engine's state blob.
+namespace {
+struct CkptHead {
+  char magic[8];
+  uint32_t version, mode, n, fp64, slots, interval, lin_receptors, pad;
+  uint64_t lin_edges, nmda_edges, state_bytes, total_bytes;
+};
+constexpr char kCkptMagic[8] = {'F', 'S', 'B', '2', 'C', 'K', 'P', '\0'};
+
+int ckpt_head(fs_handle *h, CkptHead &c) {
+  if (!h) return set_err(nullptr, FS_ERR_ARG, "null handle");
+  if (h->mode == FS_MODE_COMPAT || !h->prod)
+    return set_err(h, FS_ERR_UNSUPPORTED, "checkpoints need a production mode (FS_MODE_FP32 or FS_MODE_FP64)");
+  fsp::ProdInfo pi{};
+  fsp::prod_info(h->prod, &pi);
+  std::memset(&c, 0, sizeof c);
+  std::memcpy(c.magic, kCkptMagic, 8);
+  c.version = 1;
+  c.mode = (uint32_t)h->mode;
+  c.n = h->n;
+  c.fp64 = (uint32_t)pi.fp64;
+  c.slots = pi.slots;
+  c.interval = pi.interval;
+  c.lin_receptors = pi.lin_receptors;
+  c.lin_edges = pi.lin_edges;
+  c.nmda_edges = pi.nmda_edges;
+  c.state_bytes = fsp::prod_state_bytes(h->prod);
+  c.total_bytes = sizeof(CkptHead) + (uint64_t)h->n * 4 * (FS_NREC + 3) + c.state_bytes;
+  return FS_OK;
+}
+}  // namespace
+
+int fs_checkpoint_size(fs_handle *h, uint64_t *bytes) {
+  CkptHead c;
+  int rc = ckpt_head(h, c);
+  if (rc) return rc;
+  if (!bytes) return set_err(h, FS_ERR_ARG, "fs_checkpoint_size: null bytes");
+  *bytes = c.total_bytes;
+  return FS_OK;
+}
+
+int fs_checkpoint_save(fs_handle *h, void *buf, uint64_t cap, uint64_t *bytes) {
+  CkptHead c;
+  int rc = ckpt_head(h, c);
+  if (rc) return rc;
+  if (bytes) *bytes = c.total_bytes;
+  if (!buf) return set_err(h, FS_ERR_ARG, "fs_checkpoint_save: null buffer");
+  if (cap < c.total_bytes) return set_err(h, FS_ERR_CAPACITY, "fs_checkpoint_save: buffer smaller than fs_checkpoint_size");
+  CK(cudaSetDevice(h->device));
+  uint8_t *o = (uint8_t *)buf;
+  const size_t n = h->n;
+  std::memcpy(o, &c, sizeof c);
+  o += sizeof c;
+  std::memcpy(o, h->pb.data(), (size_t)FS_NREC * n * 4);
+  o += (size_t)FS_NREC * n * 4;
+  std::memcpy(o, h->act.data(), n * 4);
+  o += n * 4;
+  std::memcpy(o, h->inj_mean.data(), n * 4);
+  o += n * 4;
+  std::memcpy(o, h->inj_std.data(), n * 4);
+  o += n * 4;
+  rc = fsp::prod_state_save(h->prod, o, h->st, h->err);
+  if (rc) return set_err(h, rc, h->err);
+  return FS_OK;
+}
+
+int fs_checkpoint_load(fs_handle *h, const void *buf, uint64_t bytes) {
+  CkptHead c;
+  int rc = ckpt_head(h, c);
+  if (rc) return rc;
+  if (!buf || bytes < sizeof(CkptHead)) return set_err(h, FS_ERR_ARG, "fs_checkpoint_load: no checkpoint");
+  CkptHead f;
+  std::memcpy(&f, buf, sizeof f);
+  if (std::memcmp(f.magic, kCkptMagic, 8) != 0 || f.version != c.version)
+    return set_err(h, FS_ERR_ARG, "fs_checkpoint_load: not a checkpoint of this library version");
+  if (f.mode != c.mode || f.n != c.n || f.fp64 != c.fp64 || f.slots != c.slots || f.interval != c.interval ||
+      f.lin_receptors != c.lin_receptors || f.lin_edges != c.lin_edges || f.nmda_edges != c.nmda_edges ||
+      f.state_bytes != c.state_bytes || f.total_bytes != c.total_bytes)
+    return set_err(h, FS_ERR_ARG, "fs_checkpoint_load: checkpoint of another network or mode");
+  if (bytes < c.total_bytes) return set_err(h, FS_ERR_ARG, "fs_checkpoint_load: checkpoint truncated");
+  CK(cudaSetDevice(h->device));
+  const uint8_t *i = (const uint8_t *)buf + sizeof f;
+  const size_t n = h->n;
+  std::memcpy(h->pb.data(), i, (size_t)FS_NREC * n * 4);
+  i += (size_t)FS_NREC * n * 4;
+  std::memcpy(h->act.data(), i, n * 4);
+  i += n * 4;
+  std::memcpy(h->inj_mean.data(), i, n * 4);
+  i += n * 4;
+  std::memcpy(h->inj_std.data(), i, n * 4);
+  i += n * 4;
+  h->dirty = true;
+  rc = fsp::prod_state_load(h->prod, i, h->st, h->err);
+  if (rc) return set_err(h, rc, h->err);
+  uint64_t t = 0, spk = 0;
+  std::memcpy(&t, i, 8);
+  std::memcpy(&spk, i + c.state_bytes - 8, 8);
+  h->steps_done = t;
+  h->spikes_total = spk;
+  return upload_params(h);
+}
+
 int fs_get_syn_state(fs_handle *h, float *g, float *Isyn) {
   if (!h) return set_err(nullptr, FS_ERR_ARG, "null handle");
   CK(cudaStreamSynchronize(h->st));

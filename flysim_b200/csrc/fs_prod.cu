@@ -1780,6 +1780,103 @@ int batch_spike_totals(Batch *B, uint64_t *totals, cudaStream_t st, std::string 
 
 uint32_t batch_size(const Batch *B) { return (uint32_t)B->inst.size(); }
 
+// ---- checkpoints --------------------------------------------------------
+// The state a production engine carries from one step to the next, in the
+// order it is saved: neuron and receptor state, presynaptic gates and NMDA
+// kinetics, the s history, spike counters, plasticity state and the delay
+// ring (pushes already made for future steps), then the spike total.
+namespace {
+struct StateHead {
+  uint64_t t;
+  uint32_t key0, key1;
+  float rg[5];
+  uint32_t pad;
+};
+void state_regions(Prod *p, std::vector<std::pair<void *, size_t>> &r) {
+  const size_t n = p->n, T = p->fp64 ? 8 : 4;
+  Params &P = p->P;
+  r.clear();
+  r.push_back({P.V, n * T});
+  r.push_back({P.G, 4 * n * T});
+  r.push_back({P.ext_st, 4 * n * T});
+  r.push_back({P.ext_x, n * T});
+  r.push_back({P.ext_s, n * T});
+  r.push_back({P.st_pre, 4 * n * T});
+  r.push_back({P.x_pre, n * T});
+  r.push_back({P.s_pre, n * T});
+  r.push_back({P.s_hist, (size_t)P.slots * n * T * (p->fp64 ? 1 : kSH)});
+  r.push_back({P.Count, n * 4});
+  r.push_back({P.NS, n * 4});
+  r.push_back({P.D, n * 4});
+  r.push_back({P.F, n * 4});
+  r.push_back({P.Cap, n * 4});
+  r.push_back({P.Car, n * 4});
+  r.push_back({P.tm_u, n * 4});
+  r.push_back({P.tm_x, n * 4});
+  r.push_back({P.nspk, n * 4});
+  r.push_back({P.Irep, (size_t)5 * n * 4});
+  r.push_back({P.ring, (size_t)std::max<uint32_t>(1, p->nlin) * P.slots * n * 8});
+  r.push_back({p->spike_total, 8});
+}
+}  // namespace
+
+uint64_t prod_state_bytes(Prod *p) {
+  std::vector<std::pair<void *, size_t>> r;
+  state_regions(p, r);
+  uint64_t b = sizeof(StateHead);
+  for (auto &x : r) b += x.second;
+  return b;
+}
+
+int prod_state_save(Prod *p, uint8_t *buf, cudaStream_t st, std::string &err) {
+  cudaError_t e = cudaStreamSynchronize(st);
+  StateHead h{};
+  h.t = p->t;
+  h.key0 = p->P.key0;
+  h.key1 = p->P.key1;
+  std::memcpy(h.rg, p->P.rg, sizeof h.rg);
+  std::memcpy(buf, &h, sizeof h);
+  std::vector<std::pair<void *, size_t>> r;
+  state_regions(p, r);
+  size_t off = sizeof h;
+  for (auto &x : r) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(buf + off, x.first, x.second, cudaMemcpyDeviceToHost, st);
+    off += x.second;
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("checkpoint save: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  return FS_OK;
+}
+
+int prod_state_load(Prod *p, const uint8_t *buf, cudaStream_t st, std::string &err) {
+  cudaError_t e = cudaStreamSynchronize(st);
+  StateHead h;
+  std::memcpy(&h, buf, sizeof h);
+  std::vector<std::pair<void *, size_t>> r;
+  state_regions(p, r);
+  size_t off = sizeof h;
+  for (auto &x : r) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(x.first, buf + off, x.second, cudaMemcpyHostToDevice, st);
+    off += x.second;
+  }
+  if (e == cudaSuccess) e = cudaMemsetAsync(p->err, 0, 4, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("checkpoint load: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  p->t = h.t;
+  p->P.key0 = h.key0;
+  p->P.key1 = h.key1;
+  std::memcpy(p->P.rg, h.rg, sizeof h.rg);
+  p->ms = 0.0;
+  p->kl = 0;
+  return FS_OK;
+}
+
 void prod_set_gains(Prod *p, const float *g) {
   for (int r = 0; r < 5; r++) p->P.rg[r] = g[r];
 }

@@ -31,6 +31,11 @@ struct ProdInfo {
 };
 void prod_info(const Prod *p, ProdInfo *info);
 int prod_spike_counts(Prod *p, uint32_t *counts, cudaStream_t st, std::string &err);
+// Checkpoint blob of the engine's step-to-step state (step counter, drive
+// stream key, gains, every state array and the delay ring).
+uint64_t prod_state_bytes(Prod *p);
+int prod_state_save(Prod *p, uint8_t *buf, cudaStream_t st, std::string &err);
+int prod_state_load(Prod *p, const uint8_t *buf, cudaStream_t st, std::string &err);
 
 // Batch: independent production networks advanced by one persistent launch.
 struct Batch;

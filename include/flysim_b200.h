@@ -250,6 +250,22 @@ int fs_debug_expf(const float *x, float *y, uint64_t k);
  * stream (cudaStreamPerThread) and returns when y is written. */
 #define FS_NOALLOC_MAX_K 262144u
 int fs_debug_expf_noalloc(const float *x, float *y, uint64_t k);
+/* Checkpoints of a production-mode handle (FS_MODE_FP32 / FS_MODE_FP64).
+ * The reference parses a SaveAllStates output and Resume event subtypes
+ * (code/parser.cpp:1167-1176, :1254-1258) but implements neither; here a
+ * checkpoint holds everything a step reads from the steps before it: the
+ * step counter and drive stream key, the event-set parameters (drive,
+ * receptor switches, injection), the synaptic gains, every neuron, receptor,
+ * plasticity and spike-count state array, the NMDA s history and the delay
+ * ring with the pushes already made for future steps.  A handle created
+ * from the same description and mode continues from fs_checkpoint_load
+ * exactly as the saved handle would (bit for bit: the drive draws are a
+ * function of the step counter and key).  fs_checkpoint_size gives the
+ * buffer size; loading a checkpoint of another network or mode returns
+ * FS_ERR_ARG; the compat mode returns FS_ERR_UNSUPPORTED. */
+int fs_checkpoint_size(fs_handle *h, uint64_t *bytes);
+int fs_checkpoint_save(fs_handle *h, void *buf, uint64_t cap, uint64_t *bytes);
+int fs_checkpoint_load(fs_handle *h, const void *buf, uint64_t bytes);
 /* Copy state out (V, Count, NState) for checks; arrays of length n. */
 int fs_get_state(fs_handle *h, float *V, int32_t *Count, uint32_t *NState);
 /* Full conductance view for checks: RVs (FS_NREC*n) after the last step and

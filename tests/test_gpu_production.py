@@ -192,6 +192,59 @@ def test_results_do_not_depend_on_call_split_or_blocks(built):
             assert np.array_equal(V.view(np.uint32), Vref.view(np.uint32)), "blocks/SM %d, splits %s" % (bps, splits)
 
 
+@pytest.mark.parametrize("mode,tm", [("fp32", False), ("fp32", True), ("fp64", False)])
+def test_checkpoint_resumes_bit_for_bit(built, mode, tm):
+    # a drive event before the save, delays in flight in the ring, TM state:
+    # a fresh handle restored from the checkpoint continues exactly as the
+    # saved one, and the saved handle can be rewound to it
+    from flysim_b200 import netgen, network
+    c = netgen.connectome(n=2000, regions=5, seed=3)
+    na = network.connectome_net(c, tm=tm)
+    e = built.Engine(na.desc, mode, chunk_steps=256)
+    f = built.Engine(na.desc, mode, chunk_steps=256)
+    try:
+        e.reset(7)
+        e.step(1234)
+        e.set_drive(0, 300, 0, 0.05)
+        e.step(17)
+        ck = e.checkpoint()
+        a = e.step(1500)[0]
+        Va = e.state()[0].copy()
+        f.reset(99)  # another seed: the checkpoint carries the drive stream key
+        f.restore(ck)
+        assert f.stats()["steps"] == 1251
+        b = f.step(1500)[0]
+        assert sum(x.size for x in a) > 100
+        assert all(np.array_equal(x, y) for x, y in zip(a, b))
+        assert np.array_equal(f.state()[0].view(np.uint8), Va.view(np.uint8))
+        assert f.stats()["spikes"] == e.stats()["spikes"]
+        e.restore(ck)
+        assert all(np.array_equal(x, y) for x, y in zip(a, e.step(1500)[0]))
+    finally:
+        e.close()
+        f.close()
+    # a checkpoint of another network, or a compat handle, is refused
+    other = network.connectome_net(netgen.connectome(n=2100, regions=5, seed=4), tm=tm)
+    g = built.Engine(other.desc, mode)
+    try:
+        with pytest.raises(built.FsError) as ex:
+            g.restore(ck)
+        assert ex.value.code == built.FS_ERR_ARG
+    finally:
+        g.close()
+
+
+def test_checkpoint_needs_a_production_mode(built):
+    m = built.Model(os.path.join(GOLDEN, "small", "net.conf"), os.path.join(GOLDEN, "small", "net.pro"))
+    e = built.Engine(m.desc(), "compat")
+    try:
+        with pytest.raises(built.FsError) as ex:
+            e.checkpoint()
+        assert ex.value.code == built.FS_ERR_UNSUPPORTED
+    finally:
+        e.close()
+
+
 def test_seed_and_key_change_the_drive(built):
     na = _conn_net()
     out = []
