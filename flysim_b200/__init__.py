@@ -135,6 +135,7 @@ def lib() -> C.CDLL:
         "fs_debug_expf": (C.c_int, [_f, _f, C.c_uint64]),
         "fs_debug_expf_noalloc": (C.c_int, [_f, _f, C.c_uint64]),
         "fs_get_state": (C.c_int, [vp, _f, _i32, _u32]),
+        "fs_debug_barrier_timeout": (C.c_int, [C.c_uint32]),
         "fs_checkpoint_size": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
         "fs_checkpoint_save": (C.c_int, [vp, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
         "fs_checkpoint_load": (C.c_int, [vp, C.c_void_p, C.c_uint64]),
@@ -192,7 +193,7 @@ def exported_symbols() -> Sequence[str]:
                         "fs_reset", "fs_set_drive", "fs_set_act", "fs_set_injection", "fs_step", "fs_run",
                         "fs_run_timed",
                         "fs_sync", "fs_stats", "fs_kernel_time", "fs_debug_expf", "fs_debug_expf_noalloc",
-                        "fs_get_state", "fs_checkpoint_size", "fs_checkpoint_save", "fs_checkpoint_load",
+                        "fs_get_state", "fs_debug_barrier_timeout", "fs_checkpoint_size", "fs_checkpoint_save", "fs_checkpoint_load",
                         "fs_get_syn_state", "fs_model_load", "fs_model_load_cached", "fs_model_confs_info", "fs_model_network_log",
                         "fs_model_free", "fs_model_error",
                         "fs_model_desc", "fs_model_info", "fs_model_seed", "fs_model_run",

@@ -649,6 +649,17 @@ int fs_get_state(fs_handle *h, float *V, int32_t *Count, uint32_t *NState) {
   return FS_OK;
 }
 
+int fs_debug_barrier_timeout(uint32_t poll_limit) {
+  if (poll_limit == 0 || poll_limit > (1u << 24))
+    return set_err(nullptr, FS_ERR_ARG, "fs_debug_barrier_timeout: poll limit must be 1 .. 2^24");
+  std::string err;
+  int word = 0;
+  int rc = fsp::prod_barrier_probe(poll_limit, &word, err);
+  if (rc) return set_err(nullptr, rc, err);
+  if (word) return set_err(nullptr, FS_ERR_TIMEOUT, "barrier wait gave up (device error word set)");
+  return FS_OK;
+}
+
 // ---- checkpoints (production modes) ----------------------------------------
 // Layout: CkptHead, the event-set parameters (pb [FS_NREC][n], act [n],
 // inj_mean [n], inj_std [n]), then the engine's state blob.

@@ -143,7 +143,8 @@ __device__ __forceinline__ void red_release_gpu(unsigned int *p, unsigned int v)
 }
 __device__ __forceinline__ void fence_acquire_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
-__device__ __forceinline__ bool grid_sync(unsigned int *bar, int *err, uint32_t count) {
+__device__ __forceinline__ bool grid_sync(unsigned int *bar, int *err, uint32_t count,
+                                          unsigned int limit = 1u << 24) {
   __syncthreads();
   if (count <= 1) return *(volatile int *)err == 0;
   if (threadIdx.x == 0) {
@@ -157,7 +158,7 @@ __device__ __forceinline__ bool grid_sync(unsigned int *bar, int *err, uint32_t 
       unsigned int spins = 0;
       while (ld_relaxed_gpu(gen) == g) {
         if (*(volatile int *)err) break;
-        if (++spins > (1u << 24)) {
+        if (++spins > limit) {
           atomicExch(err, 2);
           break;
         }
@@ -1779,6 +1780,34 @@ int batch_spike_totals(Batch *B, uint64_t *totals, cudaStream_t st, std::string 
 }
 
 uint32_t batch_size(const Batch *B) { return (uint32_t)B->inst.size(); }
+
+// ---- failure detection check ---------------------------------------------
+// One block waits at a barrier of two blocks that the second never reaches:
+// the bounded wait gives up after `limit` polls, sets the error word and
+// returns, and the context stays usable.
+__global__ void k_barrier_probe(unsigned int *bar, int *err, unsigned int limit) { grid_sync(bar, err, 2, limit); }
+
+int prod_barrier_probe(unsigned int limit, int *err_word, std::string &err) {
+  unsigned int *bar = nullptr;
+  int *ew = nullptr;
+  cudaError_t e = cudaMalloc(&bar, 64 * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&ew, 4);
+  if (e == cudaSuccess) e = cudaMemset(bar, 0, 64 * 4);
+  if (e == cudaSuccess) e = cudaMemset(ew, 0, 4);
+  if (e == cudaSuccess) {
+    k_barrier_probe<<<1, 32>>>(bar, ew, limit);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(err_word, ew, 4, cudaMemcpyDeviceToHost);
+  if (bar) cudaFree(bar);
+  if (ew) cudaFree(ew);
+  if (e != cudaSuccess) {
+    err = std::string("barrier probe: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  return FS_OK;
+}
 
 // ---- checkpoints --------------------------------------------------------
 // The state a production engine carries from one step to the next, in the

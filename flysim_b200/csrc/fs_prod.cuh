@@ -31,6 +31,8 @@ struct ProdInfo {
 };
 void prod_info(const Prod *p, ProdInfo *info);
 int prod_spike_counts(Prod *p, uint32_t *counts, cudaStream_t st, std::string &err);
+// Runs the bounded barrier wait to its limit (see k_barrier_probe).
+int prod_barrier_probe(unsigned int limit, int *err_word, std::string &err);
 // Checkpoint blob of the engine's step-to-step state (step counter, drive
 // stream key, gains, every state array and the delay ring).
 uint64_t prod_state_bytes(Prod *p);

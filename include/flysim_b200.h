@@ -250,6 +250,15 @@ int fs_debug_expf(const float *x, float *y, uint64_t k);
  * stream (cudaStreamPerThread) and returns when y is written. */
 #define FS_NOALLOC_MAX_K 262144u
 int fs_debug_expf_noalloc(const float *x, float *y, uint64_t k);
+/* Failure-detection check: a kernel waits at a grid barrier that a missing
+ * block never reaches.  Every device wait in this library is bounded (the
+ * production kernels' interval barrier gives up after 2^24 polls); here the
+ * bound is poll_limit (1 .. 2^24), after which the kernel sets its error word
+ * and returns.  Returns FS_ERR_TIMEOUT (the expected outcome), and the device
+ * stays usable for the next call.  The reference has no counterpart: its
+ * step threads meet at condition-variable waits with no time limit
+ * (code/NetSimGnl2.cpp:198-224) and are joined at the end (:348). */
+int fs_debug_barrier_timeout(uint32_t poll_limit);
 /* Checkpoints of a production-mode handle (FS_MODE_FP32 / FS_MODE_FP64).
  * The reference parses a SaveAllStates output and Resume event subtypes
  * (code/parser.cpp:1167-1176, :1254-1258) but implements neither; here a

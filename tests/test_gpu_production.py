@@ -234,6 +234,23 @@ def test_checkpoint_resumes_bit_for_bit(built, mode, tm):
         g.close()
 
 
+def test_bounded_wait_reports_timeout_and_device_stays_usable(built):
+    # a grid barrier that a missing block never reaches: the wait gives up
+    # after its poll limit, the host reads the error word as FS_ERR_TIMEOUT,
+    # and the next engine runs normally
+    rc = built.lib().fs_debug_barrier_timeout(1 << 14)
+    assert rc == built.FS_ERR_TIMEOUT, rc
+    assert built.lib().fs_debug_barrier_timeout(0) == built.FS_ERR_ARG
+    na = _conn_net()
+    e = built.Engine(na.desc, "fp32")
+    try:
+        e.reset(5)
+        spk = e.step(3000)[0]
+        assert sum(x.size for x in spk) > 100
+    finally:
+        e.close()
+
+
 def test_checkpoint_needs_a_production_mode(built):
     m = built.Model(os.path.join(GOLDEN, "small", "net.conf"), os.path.join(GOLDEN, "small", "net.pro"))
     e = built.Engine(m.desc(), "compat")
