@@ -794,14 +794,15 @@ __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32
   }
 }
 
-// FP32: two blocks per SM (128 registers); FP64 runs one block per SM.  For
-// one network four NMDA edges in flight per lane and ring slots two steps
-// ahead measured fastest (20k connectome: 4.05 us per timestep; 4.60 with
-// one step ahead, 4.71 with eight edges); batches of small networks run
-// eight edges and one step ahead (their kernel has fewer registers to spare).
-template <class T>
+// FP32: two blocks per SM (128 registers); FP64 runs one block per SM.  PU
+// NMDA edges in flight per lane: four when a block's posts fit one tile
+// (20k connectome: 4.05 us per timestep against 4.71 with eight), eight when
+// they span several (250k network: 43.3 against 46.3 us); ring slots two
+// steps ahead (4.60 us with one).  Batches of small networks run eight edges
+// and one step ahead (their kernel has fewer registers to spare).
+template <class T, int PU>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) k_prod(const __grid_constant__ Params P) {
-  prod_blocks<T, 4, 2>(P, P.block_post[blockIdx.x], P.block_post[blockIdx.x + 1], gridDim.x);
+  prod_blocks<T, PU, 2>(P, P.block_post[blockIdx.x], P.block_post[blockIdx.x + 1], gridDim.x);
 }
 
 // ---- batch: many independent networks in one persistent launch -----------
@@ -835,6 +836,7 @@ __global__ void k_batch_advance(Params *Ps, uint32_t count, uint32_t nsteps) {
 // ---- host side -------------------------------------------------------------
 struct Prod {
   bool fp64 = false;
+  bool wide = false;  // some block's posts span several tiles: eight NMDA edges in flight
   uint32_t n = 0, sm = 148;
   Params P{};
   std::vector<void *> allocs;
@@ -939,8 +941,10 @@ int launch(Prod *p, uint32_t nsteps, bool want_bits, bool wantV, cudaStream_t st
   P.spike_total = p->spike_total;
   void *args[] = {&P};
   cudaEventRecord(p->e0, st);
-  if (p->fp64) e = cudaLaunchCooperativeKernel((void *)k_prod<double>, p->blocks, kThreads, args, 0, st);
-  else e = cudaLaunchCooperativeKernel((void *)k_prod<float>, p->blocks, kThreads, args, 0, st);
+  // (the FP64 pull does not take the edges-in-flight parameter)
+  const void *k = p->fp64 ? (const void *)k_prod<double, 4>
+                          : (p->wide ? (const void *)k_prod<float, 8> : (const void *)k_prod<float, 4>);
+  e = cudaLaunchCooperativeKernel(k, p->blocks, kThreads, args, 0, st);
   cudaEventRecord(p->e1, st);
   if (e != cudaSuccess) {
     err = std::string("cooperative launch: ") + cudaGetErrorString(e);
@@ -1089,7 +1093,7 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
   }
   // ---- grid: all blocks co-resident; posts split by estimated cost ----
   int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p->fp64 ? (const void *)k_prod<double> : (const void *)k_prod<float>,
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p->fp64 ? (const void *)k_prod<double, 4> : (const void *)k_prod<float, 4>,
                                                 kThreads, 0);
   if (occ < 1) occ = 1;
   int per_sm = std::min(occ, 4);
@@ -1112,6 +1116,8 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
     for (; b < blocks; b++) block_post[b] = n;
   }
   p->chunks = blocks;
+  for (uint32_t b = 0; b < blocks; b++)
+    if (block_post[b + 1] - block_post[b] > kTile) p->wide = true;
   p->in_row_h = in_row;
   // ---- device arrays ----
   int rc = 0;
