@@ -441,10 +441,13 @@ __device__ __forceinline__ void draw_inputs(const Params &P, uint32_t p0, uint32
 #pragma unroll
     for (int r = 0; r < 4; r++)
       if (__ldg(P.pb + (size_t)r * n + p) > u24(rnd[r])) h |= 1u << r;
-    if (a & (FS_ACT_NMDA | FS_ACT_INJ)) {
+    // the second block serves the NMDA drive and the injection noise; a
+    // drive probability that is not positive never draws a hit
+    const float pbn = __ldg(P.pb + (size_t)FS_NMDA * n + p);
+    if (((a & FS_ACT_NMDA) && pbn > 0.0f) || (a & FS_ACT_INJ)) {
       uint32_t r2[4] = {(uint32_t)t, (uint32_t)(t >> 32), p, 1u};
       philox(r2, P.key0, P.key1);
-      if (__ldg(P.pb + (size_t)FS_NMDA * n + p) > u24(r2[0])) h |= 1u << FS_NMDA;
+      if (pbn > u24(r2[0])) h |= 1u << FS_NMDA;
       if (a & FS_ACT_INJ) {  // Box-Muller normal
         const double u1 = ((double)(r2[1] >> 8) + 1.0) * 5.9604644775390625e-08;
         const double u2 = (double)(r2[2] >> 8) * 5.9604644775390625e-08;
