@@ -52,8 +52,16 @@ def model_for(fb, case, **kw):
     d = os.path.join(GOLDEN, case)
     flags = json.load(open(os.path.join(d, "cmd.json")))
     opts = dict(stp="-STP" in flags, std="-STD" in flags, ltp="-LTP" in flags)
-    if "-rp" in flags:
-        opts["repeats"] = int(flags[flags.index("-rp") + 1])
+    val = {f: flags[i + 1] for i, f in enumerate(flags[:-1])}
+    if "-rp" in val:
+        opts["repeats"] = int(val["-rp"])
+    if "-udfsed" in val:
+        opts["user_seed"] = int(val["-udfsed"])
+    if "-dt" in val:
+        opts["dt"] = float(val["-dt"])
+    for flag, key in (("-om", "out_mem"), ("-os", "out_spike"), ("-or", "out_rate")):
+        if flag in val:
+            opts[key] = val[flag]
     opts.update(kw)
     return fb.Model(os.path.join(d, "net.conf"), os.path.join(d, "net.pro"), **opts)
 

@@ -10,6 +10,7 @@ reference's output files; the two log files it writes on every run
 
     python tests/golden/make_golden.py              # all cases from scratch
     python tests/golden/make_golden.py --logs-only  # logs.json of the committed cases
+    python tests/golden/make_golden.py --case NAME  # one case (or several names)
 """
 from __future__ import annotations
 
@@ -122,6 +123,12 @@ def cases():
                  {"name": "FRates.dat", "type": "FiringRate", "pop": "Exc2", "win": 50, "step": 10}],
         events=[{"t": 300, "type": "ChangeExtFreq", "pop": "Exc1", "f": 24000},
                 {"t": 650, "type": "ChangeMembraneNoise", "pop": "Exc1", "mean": 0.43, "std": 0.03}]), flags=[])
+    # command-line options: user seed (which also switches STD on, as the
+    # reference's flag parser does), a non-default time step, and the
+    # -om / -os / -or outputs added on top of the .pro's
+    c["cli_flags"] = dict(conf=lambda p: netgen.write_two_pop(p, n_e=16, n_i=8), pro=dict(
+        t_end_ms=40, seeds=(5,), outputs=OUTS[:1]),
+        flags=["-udfsed", "7", "-dt", "0.05", "-om", "m.dat", "-os", "s.dat", "-or", "r.dat"])
     return c
 
 
@@ -163,7 +170,10 @@ def main():
         sys.exit("reference binary missing: build it with  make -f oracle/Makefile.ref")
     if "--logs-only" in sys.argv:
         return logs_only()
+    only = sys.argv[sys.argv.index("--case") + 1:] if "--case" in sys.argv else None
     for name, cs in cases().items():
+        if only and name not in only:
+            continue
         d = os.path.join(HERE, name)
         shutil.rmtree(d, ignore_errors=True)
         os.makedirs(d)
