@@ -68,6 +68,7 @@ int main(int argc, char **argv) {
     else if (a == "-chunk") ro.chunk_steps = (uint32_t)std::atoi(val());
     else if (a == "-cache") cache = val();
     else if (a == "-nolog") netlog = false;
+    else if (a == "-daemon") return 0;  // the reference parses it, then stops without a run or a message (code/main.cpp:86, :205-208)
     else if (a == "-mode") {
       std::string v = val();
       if (v == "compat") ro.mode = FS_MODE_COMPAT;
