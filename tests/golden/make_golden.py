@@ -147,6 +147,25 @@ def record_logs(d):
         json.dump(rec, f, indent=1, sort_keys=True)
 
 
+def record_threaded_log(d, flags):
+    """Adds to logs.json the digest of the network.log the reference writes
+    with -t 4: set-up draws depend on the thread count (the run itself is
+    not reproducible with several threads, its set-up is)."""
+    with tempfile.TemporaryDirectory() as t:
+        for f in ("net.conf", "net.pro"):
+            shutil.copy(os.path.join(d, f), t)
+        r = subprocess.run([REF, "-conf", "net.conf", "-pro", "net.pro"] + flags + ["-t", "4"], cwd=t,
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.exit("reference failed on %s -t 4: %s" % (d, r.stderr[-400:]))
+        data = open(os.path.join(t, "network.log"), "rb").read()
+    p = os.path.join(d, "logs.json")
+    rec = json.load(open(p))
+    rec["network.log -t 4"] = {"bytes": len(data), "sha256": hashlib.sha256(data).hexdigest()}
+    with open(p, "w") as f:
+        json.dump(rec, f, indent=1, sort_keys=True)
+
+
 def logs_only():
     for name in sorted(os.listdir(HERE)):
         d = os.path.join(HERE, name)
@@ -162,6 +181,7 @@ def logs_only():
                 sys.exit("reference failed on %s: %s" % (name, r.stderr[-400:]))
             record_logs(t)
             shutil.copy(os.path.join(t, "logs.json"), d)
+        record_threaded_log(d, flags)
         print(name, open(os.path.join(d, "logs.json")).read().replace("\n", " "))
 
 
@@ -186,6 +206,7 @@ def main():
         if r.returncode != 0:
             sys.exit("reference failed on %s: %s" % (name, r.stderr[-400:]))
         record_logs(d)
+        record_threaded_log(d, cs["flags"])
         outs = sorted(f for f in os.listdir(d) if f not in ("net.conf", "net.pro", "cmd.json", "logs.json"))
         print(name, outs)
 

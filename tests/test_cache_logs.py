@@ -4,7 +4,8 @@
   the parsed model and network.log (NetSimGnl2::logDataWrite,
   code/NetSimGnl2_info.cpp:93-546) written from the built network are
   byte-identical to the reference's for every golden case (size and SHA-256
-  recorded in tests/golden/<case>/logs.json).
+  recorded in tests/golden/<case>/logs.json), network.log also for the
+  reference run with -t 4, whose set-up draws depend on the thread count.
 * A model read back from the cache drives the oracle to the same output files
   as the reference, byte for byte, and its counts and seeds equal a fresh load.
 * Any change of the .conf, the .pro or a load option misses the cache; a
@@ -32,6 +33,16 @@ def test_network_log_matches_reference(built, case, tmp_path):
     p = str(tmp_path / "network.log")
     m.network_log(p)
     assert file_digest(p) == golden_log_digest(case, "network.log")
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_threaded_setup_matches_reference(built, case, tmp_path):
+    # -t 4 changes the reference's set-up draws (its run is not reproducible
+    # with several threads, its set-up is); network.log lists every synapse
+    m = model_for(built, case, threads=4)
+    p = str(tmp_path / "network.log")
+    m.network_log(p)
+    assert file_digest(p) == golden_log_digest(case, "network.log -t 4")
 
 
 def _copy_case(case, d):
