@@ -100,6 +100,12 @@ struct Params {
   float *outI;                      // [steps][5][n] Irep per step (or null)
   uint32_t *outNS;                  // [steps][n] LIF state word per step (or null)
   float rg[5];                      // synaptic gain per receptor (scales every weight; 1 = as built)
+  // gap junctions (or null): terms of neuron p are [gap_row[p], gap_row[p+1])
+  // (other neuron, conductance); Vg [2][n] holds V at the end of the last two
+  // steps (parity of the step), which the next step's gap currents read
+  const uint32_t *gap_row, *gap_other;
+  const float *gap_w;
+  void *Vg;
 };
 
 // ---- Philox-4x32-10 -------------------------------------------------------
@@ -468,7 +474,8 @@ __device__ __forceinline__ void draw_inputs(const Params &P, uint32_t p0, uint32
 template <class T, int PD>
 __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint32_t np, uint32_t sb, uint32_t L,
                                              T (*gn)[TileW<T>::W], const uint8_t (*hits)[TileW<T>::W],
-                                             const T (*gauss)[TileW<T>::W], const SpikeList<T> &lst) {
+                                             const T (*gauss)[TileW<T>::W], const SpikeList<T> &lst,
+                                             const T *gapI) {
   const uint32_t tid = threadIdx.x, lane = tid & 31;
   const uint32_t n = P.n, S = P.slots, mask = P.mask;
   const bool own = tid < np;
@@ -564,6 +571,7 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
       g[FS_NMDA] = g[FS_NMDA] + extg[FS_NMDA] * es;
     }
     if (a & FS_ACT_INJ) isyn = (T)gauss[j][qs];
+    if (P.gap_row) isyn = isyn + gapI[qs];  // batches of one step (interval 1)
     // VmEul + firing (code/EqsGnl2.cpp:152-251)
     bool fire_now = false;
     if (ns & FS_NS_FIRE) {
@@ -714,6 +722,7 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
   }
   if (own) {
     ((T *)P.V)[p] = V;
+    if (P.gap_row) ((T *)P.Vg)[(size_t)((P.t0 + sb) & 1u) * n + p] = V;
     P.Count[p] = cnt;
     P.NS[p] = ns;
 #pragma unroll
@@ -739,9 +748,10 @@ __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32
   // FP64 tiles are half as wide so the per-tile buffers stay in static
   // shared memory
   constexpr uint32_t kT = TileW<T>::W;
-  constexpr uint32_t kCap = sizeof(T) == 4 ? 512 : 192;
+  constexpr uint32_t kCap = sizeof(T) == 4 ? 448 : 192;
   __shared__ T gn[kLB][kT];
   __shared__ T gauss[kLB][kT];
+  __shared__ T gapI[kT];
   __shared__ uint8_t hits[kLB][kT];
   __shared__ uint32_t l_n, l_p[kCap];
   __shared__ uint16_t l_tm[kCap];
@@ -763,9 +773,25 @@ __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32
         }
         else nmda_pull<T>(P, tp0, np, P.t0 + bs, L, gn, wid, lane);
         draw_inputs<T>(P, tp0, np, P.t0 + bs, L, hits, gauss);
+        if (P.gap_row) {
+          // gap currents of this step (interval 1): g (V_other - V_self) over
+          // V at the end of the previous step (none before the first step)
+          const uint64_t t = P.t0 + bs;
+          for (uint32_t q = tid; q < np; q += kThreads) {
+            T acc = (T)0;
+            if (t > 0) {
+              const T *vp = (const T *)P.Vg + (size_t)((t - 1u) & 1u) * P.n;
+              const uint32_t pq = tp0 + q;
+              const T vs = __ldcg(vp + pq);
+              for (uint32_t e = __ldg(P.gap_row + pq), e1 = __ldg(P.gap_row + pq + 1); e < e1; e++)
+                acc = acc + (T)__ldg(P.gap_w + e) * (__ldcg(vp + __ldg(P.gap_other + e)) - vs);
+            }
+            gapI[q] = acc;
+          }
+        }
         __syncthreads();
         // warps without neurons in this tile skip the steps
-        if ((tid & ~31u) < np) neuron_steps<T, PD>(P, tp0, np, bs, L, gn, hits, gauss, lst);
+        if ((tid & ~31u) < np) neuron_steps<T, PD>(P, tp0, np, bs, L, gn, hits, gauss, lst, gapI);
         __syncthreads();
         // the batch's spikes: with fewer spikes than warps the whole block
         // walks each spike's out-edges (a hub's hundreds of edges in one or
@@ -996,10 +1022,11 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
     err = "production modes do not implement LTP (use FS_MODE_COMPAT)";
     return FS_ERR_UNSUPPORTED;
   }
-  if (d->compat && d->compat->gap_rowptr && d->compat->gap_rowptr[n] != 0) {
-    err = "production modes do not implement gap junctions (use FS_MODE_COMPAT)";
-    return FS_ERR_UNSUPPORTED;
-  }
+  // gap junctions: the per-neuron term lists of the compat layout (other
+  // neuron, conductance), applied with a one-step lag as the reference does
+  // (its Spike phase adds them to Isyn for the next step's VmEul,
+  // code/EqsGnl2.cpp:705-725, :982-999)
+  const bool gap = d->compat && d->compat->gap_rowptr && d->compat->gap_rowptr[n] != 0;
   Prod *p = new Prod();
   p->fp64 = (o.mode == FS_MODE_FP64);
   p->n = n;
@@ -1066,6 +1093,7 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
     P.mask = S - 1;
   }
   P.interval = std::max<uint32_t>(1, dmin);
+  if (gap) P.interval = 1;  // a gap current reads every neuron's V of the step before
   for (int r = 0; r < 4; r++) P.lin_of_rec[r] = present[r] ? (int)(p->nlin++) : -1;
   P.nlin = p->nlin;
   for (auto &x : pdf) if (x < 0) x = 0;
@@ -1187,6 +1215,17 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
     P.in_row = nullptr;
   }
   UPU(block_post, block_post.data(), block_post.size());
+  if (gap) {
+    const uint32_t ng = d->compat->gap_rowptr[n];
+    UPU(gap_row, d->compat->gap_rowptr, (size_t)n + 1);
+    UPU(gap_other, d->compat->gap_other, ng);
+    UPF(gap_w, d->compat->gap_g, ng);
+    if ((rc = dup(p, (uint8_t **)&P.Vg, (const uint8_t *)nullptr, 2 * n * T, st, err))) goto fail;
+  } else {
+    P.gap_row = P.gap_other = nullptr;
+    P.gap_w = nullptr;
+    P.Vg = nullptr;
+  }
   if ((rc = dal(p, &p->bar, 64, err)) || (rc = dal(p, &p->err, 1, err)) ||
       (rc = dup(p, &p->spike_total, (const unsigned long long *)nullptr, 1, st, err)))
     goto fail;
@@ -1252,6 +1291,7 @@ int prod_reset(Prod *p, uint32_t seed, cudaStream_t st, std::string &err) {
   z(P.st_pre, 4 * n * T); z(P.x_pre, n * T); z(P.s_pre, n * T); z(P.s_hist, (size_t)P.slots * n * T * (p->fp64 ? 1 : kSH));
   z(P.Count, n * 4); z(P.NS, n * 4); z(P.Cap, n * 4); z(P.Car, n * 4); z(P.nspk, n * 4); z(P.Irep, (size_t)5 * n * 4);
   z(P.ring, (size_t)std::max<uint32_t>(1, p->nlin) * P.slots * n * 8);
+  z(P.Vg, 2 * n * T);
   z(p->err, 4);
   z(p->spike_total, 8);
   if (e == cudaSuccess) {
@@ -1854,6 +1894,7 @@ void state_regions(Prod *p, std::vector<std::pair<void *, size_t>> &r) {
   r.push_back({P.nspk, n * 4});
   r.push_back({P.Irep, (size_t)5 * n * 4});
   r.push_back({P.ring, (size_t)std::max<uint32_t>(1, p->nlin) * P.slots * n * 8});
+  if (P.Vg) r.push_back({P.Vg, 2 * n * T});
   r.push_back({p->spike_total, 8});
 }
 }  // namespace

@@ -246,8 +246,10 @@ def write_connectome(c: Connectome, path: str, with_delays: bool = True) -> None
 
 def write_two_pop(path: str, n_e: int = 800, n_i: int = 200, p: float = 0.2,
                   freq_ext: float = 2400.0, ampa: float = 0.05, nmda: float = 0.02,
-                  gaba: float = 8.0, extra_pop: str = "", delay_ms: float = 0.0) -> None:
-    """E/I two-population network (the CPU-runnable plain method)."""
+                  gaba: float = 8.0, extra_pop: str = "", delay_ms: float = 0.0,
+                  gap: float = 0.0, gap_p: float = 0.02) -> None:
+    """E/I two-population network (the CPU-runnable plain method); gap > 0
+    adds gap junctions E->E and I->I (MeanEff gap, Connectivity gap_p)."""
     dl = ("Delay=%s\n" % _fmt(delay_ms)) if delay_ms > 0 else ""
     recs = """Receptor:AMPA
 Tau=2
@@ -268,8 +270,11 @@ RevPot=0
 EndReceptor
 """.format(f=_fmt(freq_ext))
     body = ""
-    for name, n, links in (("E", n_e, (("E", "AMPA", ampa), ("I", "AMPA", ampa), ("E", "NMDA", nmda), ("I", "NMDA", nmda))),
-                           ("I", n_i, (("E", "GABA", gaba), ("I", "GABA", gaba)))):
+    gl_e = (("E", "GAP", gap, gap_p),) if gap > 0 else ()
+    gl_i = (("I", "GAP", gap, gap_p),) if gap > 0 else ()
+    for name, n, links in (("E", n_e, tuple((t, r, e, p) for t, r, e in (("E", "AMPA", ampa), ("I", "AMPA", ampa),
+                                                                       ("E", "NMDA", nmda), ("I", "NMDA", nmda))) + gl_e),
+                           ("I", n_i, tuple((t, r, e, p) for t, r, e in (("E", "GABA", gaba), ("I", "GABA", gaba))) + gl_i)):
         body += """NeuralPopulation: {name}
 N={n}
 C=0.5
@@ -282,9 +287,10 @@ SpikeDly=0
 
 {recs}
 """.format(name=name, n=n, recs=recs)
-        for tgt, rec, eff in links:
+        for tgt, rec, eff, pc in links:
             body += ("TargetPopulation: {t}\nTargetReceptor={r}\nMeanEff={e}\nConnectivity={p}\n{dl}"
-                     "EndTargetPopulation\n\n").format(t=tgt, r=rec, e=_fmt(eff), p=_fmt(p), dl=dl)
+                     "EndTargetPopulation\n\n").format(t=tgt, r=rec, e=_fmt(eff), p=_fmt(pc),
+                                                        dl=dl if rec != "GAP" else "")
         body += "EndNeuralPopulation\n\n"
     with open(path, "w") as f:
         f.write(body + extra_pop)

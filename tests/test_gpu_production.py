@@ -161,6 +161,35 @@ def test_two_population_fp32_vs_fp64_and_compat(built):
     assert dr.max() < 0.02 and dcv.max() < 0.05, (dr, dcv)
 
 
+def test_gap_junctions_fp32_fp64_and_compat(built, tmp_path):
+    # E/I network with gap junctions (E-E and I-I): the production modes run
+    # them with the reference's one-step lag (interval 1); the coupling must
+    # matter (compat rates with and without it differ) and the production
+    # rates and ISI CVs hold to compat and to each other
+    from flysim_b200 import netgen
+    pro = os.path.join(GOLDEN, "two_pop", "net.pro")
+    groups = np.r_[np.zeros(800, np.int64), np.ones(200, np.int64)]
+    rates = {}
+    for gap in (0.0, 0.002):
+        conf = str(tmp_path / ("g%s.conf" % gap))
+        netgen.write_two_pop(conf, gap=gap)
+        m = built.Model(conf, pro)
+        e = built.Engine(m.desc(), "compat", chunk_steps=10000)
+        try:
+            e.reset(1)
+            _, t, k = _raster(e, 20000)
+        finally:
+            e.close()
+        rates[gap] = _pop_stats(t, k, groups, 1000, 2.0)[0]
+    assert rates[0.002][0] < 0.85 * rates[0.0][0], rates  # the gap coupling lowers the E rate
+    desc = m.desc()
+    first, dr, dcv, r = _compare_modes(built, desc, 1000, groups, 100000, "fp32", "fp64")
+    assert first >= 500, "rasters differ at step %d (< 50 ms)" % first
+    assert np.all(r > 5.0) and dr.max() < 0.02 and dcv.max() < 0.05, (r, dr, dcv)
+    _, dr, dcv, _ = _compare_modes(built, desc, 1000, groups, 100000, "fp32", "compat")
+    assert dr.max() < 0.02 and dcv.max() < 0.05, (dr, dcv)
+
+
 def _conn_net(n=2000, seed=3):
     from flysim_b200 import netgen, network
     c = netgen.connectome(n=n, regions=max(2, n // 345), seed=seed)
