@@ -84,6 +84,38 @@ def _small_conf(path):
         f.write(s)
 
 
+def _keywords_case(d):
+    """Less common keywords: LeakyConductance (shown in ConfsInfo.log only),
+    MeanExtCon, the LTP_* parameters (with -LTP, on single-target records),
+    a CurrentInjec event on a group, the SubType keyword, a group output."""
+    recs = ("Receptor:AMPA\nTau=3\nRevPot=0\nFreqExt=2500\nMeanExtEff=2.0\nMeanExtCon=1.5\nEndReceptor\n\n"
+            "Receptor:GABA\nTau=5\nRevPot=-70\nEndReceptor\n\n"
+            "Receptor:NMDA\nTau=80\nTauXT=2\nRevPot=0\nEndReceptor\n\n")
+    conf = ""
+    for name, n, extra, links in (
+            ("P", 30, "LeakyConductance=20\nLTP_tLP=30\nLTP_SpiLPDy=2\nLTP_PosISI=0.02\nLTP_NegISI=-0.01\n",
+             (("Q", "AMPA", 1.5, 0.02), ("Q", "NMDA", 0.3, 0.02), ("P", "AMPA", 0.2, 0.3))),
+            ("Q", 20, "", (("P", "GABA", 2, 0.5), ("P", "AMPA", 1.0, 0.01)))):
+        conf += ("NeuralPopulation: %s\nN=%d\nC=0.5\nTaum=15\nRestPot=-65\nThreshold=-50\nResetPot=-60\n"
+                 "RefractoryPeriod=2\nSpikeDly=0.5\n%s\n%s") % (name, n, extra, recs)
+        for tgt, rec, eff, conn in links:
+            conf += ("TargetPopulation: %s\nTargetReceptor=%s\nMeanEff=%s\nConnectivity=%s\n"
+                     "EndTargetPopulation\n\n") % (tgt, rec, eff, conn)
+        conf += "EndNeuralPopulation\n\n"
+    with open(os.path.join(d, "net.conf"), "w") as f:
+        f.write(conf)
+    pro = ("DefineMacro\nGroupName:PQ\nGroupMembers:P,Q\nEndGroupMembers\nRandomSeeds: 77\nEndRandomSeeds\n"
+           "EndDefineMacro\n\n"
+           "EventTime 40\nType=CurrentInjec\nLabel=inj\nPopulation: PQ\nGaussMean=0.2\nGaussSTD=0.5\nEndEvent\n\n"
+           "EventTime 80\nType=ChangeExtFreq\nLabel=#2#\nPopulation: Q\nSubType: AMPA\nFreqExt=0\nEndEvent\n\n"
+           "EventTime 150\nType=EndTrial\nLabel=End_of_the_trial\nEndEvent\n\n"
+           "OutControl\nFileName:Spikes.dat\nType=Spike\npopulation:AllPopulation\nEndOutputFile\n\n"
+           "FileName:FR.dat\nType=FiringRate\nFiringRateWindow=20\nPrintStep=10\npopulation:PQ\nEndOutputFile\n\n"
+           "EndOutControl\n")
+    with open(os.path.join(d, "net.pro"), "w") as f:
+        f.write(pro)
+
+
 def cases():
     c = {}
     c["two_pop"] = dict(conf=lambda p: netgen.write_two_pop(p),
@@ -123,6 +155,7 @@ def cases():
                  {"name": "FRates.dat", "type": "FiringRate", "pop": "Exc2", "win": 50, "step": 10}],
         events=[{"t": 300, "type": "ChangeExtFreq", "pop": "Exc1", "f": 24000},
                 {"t": 650, "type": "ChangeMembraneNoise", "pop": "Exc1", "mean": 0.43, "std": 0.03}]), flags=[])
+    c["keywords"] = dict(raw=_keywords_case, flags=["-LTP"])
     # command-line options: user seed (which also switches STD on, as the
     # reference's flag parser does), a non-default time step, and the
     # -om / -os / -or outputs added on top of the .pro's
@@ -197,8 +230,11 @@ def main():
         d = os.path.join(HERE, name)
         shutil.rmtree(d, ignore_errors=True)
         os.makedirs(d)
-        cs["conf"](os.path.join(d, "net.conf"))
-        netgen.write_pro(os.path.join(d, "net.pro"), **cs["pro"])
+        if "raw" in cs:
+            cs["raw"](d)
+        else:
+            cs["conf"](os.path.join(d, "net.conf"))
+            netgen.write_pro(os.path.join(d, "net.pro"), **cs["pro"])
         with open(os.path.join(d, "cmd.json"), "w") as f:
             json.dump(cs["flags"], f)
         r = subprocess.run([REF, "-conf", "net.conf", "-pro", "net.pro"] + cs["flags"], cwd=d,
