@@ -203,17 +203,83 @@ def cpu_baseline_port(c, samples: int = 2000):
                       "oracle/fs_oracle.cpp single thread, %.2f s wall" % (samples, samples * DT, dt_wall)}
 
 
+def same_network_block(c, args, world, rank, flush, barrier, cap_hint: float):
+    """value and e2e of the FP32 engine on the delays-0 form of the bench
+    network (what --impl reference runs), with its mean rate; every rank runs
+    its replica, the figures are the slowest rank's."""
+    import flysim_b200 as fb
+    from flysim_b200 import network
+    na0 = network.connectome_net(c, dt=DT, with_delays=False)
+    local = _env_int("LOCAL_RANK", 0)
+    eng = fb.Engine(na0.desc, "fp32", device=local, chunk_steps=STEPS_PER_BENCH_STEP)
+    try:
+        eng.reset(SEED + rank)
+        for _ in range(max(1, args.warmup)):
+            eng.run_timed(STEPS_PER_BENCH_STEP)
+        s0 = eng.stats()
+        k = max(1, min(args.steps, 5))
+        ms = []
+        for _ in range(k):
+            flush.zero_()
+            barrier()
+            ms.append(eng.run_timed(STEPS_PER_BENCH_STEP))
+            barrier()
+        kern = eng.kernel_time()[0]
+        s1 = eng.stats()
+        tot = max_over_ranks(float(np.sum(ms)), world)
+        sim_s = k * STEPS_PER_BENCH_STEP * DT * 1e-3
+        spikes = s1["spikes"] - s0["spikes"]
+        # e2e: drive table up, spike lists down, per bench step
+        pb_host = np.ascontiguousarray(na0.fields["pb"].reshape(5, na0.n)[0])
+        cuts = np.flatnonzero(np.diff(c.region)) + 1
+        starts = np.concatenate([[0], cuts])
+        bounds = list(zip(starts, np.concatenate([cuts, [na0.n]])))
+        cap = int(2 * cap_hint) + STEPS_PER_BENCH_STEP * 64
+        walls = []
+        d2h = 0
+        for i in range(3):
+            flush.zero_()
+            barrier()
+            t0 = time.perf_counter()
+            for lo, hi in bounds:
+                eng.set_drive(int(lo), int(hi - lo), 0, float(pb_host[lo]))
+            counts, idx = eng.step_csr(STEPS_PER_BENCH_STEP, spike_cap=cap)
+            t1 = time.perf_counter()
+            if i:
+                walls.append(t1 - t0)
+            d2h = 4 * STEPS_PER_BENCH_STEP + 4 * int(idx.size) + 4
+        e2e_s = max_over_ranks(float(np.median(walls)), world)
+        return {"workload": "the same connectome-shaped network with delays 0 (as --impl reference runs it), "
+                            "fp32 mode; one step = 1 s simulated (10,000 timesteps)",
+                "value": world * sim_s / (tot * 1e-3), "unit": UNIT, "steps": k,
+                "us_per_timestep": 1e3 * tot / (k * STEPS_PER_BENCH_STEP),
+                "kernel_ms_per_launch": kern,
+                "mean_rate_hz": spikes / (k * STEPS_PER_BENCH_STEP * DT * 1e-3) / na0.n,
+                "e2e": {"value": world * STEPS_PER_BENCH_STEP * DT * 1e-3 / e2e_s, "unit": UNIT,
+                        "h2d_bytes_per_step": int(32 * na0.n), "d2h_bytes_per_step": int(d2h)}}
+    finally:
+        eng.close()
+
+
 def run_reference(args, rank):
-    """--impl reference: the reference binary on the same network (delays 0)."""
-    ref = os.path.join(ROOT, "oracle", "_ref", "flysim_ref")
+    """--impl reference: the reference binary on the same network (delays 0).
+
+    One bench step = one repeat (-rp) of a trial of FS_REF_TRIAL_MS (default
+    200 ms) simulated, timed by the reference's own Run-phase timer; the
+    first W repeats are discarded.  The build is FS_REF_BUILD (stock or ftz,
+    the -mdaz-ftz build of the same sources; default stock) at -t = all host
+    threads (FS_REF_THREADS overrides)."""
+    build = os.environ.get("FS_REF_BUILD", "stock")
+    ref = os.path.join(ROOT, "oracle", "_ref", "flysim_ref" + ("_ftz" if build == "ftz" else ""))
     if rank != 0:
         return 0
     if not os.path.exists(ref):
-        print(json.dumps({"impl": "reference", "unavailable": "reference binary oracle/_ref/flysim_ref not built"}))
+        print(json.dumps({"impl": "reference", "unavailable": "reference binary %s not built" %
+                          os.path.relpath(ref, ROOT)}))
         return 0
     from flysim_b200 import netgen
     c, _ = build_network(0)
-    sample_ms = float(os.environ.get("FS_REF_SAMPLE_MS", "20"))
+    sample_ms = float(os.environ.get("FS_REF_TRIAL_MS", "200"))
     reps = args.warmup + args.steps
     tmp = tempfile.mkdtemp()
     try:
@@ -221,7 +287,7 @@ def run_reference(args, rank):
         seeds = [SEED + i for i in range(reps)]
         netgen.write_pro(os.path.join(tmp, "net.pro"), sample_ms, seeds=seeds,
                          outputs=({"name": "Spikes.dat", "type": "Spike", "pop": "AllPopulation"},))
-        threads = os.cpu_count() or 1
+        threads = _env_int("FS_REF_THREADS", os.cpu_count() or 1)
         t0 = time.time()
         r = subprocess.run([ref, "-conf", "net.conf", "-pro", "net.pro", "-rp", str(reps), "-t", str(threads)],
                            cwd=tmp, capture_output=True, text=True, timeout=3600)
@@ -246,14 +312,15 @@ def run_reference(args, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / len(timed),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "connectome-shaped network, 20000 neurons / 58 regions / %d connections, "
-                               "delays 0 (the reference has none), dt 0.1 ms; one step = %g ms simulated"
-                               % (c.n_connections, sample_ms),
-                   "threads": threads, "setup_and_run_s": round(setup_and_run, 1)},
+                               "delays 0 (the reference has none), dt 0.1 ms; one step = one repeat of a "
+                               "%g ms trial" % (c.n_connections, sample_ms),
+                   "threads": threads, "build": build, "setup_and_run_s": round(setup_and_run, 1)},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": "%d repeats of %g ms simulated, flysim reference -t %d, Run-phase timer"
-                                   % (len(timed), sample_ms, threads)},
+                         "sample": "%d repeats of a %g ms trial (after %d discarded), flysim reference (%s build) "
+                                   "-t %d, Run-phase timer" % (len(timed), sample_ms, args.warmup, build, threads)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "spikes_per_step": spikes / max(1, len(timed)),
+        "mean_rate_hz": spikes / max(1, len(timed)) / (sample_ms * 1e-3) / c.n,
     }
     print(json.dumps(line))
     return 0
@@ -267,6 +334,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-same-network", action="store_true",
+                    help="skip the delays-0 measurement of the network the reference arm runs")
     ap.add_argument("--workload", default="connectome20k", choices=sorted(WORKLOADS))
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="run this many timesteps once and exit (for ncu captures)")
@@ -366,6 +435,14 @@ def main():
         e2e = {"value": world * STEPS_PER_BENCH_STEP * DT * 1e-3 / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 
+    # the same network with delays 0: the form the reference can express and
+    # the one --impl reference times, measured the same way (device-resident
+    # value, e2e through the C ABI with host copies), so the two arms'
+    # figures compare like for like
+    same = None
+    if args.workload == "connectome20k" and not args.no_same_network:
+        same = same_network_block(c, args, world, rank, flush, barrier, cap_hint=spikes / max(1, args.steps))
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -402,6 +479,7 @@ def main():
             "clocks": clk,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "same_network": same,
         }
         print(json.dumps(line))
     eng.close()

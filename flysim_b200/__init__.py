@@ -26,6 +26,7 @@ FS_OK, FS_ERR_ARG, FS_ERR_CUDA, FS_ERR_NOMEM, FS_ERR_CAPACITY, FS_ERR_PARSE, FS_
     FS_ERR_TIMEOUT, FS_ERR_IO, FS_ERR_NODEVICE = range(10)
 FS_AMPA, FS_GABA, FS_ACH, FS_GCL, FS_NMDA, FS_NREC = 0, 1, 2, 3, 4, 5
 FS_MODE_COMPAT, FS_MODE_FP32, FS_MODE_FP64 = 0, 1, 2
+FS_RUN_INTERVAL_KERNEL = 1
 MODES = {"compat": FS_MODE_COMPAT, "fp32": FS_MODE_FP32, "fp64": FS_MODE_FP64}
 ACT = dict(AMPA=1, GABA=2, NMDA=4, GAP=8, ACH=32, GCL=64, INJ=128, LIF=256, LTP=8192, STD=16384, STP=32768)
 NS_FIRE, NS_SPIKE = 1, 2
@@ -79,7 +80,7 @@ class NetDesc(C.Structure):
 
 class RunOpts(C.Structure):
     _fields_ = [("mode", C.c_int), ("device", C.c_int), ("chunk_steps", C.c_uint32), ("philox_key", C.c_uint64),
-                ("blocks_per_sm", C.c_uint32)]
+                ("blocks_per_sm", C.c_uint32), ("flags", C.c_uint32)]
 
 
 class StepOut(C.Structure):
@@ -136,6 +137,11 @@ def lib() -> C.CDLL:
         "fs_debug_expf_noalloc": (C.c_int, [_f, _f, C.c_uint64]),
         "fs_get_state": (C.c_int, [vp, _f, _i32, _u32]),
         "fs_debug_barrier_timeout": (C.c_int, [C.c_uint32]),
+        "fs_debug_philox": (C.c_int, [_u32, _u32, C.c_uint64, _u32]),
+        "fs_engine_layout": (C.c_int, [vp, _u32, _u32, _u32, C.POINTER(C.c_int)]),
+        "fs_debug_drive": (C.c_int, [vp, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32,
+                                     C.POINTER(C.c_uint8), C.POINTER(C.c_double)]),
+        "fs_debug_inject_wait_failure": (C.c_int, [vp]),
         "fs_checkpoint_size": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
         "fs_checkpoint_save": (C.c_int, [vp, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
         "fs_checkpoint_load": (C.c_int, [vp, C.c_void_p, C.c_uint64]),
@@ -193,7 +199,9 @@ def exported_symbols() -> Sequence[str]:
                         "fs_reset", "fs_set_drive", "fs_set_act", "fs_set_injection", "fs_step", "fs_run",
                         "fs_run_timed",
                         "fs_sync", "fs_stats", "fs_kernel_time", "fs_debug_expf", "fs_debug_expf_noalloc",
-                        "fs_get_state", "fs_debug_barrier_timeout", "fs_checkpoint_size", "fs_checkpoint_save", "fs_checkpoint_load",
+                        "fs_get_state", "fs_debug_barrier_timeout", "fs_engine_layout", "fs_debug_philox",
+                        "fs_debug_drive",
+                        "fs_debug_inject_wait_failure", "fs_checkpoint_size", "fs_checkpoint_save", "fs_checkpoint_load",
                         "fs_get_syn_state", "fs_model_load", "fs_model_load_cached", "fs_model_confs_info", "fs_model_network_log",
                         "fs_model_free", "fs_model_error",
                         "fs_model_desc", "fs_model_info", "fs_model_seed", "fs_model_run",
@@ -224,10 +232,11 @@ class Model:
 
     cache: path of a binary network cache; the model is read from it when it
     was written for the same .conf/.pro bytes and options, else parsed, built
-    and stored there.  cache_status is then "hit", "stored" or "unwritable"
-    ("off" without a cache)."""
+    and stored there.  cache_status is then "hit", "stored", "unwritable" or
+    "unseeded" (a network without a fixed seed draws a new one on every load,
+    as the reference does, and is never cached); "off" without a cache."""
 
-    CACHE_STATUS = {0: "off", 1: "hit", 2: "stored", 3: "unwritable"}
+    CACHE_STATUS = {0: "off", 1: "hit", 2: "stored", 3: "unwritable", 4: "unseeded"}
 
     def __init__(self, conf: str, pro: str, dt: float = 0.1, stp: bool = False, std: bool = False,
                  ltp: bool = False, repeats: int = 1, threads: int = 1, user_seed: Optional[int] = None,
@@ -319,10 +328,11 @@ class Engine:
     """One network instance on one GPU (fs_create ... fs_destroy)."""
 
     def __init__(self, desc, mode: str = "compat", device: int = 0, chunk_steps: int = 0, philox_key: int = 0,
-                 blocks_per_sm: int = 0):
+                 blocks_per_sm: int = 0, interval_kernel: bool = False):
         L = lib()
         self._keep = getattr(desc, "_keep", None)
-        o = RunOpts(MODES[mode], device, chunk_steps, philox_key, blocks_per_sm)
+        o = RunOpts(MODES[mode], device, chunk_steps, philox_key, blocks_per_sm,
+                    FS_RUN_INTERVAL_KERNEL if interval_kernel else 0)
         h = C.c_void_p()
         dp = desc if isinstance(desc, C._Pointer) else C.pointer(desc)
         rc = L.fs_create(dp, C.byref(o), C.byref(h))
@@ -418,6 +428,13 @@ class Engine:
         _check(lib().fs_stats(self._h, C.byref(a), C.byref(b), C.byref(c)), self._h)
         return dict(steps=a.value, spikes=b.value, launches=c.value)
 
+    def layout(self):
+        """Launch layout (production modes): blocks, threads, interval and
+        whether the single-step kernel runs the network."""
+        b, t, i, sgl = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_int()
+        _check(lib().fs_engine_layout(self._h, C.byref(b), C.byref(t), C.byref(i), C.byref(sgl)), self._h)
+        return dict(blocks=b.value, threads=t.value, interval=i.value, single_step=bool(sgl.value))
+
     def kernel_time(self):
         ms, n = C.c_double(), C.c_uint64()
         _check(lib().fs_kernel_time(self._h, C.byref(ms), C.byref(n)), self._h)
@@ -455,6 +472,21 @@ class Engine:
     def restore(self, data: bytes):
         _check(lib().fs_checkpoint_load(self._h, data, len(data)), self._h)
 
+    def drive_draws(self, t0: int, nsteps: int, first: int = 0, count: Optional[int] = None):
+        """The production drive draws of steps [t0, t0 + nsteps) for neurons
+        [first, first + count): (hits uint8 [nsteps, count], bit r = receptor
+        r hit; injection current float64 [nsteps, count], 0 where off)."""
+        count = self.n - first if count is None else count
+        hits = np.zeros((nsteps, count), np.uint8)
+        gauss = np.zeros((nsteps, count), np.float64)
+        _check(lib().fs_debug_drive(self._h, t0, nsteps, first, count, hits.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                    gauss.ctypes.data_as(C.POINTER(C.c_double))), self._h)
+        return hits, gauss
+
+    def inject_wait_failure(self):
+        """Sets the device error word as a bounded wait that gave up would."""
+        _check(lib().fs_debug_inject_wait_failure(self._h), self._h)
+
     def syn_state(self):
         g = np.zeros(FS_NREC * self.n, np.float32)
         isyn = np.zeros(self.n, np.float32)
@@ -464,6 +496,17 @@ class Engine:
 
 def device_engine_vtbl():
     return lib().fs_device_engine()
+
+
+def debug_philox(ctr: np.ndarray, key: np.ndarray) -> np.ndarray:
+    """The device Philox-4x32-10 on counters ctr [k, 4] and keys key [k, 2]."""
+    ctr = np.ascontiguousarray(ctr, np.uint32).reshape(-1, 4)
+    key = np.ascontiguousarray(key, np.uint32).reshape(-1, 2)
+    assert ctr.shape[0] == key.shape[0]
+    out = np.zeros_like(ctr)
+    _check(lib().fs_debug_philox(ctr.ctypes.data_as(_u32), key.ctypes.data_as(_u32), ctr.shape[0],
+                                 out.ctypes.data_as(_u32)))
+    return out
 
 
 def debug_expf(x: np.ndarray) -> np.ndarray:

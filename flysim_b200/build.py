@@ -87,17 +87,24 @@ def build(verbose: bool = False, tables: bool = True) -> str:
     return lib
 
 
-def build_oracle(verbose: bool = False) -> str:
-    """Test infrastructure: the CPU oracle (oracle/fs_oracle.cpp) and, when
-    the reference sources are present, the reference itself (oracle/_ref)."""
+def build_oracle(verbose: bool = False, ref_src: str | None = None) -> str:
+    """Test infrastructure: the CPU oracle (oracle/fs_oracle.cpp,
+    oracle/fs_philox.c) and, when the reference's sources are given, the
+    reference itself (oracle/_ref).  ref_src is the reference's code/
+    directory; without it the environment variable FLYSIM_REF_SRC is used,
+    and with neither the reference is not built."""
     odir = os.path.join(ROOT, "oracle", "_build")
     os.makedirs(odir, exist_ok=True)
     src = os.path.join(ROOT, "oracle", "fs_oracle.cpp")
+    csrc = os.path.join(ROOT, "oracle", "fs_philox.c")
+    cobj = os.path.join(odir, "fs_philox.o")
     lib = os.path.join(odir, "liboracle.so")
-    if _newer(lib, [src, os.path.join(INC, "flysim_b200.h")]):
-        _run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-I", INC, src, "-o", lib], verbose)
-    ref_src = "/root/reference/code"
-    if os.path.isdir(ref_src):
+    if _newer(cobj, [csrc]):
+        _run(["gcc", "-std=c11", "-O2", "-fPIC", "-ffp-contract=off", "-c", csrc, "-o", cobj], verbose)
+    if _newer(lib, [src, cobj, os.path.join(INC, "flysim_b200.h")]):
+        _run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-I", INC, src, cobj, "-o", lib, "-lm"], verbose)
+    ref_src = ref_src or os.environ.get("FLYSIM_REF_SRC")
+    if ref_src and os.path.isdir(ref_src):
         _run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "Makefile.ref"), "-j8", "REF=" + ref_src,
               "OUT=" + os.path.join(ROOT, "oracle", "_ref")], verbose)
     return lib
@@ -105,4 +112,4 @@ def build_oracle(verbose: bool = False) -> str:
 
 if __name__ == "__main__":
     print(build(verbose=True))
-    print(build_oracle(verbose=True))
+    print(build_oracle(verbose=True, ref_src=sys.argv[1] if len(sys.argv) > 1 else None))

@@ -660,6 +660,53 @@ int fs_debug_barrier_timeout(uint32_t poll_limit) {
   return FS_OK;
 }
 
+int fs_engine_layout(fs_handle *h, uint32_t *blocks, uint32_t *threads, uint32_t *interval, int *single_step) {
+  if (!h) return set_err(nullptr, FS_ERR_ARG, "null handle");
+  if (h->mode == FS_MODE_COMPAT || !h->prod)
+    return set_err(h, FS_ERR_UNSUPPORTED, "fs_engine_layout: production modes only");
+  fsp::ProdInfo pi{};
+  fsp::prod_info(h->prod, &pi);
+  if (blocks) *blocks = pi.blocks;
+  if (threads) *threads = pi.threads;
+  if (interval) *interval = pi.interval;
+  if (single_step) *single_step = pi.single_step;
+  return FS_OK;
+}
+
+int fs_debug_philox(const uint32_t *ctr, const uint32_t *key, uint64_t k, uint32_t *out) {
+  if (k == 0) return FS_OK;
+  if (!ctr || !key || !out) return set_err(nullptr, FS_ERR_ARG, "fs_debug_philox: null argument");
+  if (k > (1ull << 26)) return set_err(nullptr, FS_ERR_ARG, "fs_debug_philox: at most 2^26 blocks per call");
+  std::string err;
+  int rc = fsp::prod_debug_philox(ctr, key, k, out, err);
+  return rc ? set_err(nullptr, rc, err) : FS_OK;
+}
+
+int fs_debug_drive(fs_handle *h, uint64_t t0, uint32_t nsteps, uint32_t first, uint32_t count, uint8_t *hits,
+                   double *gauss) {
+  if (!h) return set_err(nullptr, FS_ERR_ARG, "null handle");
+  if (h->mode == FS_MODE_COMPAT || !h->prod)
+    return set_err(h, FS_ERR_UNSUPPORTED, "fs_debug_drive: the Philox drive belongs to the production modes");
+  if (!hits || !gauss) return set_err(h, FS_ERR_ARG, "fs_debug_drive: null output");
+  if ((uint64_t)first + count > h->n) return set_err(h, FS_ERR_ARG, "fs_debug_drive: neuron range out of bounds");
+  if ((uint64_t)nsteps * count > (1ull << 28)) return set_err(h, FS_ERR_ARG, "fs_debug_drive: at most 2^28 draws per call");
+  if (nsteps == 0 || count == 0) return FS_OK;
+  CK(cudaSetDevice(h->device));
+  int rc = upload_params(h);
+  if (rc) return rc;
+  rc = fsp::prod_debug_drive(h->prod, t0, nsteps, first, count, hits, gauss, h->st, h->err);
+  return rc ? set_err(h, rc, h->err) : FS_OK;
+}
+
+int fs_debug_inject_wait_failure(fs_handle *h) {
+  if (!h) return set_err(nullptr, FS_ERR_ARG, "null handle");
+  if (h->mode == FS_MODE_COMPAT || !h->prod)
+    return set_err(h, FS_ERR_UNSUPPORTED, "fs_debug_inject_wait_failure: production modes only");
+  CK(cudaSetDevice(h->device));
+  int rc = fsp::prod_inject_wait_failure(h->prod, h->st, h->err);
+  return rc ? set_err(h, rc, h->err) : FS_OK;
+}
+
 // ---- checkpoints (production modes) ----------------------------------------
 // Layout: CkptHead, the event-set parameters (pb [FS_NREC][n], act [n],
 // inj_mean [n], inj_std [n]), then the engine's state blob.
@@ -711,6 +758,10 @@ int fs_checkpoint_save(fs_handle *h, void *buf, uint64_t cap, uint64_t *bytes) {
   if (!buf) return set_err(h, FS_ERR_ARG, "fs_checkpoint_save: null buffer");
   if (cap < c.total_bytes) return set_err(h, FS_ERR_CAPACITY, "fs_checkpoint_save: buffer smaller than fs_checkpoint_size");
   CK(cudaSetDevice(h->device));
+  // the work in flight must have ended cleanly: a state whose barrier wait
+  // gave up is half an interval and is never saved
+  rc = fsp::prod_check(h->prod, h->st, &h->spikes_total, h->err);
+  if (rc) return set_err(h, rc, "fs_checkpoint_save: " + h->err);
   uint8_t *o = (uint8_t *)buf;
   const size_t n = h->n;
   std::memcpy(o, &c, sizeof c);
@@ -784,28 +835,35 @@ static const char *e_err(void *c) { return fs_last_error((fs_handle *)c); }
 static const fs_engine_vtbl kDeviceEngine = {e_reset, e_drive, e_act, e_inj, e_step, e_err};
 const fs_engine_vtbl *fs_device_engine(void) { return &kDeviceEngine; }
 
-// device expf used by the NMDA Mg block, for checks against glibc
+// device expf used by the NMDA Mg block, for checks against glibc; every
+// exit path frees the four staging buffers
 int fs_debug_expf(const float *x, float *y, uint64_t k) {
   std::vector<uint32_t> ek;
   std::vector<float> ev;
+  if (k && (!x || !y)) return set_err(nullptr, FS_ERR_ARG, "fs_debug_expf: null x or y");
+  if (!fsh::read_table(lib_dir() + "/expf_glibc.bin", ek, ev)) return set_err(nullptr, FS_ERR_IO, "missing expf table");
+  if (k == 0) return FS_OK;
+  struct Bufs {
+    float *dx = nullptr, *dy = nullptr, *dv = nullptr;
+    uint32_t *dk = nullptr;
+    ~Bufs() {
+      if (dx) cudaFree(dx);
+      if (dy) cudaFree(dy);
+      if (dk) cudaFree(dk);
+      if (dv) cudaFree(dv);
+    }
+  } b;
   fs_handle tmp;
   fs_handle *h = &tmp;
-  if (!fsh::read_table(lib_dir() + "/expf_glibc.bin", ek, ev)) return set_err(nullptr, FS_ERR_IO, "missing expf table");
-  float *dx = nullptr, *dy = nullptr, *dv = nullptr;
-  uint32_t *dk = nullptr;
-  CK(cudaMalloc(&dx, k * 4));
-  CK(cudaMalloc(&dy, k * 4));
-  CK(cudaMalloc(&dk, ek.size() * 4));
-  CK(cudaMalloc(&dv, ev.size() * 4));
-  CK(cudaMemcpy(dx, x, k * 4, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(dk, ek.data(), ek.size() * 4, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(dv, ev.data(), ev.size() * 4, cudaMemcpyHostToDevice));
-  CK(fsd::expf_ref_eval(dx, dy, k, dk, dv, (uint32_t)ek.size(), nullptr));
-  CK(cudaMemcpy(y, dy, k * 4, cudaMemcpyDeviceToHost));
-  cudaFree(dx);
-  cudaFree(dy);
-  cudaFree(dk);
-  cudaFree(dv);
+  CK(cudaMalloc(&b.dx, k * 4));
+  CK(cudaMalloc(&b.dy, k * 4));
+  CK(cudaMalloc(&b.dk, ek.size() * 4));
+  CK(cudaMalloc(&b.dv, ev.size() * 4));
+  CK(cudaMemcpy(b.dx, x, k * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b.dk, ek.data(), ek.size() * 4, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b.dv, ev.data(), ev.size() * 4, cudaMemcpyHostToDevice));
+  CK(fsd::expf_ref_eval(b.dx, b.dy, k, b.dk, b.dv, (uint32_t)ek.size(), nullptr));
+  CK(cudaMemcpy(y, b.dy, k * 4, cudaMemcpyDeviceToHost));
   return FS_OK;
 }
 

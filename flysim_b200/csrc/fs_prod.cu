@@ -35,6 +35,7 @@
 // S = next power of two >= max_delay + min_delay + 2 keeps the reuse of a
 // slot out of any interval that still reads it.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -61,6 +62,7 @@ enum { PL_NONE = 0, PL_STD = 1, PL_STP = 2, PL_TM = 3 };
 
 struct Params {
   uint32_t n, slots, mask, interval, nlin;
+  uint32_t dmax0;                        // every delay is 0 (single-step pull order)
   int lin_of_rec[4];
   const float *Vth, *El, *gl, *Cm, *Vreset, *df, *ef, *dVmax;
   const int32_t *RfPed, *SpiDy;
@@ -106,6 +108,27 @@ struct Params {
   const uint32_t *gap_row, *gap_other;
   const float *gap_w;
   void *Vg;
+  // single-step kernel k_prod1 (null unless the network takes it): per
+  // block, the presynaptic neurons it tracks (sorted ids, NMDA kinetics
+  // class, rows of their linear synapses onto the block's posts), the NMDA
+  // in-edges of its posts as (tracked index, weight) in CSR order, and the
+  // spike lists of the last two steps
+  const struct Blk1 *b1;
+  const uint32_t *t1_gid, *t1_lrow, *t1_lin, *t1_erow;
+  const uint8_t *t1_cls;
+  const float *t1_linw, *t1_ew, *t1_cls_tab;
+  const uint16_t *t1_eidx;
+  uint32_t t1_ncls, t1_smem;
+  uint32_t *t1_cnt;      // [2] spikes listed in the step of each parity
+  uint4 *t1_list;        // [2][n][2] (id, inc, c0, c1), (c2, c3, 0, 0)
+};
+
+// Block plan of k_prod1: posts [post0, post0 + np), tracked neurons [trk0,
+// trk0 + ntrk) of the t1 arrays (their linear rows at lrow0, ntrk + 1
+// offsets), NMDA edges [e0, e0 + ne), edge rows at erow0 (np + 1 offsets),
+// linear delivery entries from l0.
+struct Blk1 {
+  uint32_t post0, np, trk0, ntrk, lrow0, e0, ne, erow0, l0, pad;
 };
 
 // ---- Philox-4x32-10 -------------------------------------------------------
@@ -195,6 +218,13 @@ template <>
 __device__ __forceinline__ float exp_t<float>(float x) { return expf(x); }
 template <>
 __device__ __forceinline__ double exp_t<double>(double x) { return exp(x); }
+
+template <class T>
+__device__ __forceinline__ T fma_t(T a, T b, T c);
+template <>
+__device__ __forceinline__ float fma_t<float>(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+template <>
+__device__ __forceinline__ double fma_t<double>(double a, double b, double c) { return __fma_rn(a, b, c); }
 
 template <class T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -300,58 +330,33 @@ __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint
   }
 }
 
-// Single-step batches (networks whose minimum delay is 0 or 1 step pull
-// every step, and the last step of a call that ends one step into an
-// interval): each edge needs one value, so a warp takes four posts at once
-// with scalar loads, four times the edges in flight of the window path.
-// Lane (g, k) of the warp (lane = 4g + k) sums post k's edges g, g + 8,
-// g + 16, ... in order and the same xor 4, 8, 16 butterfly combines the
-// eight g, which is exactly the quad path's order for step 0: a step's
-// NMDA sum does not depend on the batch it falls in.
+// Single-step pull of networks whose delays are all 0 (every network in the
+// reference's own format): one warp per post, lane l summing the post's
+// edges l, l + 32, l + 64, ... in order (fused multiply-adds), then an xor
+// butterfly over 16, 8, 4, 2, 1.  The single-step persistent kernel
+// (k_prod1) sums its shared-memory copy of the same edges in the same
+// order, so a batch instance equals its solo run bit for bit.
 __device__ __forceinline__ void nmda_pull1_f32(const Params &P, uint32_t p0, uint32_t np, uint64_t tb,
                                                float (*gn)[kTile], uint32_t wid, uint32_t lane) {
-  constexpr int PG = 4;             // posts per warp at once
-  constexpr int U = 4;              // edges per lane per round
-  constexpr uint32_t CH = 8u * U;   // edges of a post per round
   const float *sh = (const float *)P.s_hist;
   const uint32_t S = P.slots, mask = P.mask;
   const uint32_t nw = kThreads / 32;
-  const uint32_t k = lane & 3u, g = lane >> 2;
   if (!P.in_row) {
     for (uint32_t q = wid * 32 + lane; q < np; q += nw * 32) gn[0][q] = 0.0f;
     return;
   }
-  for (uint32_t q0 = wid * PG; q0 < np; q0 += nw * PG) {
-    const uint32_t q = q0 + k;
-    const bool qv = q < np;
-    const uint32_t b0 = qv ? __ldg(P.in_row + p0 + q) : 0u, b1 = qv ? __ldg(P.in_row + p0 + q + 1) : 0u;
-    uint32_t nch = (b1 - b0 + CH - 1) / CH;
-#pragma unroll
-    for (int o = 1; o < PG; o <<= 1) nch = max(nch, __shfl_xor_sync(fsd::kFull, nch, o));
+  const uint32_t slot = (uint32_t)(tb - 1u) & mask;
+  for (uint32_t q = wid; q < np; q += nw) {
+    const uint32_t b0 = __ldg(P.in_row + p0 + q), b1 = __ldg(P.in_row + p0 + q + 1);
     float acc = 0.0f;
-    for (uint32_t c = 0; c < nch; c++) {
-      uint32_t code[U];
-      float w[U], v[U];
-#pragma unroll
-      for (int u = 0; u < U; u++) {
-        const uint32_t e = b0 + c * CH + g + 8u * u;
-        const bool ok = e < b1;
-        code[u] = ok ? __ldg(P.in_code + e) : 0u;
-        w[u] = ok ? __ldg(P.in_w + e) : 0.0f;
-      }
-#pragma unroll
-      for (int u = 0; u < U; u++) {
-        const uint32_t e = b0 + c * CH + g + 8u * u;
-        const uint32_t pre = code[u] & 0xffffffu, d = code[u] >> 24;
-        // row 0 of the shifted copies holds slot i at element i
-        v[u] = e < b1 ? __ldca(sh + (size_t)pre * kSH * S + ((uint32_t)(tb - 1u - d) & mask)) : 0.0f;
-      }
-#pragma unroll
-      for (int u = 0; u < U; u++) acc += w[u] * v[u];
+    for (uint32_t e = b0 + lane; e < b1; e += 32) {
+      const uint32_t pre = __ldg(P.in_code + e) & 0xffffffu;
+      // row 0 of the shifted copies holds slot i at element i
+      acc = __fmaf_rn(__ldg(P.in_w + e), __ldca(sh + (size_t)pre * kSH * S + slot), acc);
     }
 #pragma unroll
-    for (int o = 4; o < 32; o <<= 1) acc += __shfl_xor_sync(fsd::kFull, acc, o);
-    if (g == 0 && qv) gn[0][q] = acc;
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(fsd::kFull, acc, o);
+    if (lane == 0) gn[0][q] = acc;
   }
 }
 
@@ -429,39 +434,303 @@ struct SpikeList {
   uint32_t cap;
 };
 
-// ---- drive draws of L steps for a tile -------------------------------------
+// ---- drive draws -----------------------------------------------------------
 // The external Bernoulli outcomes (bit r: receptor r hit this step) and the
-// injection noise depend on no state, so they are drawn for the whole batch
-// by all threads at once, off the neurons' per-step dependency chain.
+// injection noise of neuron p at step t depend on no state: Philox block 0
+// keyed by (t, p) gives the four linear receptors' uniforms, block 1 (drawn
+// only for a neuron with NMDA drive or injection) the NMDA uniform and the
+// Box-Muller pair.
+template <class T>
+__device__ __forceinline__ uint32_t draw_one(const Params &P, uint32_t p, uint64_t t, T &gauss) {
+  const uint32_t n = P.n;
+  const uint32_t a = __ldg(P.act + p);
+  uint32_t rnd[4] = {(uint32_t)t, (uint32_t)(t >> 32), p, 0u};
+  philox(rnd, P.key0, P.key1);
+  uint32_t h = 0;
+#pragma unroll
+  for (int r = 0; r < 4; r++)
+    if (__ldg(P.pb + (size_t)r * n + p) > u24(rnd[r])) h |= 1u << r;
+  // a drive probability that is not positive never draws a hit
+  const float pbn = __ldg(P.pb + (size_t)FS_NMDA * n + p);
+  if (((a & FS_ACT_NMDA) && pbn > 0.0f) || (a & FS_ACT_INJ)) {
+    uint32_t r2[4] = {(uint32_t)t, (uint32_t)(t >> 32), p, 1u};
+    philox(r2, P.key0, P.key1);
+    if (pbn > u24(r2[0])) h |= 1u << FS_NMDA;
+    if (a & FS_ACT_INJ) {  // Box-Muller normal
+      const double u1 = ((double)(r2[1] >> 8) + 1.0) * 5.9604644775390625e-08;
+      const double u2 = (double)(r2[2] >> 8) * 5.9604644775390625e-08;
+      const double z = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+      gauss = fma_t<T>((T)__ldg(P.inj_std + p), (T)z, (T)__ldg(P.inj_mean + p));
+    }
+  }
+  return h;
+}
+
+// Draws of L steps for a tile, by all threads at once, off the neurons'
+// per-step dependency chain.
 template <class T>
 __device__ __forceinline__ void draw_inputs(const Params &P, uint32_t p0, uint32_t np, uint64_t tb, uint32_t L,
                                             uint8_t (*hits)[TileW<T>::W], T (*gauss)[TileW<T>::W]) {
-  const uint32_t n = P.n;
   for (uint32_t idx = threadIdx.x; idx < np * L; idx += kThreads) {
-    const uint32_t j = idx / np, q = idx - j * np, p = p0 + q;
-    const uint64_t t = tb + j;
-    const uint32_t a = __ldg(P.act + p);
-    uint32_t rnd[4] = {(uint32_t)t, (uint32_t)(t >> 32), p, 0u};
-    philox(rnd, P.key0, P.key1);
-    uint32_t h = 0;
+    const uint32_t j = idx / np, q = idx - j * np;
+    T gv = (T)0;
+    hits[j][q] = (uint8_t)draw_one<T>(P, p0 + q, tb + j, gv);
+    gauss[j][q] = gv;
+  }
+}
+
+// ---- one neuron's step (shared by every kernel) ----------------------------
+// Parameters and state of one neuron, held in registers while its thread
+// advances it; the per-step arithmetic below is the single definition used
+// by the interval kernel (k_prod / k_prod_batch) and the single-step kernel
+// (k_prod1), so the two give bit-identical neurons.
+template <class T>
+struct NeuronPar {
+  uint32_t a;
+  uint8_t pj;
+  int32_t rf, sd;
+  T vth, vreset, df, ef, dvm, cm, leak, mg;
+  T vrev[5], dfs[5], extg[5];
+  T ndfxt, nefas;
+  T pdf[4];
+  T pdfxt, pdfst, pefas;
+};
+
+template <class T>
+struct NeuronState {
+  T V;
+  int32_t cnt;
+  uint32_t ns;
+  T G[4], est[4], sp[4];
+  T ex, es, xp, spre;
+};
+
+template <class T>
+__device__ __forceinline__ void load_neuron(const Params &P, uint32_t p, NeuronPar<T> &q, NeuronState<T> &st) {
+  const uint32_t n = P.n;
+  q.a = P.act[p];
+  q.pj = P.proj[p];
+  q.rf = __ldg(P.RfPed + p);
+  q.sd = __ldg(P.SpiDy + p);
+  q.vth = (T)__ldg(P.Vth + p);
+  q.vreset = (T)__ldg(P.Vreset + p);
+  q.df = (T)__ldg(P.df + p);
+  q.ef = (T)__ldg(P.ef + p);
+  q.dvm = (T)__ldg(P.dVmax + p);
+  q.cm = (T)__ldg(P.Cm + p);
+  q.leak = (T)__ldg(P.gl + p) * (T)__ldg(P.El + p) * (T)1e3;
+  q.mg = (T)__ldg(P.nmda_mg + p);
 #pragma unroll
-    for (int r = 0; r < 4; r++)
-      if (__ldg(P.pb + (size_t)r * n + p) > u24(rnd[r])) h |= 1u << r;
-    // the second block serves the NMDA drive and the injection noise; a
-    // drive probability that is not positive never draws a hit
-    const float pbn = __ldg(P.pb + (size_t)FS_NMDA * n + p);
-    if (((a & FS_ACT_NMDA) && pbn > 0.0f) || (a & FS_ACT_INJ)) {
-      uint32_t r2[4] = {(uint32_t)t, (uint32_t)(t >> 32), p, 1u};
-      philox(r2, P.key0, P.key1);
-      if (pbn > u24(r2[0])) h |= 1u << FS_NMDA;
-      if (a & FS_ACT_INJ) {  // Box-Muller normal
-        const double u1 = ((double)(r2[1] >> 8) + 1.0) * 5.9604644775390625e-08;
-        const double u2 = (double)(r2[2] >> 8) * 5.9604644775390625e-08;
-        const double z = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
-        gauss[j][q] = (T)__ldg(P.inj_mean + p) + (T)__ldg(P.inj_std + p) * (T)z;
+  for (int r = 0; r < 5; r++) {
+    q.vrev[r] = (T)__ldg(P.Vrev + (size_t)r * n + p);
+    q.dfs[r] = (T)__ldg(P.dfst + (size_t)r * n + p);
+    q.extg[r] = (T)__ldg(P.ext_g + (size_t)r * n + p);
+  }
+  q.ndfxt = (T)__ldg(P.nmda_dfxt + p);
+  q.nefas = (T)__ldg(P.nmda_efst + p) * (T)__ldg(P.nmda_as + p);
+#pragma unroll
+  for (int r = 0; r < 4; r++) q.pdf[r] = (T)__ldg(P.pdf + (size_t)r * n + p);
+  q.pdfxt = (T)__ldg(P.p_dfxt + p);
+  q.pdfst = (T)__ldg(P.p_dfst + p);
+  q.pefas = (T)__ldg(P.p_efas + p);
+  st.V = ((T *)P.V)[p];
+  st.cnt = P.Count[p];
+  st.ns = P.NS[p];
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    st.G[r] = ((T *)P.G)[(size_t)r * n + p];
+    st.est[r] = ((T *)P.ext_st)[(size_t)r * n + p];
+    st.sp[r] = ((T *)P.st_pre)[(size_t)r * n + p];
+  }
+  st.ex = ((T *)P.ext_x)[p];
+  st.es = ((T *)P.ext_s)[p];
+  st.xp = ((T *)P.x_pre)[p];
+  st.spre = ((T *)P.s_pre)[p];
+}
+
+template <class T>
+__device__ __forceinline__ void store_neuron(const Params &P, uint32_t p, const NeuronState<T> &st) {
+  const uint32_t n = P.n;
+  ((T *)P.V)[p] = st.V;
+  P.Count[p] = st.cnt;
+  P.NS[p] = st.ns;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    ((T *)P.G)[(size_t)r * n + p] = st.G[r];
+    ((T *)P.ext_st)[(size_t)r * n + p] = st.est[r];
+    ((T *)P.st_pre)[(size_t)r * n + p] = st.sp[r];
+  }
+  ((T *)P.ext_x)[p] = st.ex;
+  ((T *)P.ext_s)[p] = st.es;
+  ((T *)P.x_pre)[p] = st.xp;
+  ((T *)P.s_pre)[p] = st.spre;
+}
+
+// NMDA presynaptic kinetics of one step (code/EqsGnl2.cpp:493): x jumps by
+// inc on a spike and decays otherwise, s follows with its (1 - s)
+// saturation.  The neuron's owner and every block that tracks a copy of it
+// (k_prod1) call this one function with the same operands.
+template <class T>
+__device__ __forceinline__ void nmda_pre_step(T &xp, T &spre, bool spk, T inc, T pdfxt, T pdfst, T pefas) {
+  xp = spk ? xp + inc : xp * pdfxt;
+  spre = fma_t<T>(pdfst, spre, (pefas * xp) * ((T)1 - spre));
+}
+
+// One step of neuron p: fold the linear conductances' delivered sums
+// (rv: 2^-40 fixed point) into G, add the external drive (hit bits, injection
+// current) and the NMDA sum gnmda, VmEul + firing (code/EqsGnl2.cpp:152-251),
+// per-step outputs of step s, then the presynaptic state: the increment inc of
+// a spike and, per linear receptor, c = inc + st(t-1)(1 - df) for the push.
+// Returns whether the neuron spiked.
+template <class T>
+__device__ __forceinline__ bool neuron_step(const Params &P, const NeuronPar<T> &q, NeuronState<T> &st,
+                                            const long long (&rv)[4], T gnmda, uint32_t hit, T gauss, T gapI,
+                                            uint32_t p, bool own, uint32_t s, T (&cinc)[4], T &inc_out) {
+  const uint32_t n = P.n;
+  T g[5];
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    g[r] = (T)0;
+    if (P.lin_of_rec[r] >= 0) {
+      st.G[r] = fma_t<T>(q.dfs[r], st.G[r], (T)rv[r] * (T)kInvFix);  // exact power-of-two scale
+      g[r] = st.G[r];
+    }
+  }
+  g[FS_NMDA] = gnmda * (T)P.rg[FS_NMDA];
+  // external drive (BgInit): bit r of hit = receptor r's Bernoulli outcome
+  const uint32_t bitsr[4] = {FS_ACT_AMPA, FS_ACT_GABA, FS_ACT_ACH, FS_ACT_GCL};
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    if (q.a & bitsr[r]) {
+      st.est[r] = (hit & (1u << r)) ? st.est[r] + (T)1 : st.est[r] * q.dfs[r];
+      g[r] = fma_t<T>(q.extg[r], st.est[r], g[r]);
+    }
+  }
+  T isyn = (T)0;
+  if (q.a & FS_ACT_NMDA) {
+    st.ex = (hit & (1u << FS_NMDA)) ? st.ex + (T)1 : st.ex * q.ndfxt;
+    st.es = fma_t<T>(q.dfs[FS_NMDA], st.es, (q.nefas * st.ex) * ((T)1 - st.es));
+    g[FS_NMDA] = fma_t<T>(q.extg[FS_NMDA], st.es, g[FS_NMDA]);
+  }
+  if (q.a & FS_ACT_INJ) isyn = gauss;
+  if (P.gap_row) isyn = isyn + gapI;  // steps of networks with gap junctions come one at a time
+  // VmEul + firing (code/EqsGnl2.cpp:152-251)
+  uint32_t ns = st.ns;
+  bool fire_now = false;
+  if (ns & FS_NS_FIRE) {
+    fire_now = true;
+  } else {
+    const T v = st.V;
+    const T Ir0 = g[FS_AMPA] * (q.vrev[FS_AMPA] - v);
+    const T Ir1 = g[FS_GABA] * (q.vrev[FS_GABA] - v);
+    const T Ir2 = g[FS_NMDA] * (q.vrev[FS_NMDA] - v) / ((T)1 + q.mg * exp_t<T>((T)-0.062 * v) / (T)3.57);
+    const T Ir3 = g[FS_ACH] * (q.vrev[FS_ACH] - v);
+    const T Ir4 = g[FS_GCL] * (q.vrev[FS_GCL] - v);
+    T I = fma_t<T>(isyn, (T)1e3, Ir0 + Ir1 + Ir2 + Ir3 + Ir4) + q.leak;
+    I = (T)1e-3 * I / q.cm;
+    if (I > q.dvm) {
+      I = q.dvm;
+      ns = (ns | FS_NS_MEMDV_OVF) & ~FS_NS_MEMDV_UDF;
+    } else if (I < -q.dvm) {
+      I = -q.dvm;
+      ns = (ns & ~FS_NS_MEMDV_OVF) | FS_NS_MEMDV_UDF;
+    } else {
+      ns &= ~(FS_NS_MEMDV_OVF | FS_NS_MEMDV_UDF);
+    }
+    st.V = fma_t<T>(q.df, v, q.ef * I);
+    if (P.outI && own) {  // kept only while requested (code/EqsGnl2.cpp:196-206)
+      P.Irep[p] = (float)Ir0;
+      P.Irep[(size_t)n + p] = (float)Ir1;
+      P.Irep[(size_t)FS_NMDA * n + p] = (float)Ir2;
+      P.Irep[(size_t)FS_ACH * n + p] = (float)Ir3;
+      P.Irep[(size_t)FS_GCL * n + p] = (float)Ir4;
+    }
+    if (st.V > q.vth) {
+      ns |= FS_NS_FIRE;
+      fire_now = true;
+    }
+  }
+  if (fire_now) {
+    if (st.cnt < q.rf) {
+      st.V = (st.cnt == 0) ? (T)0 : q.vreset;
+      if (st.cnt == q.sd) ns |= FS_NS_SPIKE;
+      else ns &= ~FS_NS_SPIKE;
+      st.cnt++;
+    } else {
+      st.cnt = 0;
+      ns &= ~FS_NS_FIRE;
+    }
+  }
+  st.ns = ns;
+  if (own && P.outV) P.outV[(size_t)s * n + p] = (float)st.V;
+  if (own && P.outNS) P.outNS[(size_t)s * n + p] = ns;
+  if (own && P.outI)
+#pragma unroll
+    for (int r = 0; r < 5; r++) P.outI[(size_t)s * 5 * n + (size_t)r * n + p] = P.Irep[(size_t)r * n + p];
+  const bool spk = own && (ns & FS_NS_SPIKE) != 0;
+  // presynaptic state: increment per spike, then plasticity update
+#pragma unroll
+  for (int r = 0; r < 4; r++) cinc[r] = (T)0;
+  T inc = (T)1;
+  if (q.pj && own) {
+    if (P.plast == PL_STD) inc = (T)P.D[p];
+    else if (P.plast == PL_STP) inc = (T)P.D[p] * (T)P.F[p];
+    else if (P.plast == PL_TM && P.tm_on[p]) {
+      T u = (T)P.tm_u[p], x = (T)P.tm_x[p];
+      const T U = (T)P.tm_U[p];
+      if (spk) {
+        u = u + U * ((T)1 - u);
+        const T rel = u * x;
+        inc = rel;
+        x = x - rel;
+      } else {
+        u = U + (u - U) * (T)P.tm_dff[p];
+        x = (T)1 + (x - (T)1) * (T)P.tm_dfr[p];
+      }
+      P.tm_u[p] = (float)u;
+      P.tm_x[p] = (float)x;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      if (q.pj & (1u << r)) {
+        if (spk) {
+          cinc[r] = inc + st.sp[r] * ((T)1 - q.pdf[r]);
+          st.sp[r] = st.sp[r] + inc;
+        } else {
+          st.sp[r] = st.sp[r] * q.pdf[r];
+        }
       }
     }
-    hits[j][q] = (uint8_t)h;
+    if (q.pj & (1u << FS_NMDA)) nmda_pre_step<T>(st.xp, st.spre, spk, inc, q.pdfxt, q.pdfst, q.pefas);
+    if (P.plast == PL_STD) {
+      P.D[p] = spk ? P.D[p] * (1.0f - P.stp_pv[p]) : P.stp_dfD[p] * P.D[p] + P.stp_efD[p];
+    } else if (P.plast == PL_STP) {
+      float Dv = P.D[p], Fv = P.F[p], Cp = P.Cap[p], Cr = P.Car[p];
+      if (spk) {
+        Cr += P.stp_aCar[p];
+        Cp += P.stp_aCap[p];
+        Fv += (Cp + Cr) * (1.0f - Fv) * P.stp_aF[p];
+        Dv *= (1.0f - P.stp_pv[p] * Fv);
+      } else {
+        Cr = P.stp_dfCar[p] * Cr + P.stp_efCar[p];
+        Cp = P.stp_dfCap[p] * Cp;
+        Fv = P.stp_dfF[p] * Fv + P.stp_efF[p] * (Cp + Cr) * (1.0f - Fv) * P.stp_aF[p];
+        Dv = P.stp_dfD[p] * Dv + P.stp_efD[p];
+      }
+      P.D[p] = Dv; P.F[p] = Fv; P.Cap[p] = Cp; P.Car[p] = Cr;
+    }
+  }
+  inc_out = inc;
+  return spk;
+}
+
+// Spike outputs of a warp's step: the per-step bitmap and count, the total.
+__device__ __forceinline__ void spike_outputs(const Params &P, uint32_t m, bool spk, uint32_t p, uint32_t s,
+                                              uint32_t lane) {
+  if (spk && P.bits) atomicOr(P.bits + (size_t)s * P.words + (p >> 5), 1u << (p & 31));
+  if (lane == 0) {
+    if (P.counts) atomicAdd(P.counts + s, (unsigned)__popc(m));
+    atomicAdd(P.spike_total, (unsigned long long)__popc(m));
   }
 }
 
@@ -480,37 +749,9 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
   const uint32_t n = P.n, S = P.slots, mask = P.mask;
   const bool own = tid < np;
   const uint32_t p = own ? p0 + tid : p0;  // non-owners read a valid neuron, write nothing
-  // ---- parameters ----
-  const uint32_t a = P.act[p];
-  const uint8_t pj = P.proj[p];
-  const int32_t rf = __ldg(P.RfPed + p), sd = __ldg(P.SpiDy + p);
-  const T vth = (T)__ldg(P.Vth + p), vreset = (T)__ldg(P.Vreset + p), df = (T)__ldg(P.df + p),
-          ef = (T)__ldg(P.ef + p), dvm = (T)__ldg(P.dVmax + p), cm = (T)__ldg(P.Cm + p),
-          leak = (T)__ldg(P.gl + p) * (T)__ldg(P.El + p) * (T)1e3, mg = (T)__ldg(P.nmda_mg + p);
-  T vrev[5], dfs[5], extg[5];
-#pragma unroll
-  for (int r = 0; r < 5; r++) {
-    vrev[r] = (T)__ldg(P.Vrev + (size_t)r * n + p);
-    dfs[r] = (T)__ldg(P.dfst + (size_t)r * n + p);
-    extg[r] = (T)__ldg(P.ext_g + (size_t)r * n + p);
-  }
-  const T ndfxt = (T)__ldg(P.nmda_dfxt + p), nefas = (T)__ldg(P.nmda_efst + p) * (T)__ldg(P.nmda_as + p);
-  T pdf[4];
-#pragma unroll
-  for (int r = 0; r < 4; r++) pdf[r] = (T)__ldg(P.pdf + (size_t)r * n + p);
-  const T pdfxt = (T)__ldg(P.p_dfxt + p), pdfst = (T)__ldg(P.p_dfst + p), pefas = (T)__ldg(P.p_efas + p);
-  // ---- state ----
-  T V = ((T *)P.V)[p];
-  int32_t cnt = P.Count[p];
-  uint32_t ns = P.NS[p];
-  T G[4], est[4], sp[4];
-#pragma unroll
-  for (int r = 0; r < 4; r++) {
-    G[r] = ((T *)P.G)[(size_t)r * n + p];
-    est[r] = ((T *)P.ext_st)[(size_t)r * n + p];
-    sp[r] = ((T *)P.st_pre)[(size_t)r * n + p];
-  }
-  T ex = ((T *)P.ext_x)[p], es = ((T *)P.ext_s)[p], xp = ((T *)P.x_pre)[p], spre = ((T *)P.s_pre)[p];
+  NeuronPar<T> q;
+  NeuronState<T> st;
+  load_neuron<T>(P, p, q, st);
   uint32_t nsp = 0;
   // ring slots of the first steps: rv for step 0, rv2 for step 1 (PD == 2)
   static_assert(PD == 1 || PD == 2, "ring prefetch distance 1 or 2");
@@ -528,19 +769,14 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
     const uint32_t s = sb + j;
     const uint64_t t = P.t0 + s;
     const uint32_t tm = (uint32_t)t & mask, tprev = (uint32_t)(t - 1u) & mask;
-    bool spk = false;
-    T cinc[4] = {0, 0, 0, 0};
-    // conductances of the previous step's spike phase
-    T g[5];
+    // the slots this step folds in; the ones of step j + PD go in flight
+    long long cur[4];
 #pragma unroll
     for (int r = 0; r < 4; r++) {
-      g[r] = (T)0;
+      cur[r] = rv[r];
       const int ri = P.lin_of_rec[r];
       if (ri >= 0) {
         if (own && rv[r]) __stcg(P.ring + ((size_t)ri * n + p) * S + tprev, 0ull);
-        G[r] = dfs[r] * G[r] + (T)rv[r] * (T)kInvFix;  // exact power-of-two scale
-        g[r] = G[r];
-        // the slot of step j + PD (final since the interval began)
         if constexpr (PD == 2) {
           rv[r] = rv2[r];
           rv2[r] = (own && j + 2 < L) ? (long long)__ldcg(P.ring + ((size_t)ri * n + p) * S + ((tm + 1u) & mask)) : 0ll;
@@ -550,140 +786,17 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
       }
     }
     const uint32_t qs = tid < np ? tid : 0;
-    g[FS_NMDA] = gn[j][qs] * (T)P.rg[FS_NMDA];
-    // external drive (BgInit): the Bernoulli outcomes of this step were drawn
-    // in the pull phase (bit r: receptor r hit)
-    const uint32_t hit = hits[j][qs];
-    const uint32_t bitsr[4] = {FS_ACT_AMPA, FS_ACT_GABA, FS_ACT_ACH, FS_ACT_GCL};
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-      if (a & bitsr[r]) {
-        if (hit & (1u << r)) est[r] = est[r] + (T)1;
-        else est[r] = est[r] * dfs[r];
-        g[r] = g[r] + extg[r] * est[r];
-      }
-    }
-    T isyn = (T)0;
-    if (a & FS_ACT_NMDA) {
-      if (hit & (1u << FS_NMDA)) ex = ex + (T)1;
-      else ex = ex * ndfxt;
-      es = dfs[FS_NMDA] * es + nefas * ex * ((T)1 - es);
-      g[FS_NMDA] = g[FS_NMDA] + extg[FS_NMDA] * es;
-    }
-    if (a & FS_ACT_INJ) isyn = (T)gauss[j][qs];
-    if (P.gap_row) isyn = isyn + gapI[qs];  // batches of one step (interval 1)
-    // VmEul + firing (code/EqsGnl2.cpp:152-251)
-    bool fire_now = false;
-    if (ns & FS_NS_FIRE) {
-      fire_now = true;
-    } else {
-      const T v = V;
-      const T Ir0 = g[FS_AMPA] * (vrev[FS_AMPA] - v);
-      const T Ir1 = g[FS_GABA] * (vrev[FS_GABA] - v);
-      const T Ir2 = g[FS_NMDA] * (vrev[FS_NMDA] - v) / ((T)1 + mg * exp_t<T>((T)-0.062 * v) / (T)3.57);
-      const T Ir3 = g[FS_ACH] * (vrev[FS_ACH] - v);
-      const T Ir4 = g[FS_GCL] * (vrev[FS_GCL] - v);
-      T I = Ir0 + Ir1 + Ir2 + Ir3 + Ir4 + isyn * (T)1e3 + leak;
-      I = (T)1e-3 * I / cm;
-      if (I > dvm) {
-        I = dvm;
-        ns = (ns | FS_NS_MEMDV_OVF) & ~FS_NS_MEMDV_UDF;
-      } else if (I < -dvm) {
-        I = -dvm;
-        ns = (ns & ~FS_NS_MEMDV_OVF) | FS_NS_MEMDV_UDF;
-      } else {
-        ns &= ~(FS_NS_MEMDV_OVF | FS_NS_MEMDV_UDF);
-      }
-      V = df * v + ef * I;
-      if (P.outI && own) {  // kept only while requested (code/EqsGnl2.cpp:196-206)
-        P.Irep[p] = (float)Ir0;
-        P.Irep[(size_t)n + p] = (float)Ir1;
-        P.Irep[(size_t)FS_NMDA * n + p] = (float)Ir2;
-        P.Irep[(size_t)FS_ACH * n + p] = (float)Ir3;
-        P.Irep[(size_t)FS_GCL * n + p] = (float)Ir4;
-      }
-      if (V > vth) {
-        ns |= FS_NS_FIRE;
-        fire_now = true;
-      }
-    }
-    if (fire_now) {
-      if (cnt < rf) {
-        V = (cnt == 0) ? (T)0 : vreset;
-        if (cnt == sd) ns |= FS_NS_SPIKE;
-        else ns &= ~FS_NS_SPIKE;
-        cnt++;
-      } else {
-        cnt = 0;
-        ns &= ~FS_NS_FIRE;
-      }
-    }
-    if (own && P.outV) P.outV[(size_t)s * n + p] = (float)V;
-    if (own && P.outNS) P.outNS[(size_t)s * n + p] = ns;
-    if (own && P.outI)
-#pragma unroll
-      for (int r = 0; r < 5; r++) P.outI[(size_t)s * 5 * n + (size_t)r * n + p] = P.Irep[(size_t)r * n + p];
-    spk = own && (ns & FS_NS_SPIKE) != 0;
+    T cinc[4], inc;
+    const bool spk = neuron_step<T>(P, q, st, cur, gn[j][qs], hits[j][qs], gauss[j][qs],
+                                    P.gap_row ? gapI[qs] : (T)0, p, own, s, cinc, inc);
     nsp += spk ? 1u : 0u;
-    // presynaptic state: increment per spike, then plasticity update
-    if (pj && own) {
-      T inc = (T)1;
-      if (P.plast == PL_STD) inc = (T)P.D[p];
-      else if (P.plast == PL_STP) inc = (T)P.D[p] * (T)P.F[p];
-      else if (P.plast == PL_TM && P.tm_on[p]) {
-        T u = (T)P.tm_u[p], x = (T)P.tm_x[p];
-        const T U = (T)P.tm_U[p];
-        if (spk) {
-          u = u + U * ((T)1 - u);
-          const T rel = u * x;
-          inc = rel;
-          x = x - rel;
-        } else {
-          u = U + (u - U) * (T)P.tm_dff[p];
-          x = (T)1 + (x - (T)1) * (T)P.tm_dfr[p];
-        }
-        P.tm_u[p] = (float)u;
-        P.tm_x[p] = (float)x;
-      }
+    if (own && (q.pj & (1u << FS_NMDA))) {
+      if constexpr (sizeof(T) == 4) {
 #pragma unroll
-      for (int r = 0; r < 4; r++) {
-        if (pj & (1u << r)) {
-          if (spk) {
-            cinc[r] = inc + sp[r] * ((T)1 - pdf[r]);
-            sp[r] = sp[r] + inc;
-          } else {
-            sp[r] = sp[r] * pdf[r];
-          }
-        }
-      }
-      if (pj & (1u << FS_NMDA)) {
-        if (spk) xp = xp + inc;
-        else xp = xp * pdfxt;
-        spre = pdfst * spre + pefas * xp * ((T)1 - spre);
-        if constexpr (sizeof(T) == 4) {
-#pragma unroll
-          for (uint32_t k = 0; k < kSH; k++)
-            __stcg((T *)P.s_hist + ((size_t)p * kSH + k) * S + ((tm - k) & mask), spre);
-        } else {
-          __stcg((T *)P.s_hist + (size_t)p * S + tm, spre);
-        }
-      }
-      if (P.plast == PL_STD) {
-        P.D[p] = spk ? P.D[p] * (1.0f - P.stp_pv[p]) : P.stp_dfD[p] * P.D[p] + P.stp_efD[p];
-      } else if (P.plast == PL_STP) {
-        float Dv = P.D[p], Fv = P.F[p], Cp = P.Cap[p], Cr = P.Car[p];
-        if (spk) {
-          Cr += P.stp_aCar[p];
-          Cp += P.stp_aCap[p];
-          Fv += (Cp + Cr) * (1.0f - Fv) * P.stp_aF[p];
-          Dv *= (1.0f - P.stp_pv[p] * Fv);
-        } else {
-          Cr = P.stp_dfCar[p] * Cr + P.stp_efCar[p];
-          Cp = P.stp_dfCap[p] * Cp;
-          Fv = P.stp_dfF[p] * Fv + P.stp_efF[p] * (Cp + Cr) * (1.0f - Fv) * P.stp_aF[p];
-          Dv = P.stp_dfD[p] * Dv + P.stp_efD[p];
-        }
-        P.D[p] = Dv; P.F[p] = Fv; P.Cap[p] = Cp; P.Car[p] = Cr;
+        for (uint32_t k = 0; k < kSH; k++)
+          __stcg((T *)P.s_hist + ((size_t)p * kSH + k) * S + ((tm - k) & mask), st.spre);
+      } else {
+        __stcg((T *)P.s_hist + (size_t)p * S + tm, st.spre);
       }
     }
     // spikes of this warp: outputs, and the spike list the block pushes at
@@ -692,11 +805,7 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
     // this warp right away
     uint32_t m = __ballot_sync(fsd::kFull, spk);
     if (m) {
-      if (spk && P.bits) atomicOr(P.bits + (size_t)s * P.words + (p >> 5), 1u << (p & 31));
-      if (lane == 0) {
-        if (P.counts) atomicAdd(P.counts + s, (unsigned)__popc(m));
-        atomicAdd(P.spike_total, (unsigned long long)__popc(m));
-      }
+      spike_outputs(P, m, spk, p, s, lane);
       bool listed = false;
       if (spk) {
         const uint32_t k = atomicAdd(lst.n, 1u);
@@ -712,29 +821,17 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
       while (over) {
         const int jl = __ffs(over) - 1;
         over &= over - 1;
-        const uint32_t q = __shfl_sync(fsd::kFull, p, jl);
+        const uint32_t qq = __shfl_sync(fsd::kFull, p, jl);
         T cj[4];
 #pragma unroll
         for (int r = 0; r < 4; r++) cj[r] = __shfl_sync(fsd::kFull, cinc[r], jl);
-        push_spike<T>(P, q, tm, cj, lane, 32);
+        push_spike<T>(P, qq, tm, cj, lane, 32);
       }
     }
   }
   if (own) {
-    ((T *)P.V)[p] = V;
-    if (P.gap_row) ((T *)P.Vg)[(size_t)((P.t0 + sb) & 1u) * n + p] = V;
-    P.Count[p] = cnt;
-    P.NS[p] = ns;
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-      ((T *)P.G)[(size_t)r * n + p] = G[r];
-      ((T *)P.ext_st)[(size_t)r * n + p] = est[r];
-      ((T *)P.st_pre)[(size_t)r * n + p] = sp[r];
-    }
-    ((T *)P.ext_x)[p] = ex;
-    ((T *)P.ext_s)[p] = es;
-    ((T *)P.x_pre)[p] = xp;
-    ((T *)P.s_pre)[p] = spre;
+    store_neuron<T>(P, p, st);
+    if (P.gap_row) ((T *)P.Vg)[(size_t)((P.t0 + sb) & 1u) * n + p] = st.V;
     if (P.nspk && nsp) P.nspk[p] += nsp;
   }
 }
@@ -768,7 +865,7 @@ __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32
       for (uint32_t tp0 = B0; tp0 < B1; tp0 += kT) {
         const uint32_t np = min(kT, B1 - tp0);
         if constexpr (sizeof(T) == 4) {
-          if (L == 1) nmda_pull1_f32(P, tp0, np, P.t0 + bs, (float (*)[kTile])gn, wid, lane);
+          if (P.dmax0) nmda_pull1_f32(P, tp0, np, P.t0 + bs, (float (*)[kTile])gn, wid, lane);
           else nmda_pull_f32<PU>(P, tp0, np, P.t0 + bs, L, (float (*)[kTile])gn, wid, lane);
         }
         else nmda_pull<T>(P, tp0, np, P.t0 + bs, L, gn, wid, lane);
@@ -834,6 +931,271 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) k_prod(const
   prod_blocks<T, PU, 2>(P, P.block_post[blockIdx.x], P.block_post[blockIdx.x + 1], gridDim.x);
 }
 
+// ---- single-step persistent kernel (networks whose delays are all 0) -------
+// Every network in the reference's own format has no synaptic delays, so a
+// spike of step t acts in step t + 1 and every step ends at a grid barrier.
+// k_prod1 keeps everything a block reads from other neurons in its own
+// shared memory, so the only traffic between blocks per step is the list of
+// the step's spikes:
+//  * each block tracks the presynaptic neurons of its posts (one block per
+//    SM, up to 512 posts): for those with NMDA synapses it keeps a copy of
+//    x and s, advanced every step by nmda_pre_step from the spike list (the
+//    same function and operands as the neuron's owner, so every copy equals
+//    the owner's value bit for bit);
+//  * the NMDA in-edges of its posts live in shared memory as (tracked index,
+//    weight), summed per post by one warp (lane-strided, then an xor
+//    butterfly: the order of nmda_pull1_f32);
+//  * a spike's linear synapses are delivered by the blocks of its targets:
+//    each block walks the rows of its tracked neurons that spiked and adds
+//    w*c (2^-40 fixed point, integer atomics: any order gives the same sum)
+//    into per-post accumulators, the same integers the interval kernel's
+//    delay ring sums;
+//  * the owner of a neuron that spikes appends (id, inc, c[4]) to the step's
+//    list; lists alternate by step parity and the last block at a barrier
+//    empties the next step's list.
+// Across launches the pending deliveries travel through the delay ring as
+// in the interval kernel: the last step pushes its spikes into the ring and
+// the first step of the next launch folds its ring slot.  The drive draws
+// of step t + 1 are made while a block waits at the barrier of step t.
+constexpr uint32_t kT1 = 512;   // threads of k_prod1 (= max posts per block)
+constexpr uint32_t kT1F = 512;  // listed spikes looked up per pass
+
+__device__ __forceinline__ int find_sorted(const uint32_t *a, uint32_t n, uint32_t x) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (a[mid] < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return (lo < n && a[lo] == x) ? (int)lo : -1;
+}
+
+// Grid barrier of k_prod1: as grid_sync, and the last block to arrive also
+// zeroes *reset (the spike count of the step after next) before releasing
+// the others; threads of warps 1.. run work() while thread 0 waits.
+template <class F>
+__device__ __forceinline__ bool grid_sync_work(unsigned int *bar, int *err, uint32_t count, uint32_t *reset,
+                                               F &&work, unsigned int limit = 1u << 24) {
+  __syncthreads();
+  if (count <= 1) {
+    if (threadIdx.x == 0) *reset = 0u;
+    else if (threadIdx.x >= 32) work();
+  } else if (threadIdx.x == 0) {
+    unsigned int *gen = bar + 32;
+    const unsigned int g = ld_relaxed_gpu(gen);
+    const unsigned int arrived = atom_add_acq_rel_gpu(bar, 1u);
+    if (arrived == count - 1) {
+      *(volatile uint32_t *)reset = 0u;
+      atomicExch(bar, 0u);
+      red_release_gpu(gen, 1u);
+    } else {
+      unsigned int spins = 0;
+      while (ld_relaxed_gpu(gen) == g) {
+        if (*(volatile int *)err) break;
+        if (++spins > limit) {
+          atomicExch(err, 2);
+          break;
+        }
+      }
+      fence_acquire_gpu();
+    }
+  } else if (threadIdx.x >= 32) {
+    work();
+  }
+  __syncthreads();
+  return *(volatile int *)err == 0;
+}
+
+__global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params P) {
+  extern __shared__ __align__(16) unsigned char sm1[];
+  __shared__ float gn[kT1], d_gauss[kT1], f_c[kT1F][4];
+  __shared__ uint8_t d_hits[kT1];
+  __shared__ uint32_t f_j[kT1F], f_n;
+  const Blk1 me = P.b1[blockIdx.x];
+  const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const uint32_t n = P.n, S = P.slots, mask = P.mask, NT = me.ntrk, np = me.np;
+  // shared-memory layout (16-byte aligned pieces first)
+  long long *acc = (long long *)sm1;                        // [nlin][kT1]
+  float *tx = (float *)(acc + (size_t)max(1u, P.nlin) * kT1);  // [NT] NMDA x copies
+  float *ts = tx + NT;                                      // [NT] NMDA s copies
+  float *tinc = ts + NT;                                    // [NT] increment of a listed spike
+  float *ctab = tinc + NT;                                  // [ncls][3]
+  float *ew = ctab + 3 * P.t1_ncls;                         // [ne]
+  uint32_t *gid = (uint32_t *)(ew + me.ne);                 // [NT]
+  uint32_t *lrow = gid + NT;                                // [NT + 1]
+  uint32_t *erow = lrow + NT + 1;                           // [np + 1]
+  uint16_t *eidx = (uint16_t *)(erow + np + 1);             // [ne]
+  uint8_t *cls = (uint8_t *)(eidx + me.ne);                 // [NT]
+  uint8_t *flag = cls + NT;                                 // [NT] listed this step
+  // ---- tables ----
+  for (uint32_t i = tid; i < max(1u, P.nlin) * kT1; i += kT1) acc[i] = 0ll;
+  for (uint32_t i = tid; i < 3 * P.t1_ncls; i += kT1) ctab[i] = __ldg(P.t1_cls_tab + i);
+  for (uint32_t j = tid; j < NT; j += kT1) {
+    const uint32_t g = __ldg(P.t1_gid + me.trk0 + j);
+    const uint8_t c = __ldg(P.t1_cls + me.trk0 + j);
+    gid[j] = g;
+    cls[j] = c;
+    flag[j] = 0;
+    // the copies start from the owners' values after the last step before
+    // this launch (written back by the previous launch)
+    tx[j] = c != 255 ? __ldcg((const float *)P.x_pre + g) : 0.0f;
+    ts[j] = c != 255 ? __ldcg((const float *)P.s_pre + g) : 0.0f;
+  }
+  for (uint32_t j = tid; j <= NT; j += kT1) lrow[j] = __ldg(P.t1_lrow + me.lrow0 + j);
+  for (uint32_t q = tid; q <= np; q += kT1) erow[q] = __ldg(P.t1_erow + me.erow0 + q);
+  for (uint32_t e = tid; e < me.ne; e += kT1) {
+    ew[e] = __ldg(P.t1_ew + me.e0 + e);
+    eidx[e] = __ldg(P.t1_eidx + me.e0 + e);
+  }
+  // ---- own neuron (thread tid owns post post0 + tid) ----
+  const bool own = tid < np;
+  const bool active = (tid & ~31u) < np;  // warps with posts
+  const uint32_t p = own ? me.post0 + tid : me.post0;
+  NeuronPar<float> q;
+  NeuronState<float> st;
+  if (active) load_neuron<float>(P, p, q, st);
+  uint32_t nsp = 0;
+  if (own) {
+    float gv = 0.0f;
+    d_hits[tid] = (uint8_t)draw_one<float>(P, p, P.t0, gv);
+    d_gauss[tid] = gv;
+  }
+  __syncthreads();
+  for (uint32_t s = 0; s < P.nsteps; s++) {
+    const uint64_t t = P.t0 + s;
+    if (s > 0) {
+      // ---- spikes of step t - 1: deliveries, then the NMDA copies ----
+      const uint32_t par = (uint32_t)(t - 1u) & 1u;
+      const uint32_t cnt = __ldcg(P.t1_cnt + par);
+      const uint4 *lst = P.t1_list + (size_t)par * n * 2;
+      for (uint32_t c0 = 0; c0 < cnt; c0 += kT1F) {
+        if (tid == 0) f_n = 0;
+        __syncthreads();
+        const uint32_t i = c0 + tid;
+        if (tid < kT1F && i < cnt) {
+          const uint4 a = __ldcg(lst + 2 * (size_t)i), b = __ldcg(lst + 2 * (size_t)i + 1);
+          const int j = find_sorted(gid, NT, a.x);
+          if (j >= 0) {
+            flag[j] = 1;
+            tinc[j] = __uint_as_float(a.y);
+            if (lrow[j + 1] > lrow[j]) {
+              const uint32_t k = atomicAdd(&f_n, 1u);
+              f_j[k] = (uint32_t)j;
+              f_c[k][0] = __uint_as_float(a.z);
+              f_c[k][1] = __uint_as_float(a.w);
+              f_c[k][2] = __uint_as_float(b.x);
+              f_c[k][3] = __uint_as_float(b.y);
+            }
+          }
+        }
+        __syncthreads();
+        // one warp per listed spike walks its synapses onto this block
+        for (uint32_t k = wid; k < f_n; k += kT1 / 32) {
+          const uint32_t j = f_j[k];
+          for (uint32_t e = lrow[j] + lane; e < lrow[j + 1]; e += 32) {
+            const uint32_t code = __ldg(P.t1_lin + me.l0 + e);
+            const float w = __ldg(P.t1_linw + me.l0 + e);
+            const uint32_t r = code >> 16, ql = code & 0xffffu;
+            const float cv = f_c[k][r] * P.rg[r];
+            const long long fx = __double2ll_rn((double)(w * cv) * kFix);
+            atomicAdd((unsigned long long *)&acc[(size_t)P.lin_of_rec[r] * kT1 + ql], (unsigned long long)fx);
+          }
+        }
+        __syncthreads();
+      }
+      for (uint32_t j = tid; j < NT; j += kT1) {
+        const uint8_t c = cls[j];
+        if (c != 255) {
+          const bool spk = flag[j] != 0;
+          float xv = tx[j], sv = ts[j];
+          nmda_pre_step<float>(xv, sv, spk, spk ? tinc[j] : 1.0f, ctab[3 * c], ctab[3 * c + 1], ctab[3 * c + 2]);
+          tx[j] = xv;
+          ts[j] = sv;
+        }
+        flag[j] = 0;
+      }
+      __syncthreads();
+    }
+    // ---- NMDA sums of the block's posts (order of nmda_pull1_f32) ----
+    for (uint32_t qq = wid; qq < np; qq += kT1 / 32) {
+      float a = 0.0f;
+      for (uint32_t e = erow[qq] + lane; e < erow[qq + 1]; e += 32) a = __fmaf_rn(ew[e], ts[eidx[e]], a);
+#pragma unroll
+      for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(fsd::kFull, a, o);
+      if (lane == 0) gn[qq] = a;
+    }
+    __syncthreads();
+    // ---- the neurons' step ----
+    if (active) {
+      long long rv[4];
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        rv[r] = 0ll;
+        const int ri = P.lin_of_rec[r];
+        if (ri >= 0 && own) {
+          if (s == 0) {  // deliveries of the step before this launch: the ring
+            long long *slot = (long long *)P.ring + ((size_t)ri * n + p) * S + ((uint32_t)(t - 1u) & mask);
+            rv[r] = __ldcg(slot);
+            if (rv[r]) __stcg(slot, 0ll);
+          } else {
+            rv[r] = acc[(size_t)ri * kT1 + tid];
+            acc[(size_t)ri * kT1 + tid] = 0ll;
+          }
+        }
+      }
+      const uint32_t qs = own ? tid : 0;
+      float cinc[4], inc;
+      const bool spk = neuron_step<float>(P, q, st, rv, gn[qs], d_hits[qs], d_gauss[qs], 0.0f, p, own, s, cinc, inc);
+      nsp += spk ? 1u : 0u;
+      const uint32_t m = __ballot_sync(fsd::kFull, spk);
+      if (m) {
+        spike_outputs(P, m, spk, p, s, lane);
+        const uint32_t par = (uint32_t)t & 1u;
+        const int leader = __ffs(m) - 1;
+        uint32_t base = 0;
+        if ((int)lane == leader) base = atomicAdd(P.t1_cnt + par, (uint32_t)__popc(m));
+        base = __shfl_sync(fsd::kFull, base, leader);
+        if (spk) {
+          uint4 *e = P.t1_list + ((size_t)par * n + base + __popc(m & ((1u << lane) - 1u))) * 2;
+          __stcg(e, make_uint4(p, __float_as_uint(inc), __float_as_uint(cinc[0]), __float_as_uint(cinc[1])));
+          __stcg(e + 1, make_uint4(__float_as_uint(cinc[2]), __float_as_uint(cinc[3]), 0u, 0u));
+        }
+        if (s + 1 == P.nsteps) {
+          // the launch's last step: its spikes go into the delay ring, which
+          // the next launch's first step folds
+          const uint32_t tm = (uint32_t)t & mask;
+          uint32_t rem = m;
+          while (rem) {
+            const int jl = __ffs(rem) - 1;
+            rem &= rem - 1;
+            const uint32_t qq = __shfl_sync(fsd::kFull, p, jl);
+            float cj[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) cj[r] = __shfl_sync(fsd::kFull, cinc[r], jl);
+            push_spike<float>(P, qq, tm, cj, lane, 32);
+          }
+        }
+      }
+    }
+    if (s + 1 < P.nsteps) {
+      // the next step's drive draws are made while the barrier is awaited
+      const uint64_t tn = t + 1;
+      const bool ok = grid_sync_work(P.bar, P.err, gridDim.x, P.t1_cnt + ((uint32_t)(t + 1u) & 1u), [&]() {
+        for (uint32_t qq = tid - 32; qq < np; qq += kT1 - 32) {
+          float gv = 0.0f;
+          d_hits[qq] = (uint8_t)draw_one<float>(P, me.post0 + qq, tn, gv);
+          d_gauss[qq] = gv;
+        }
+      });
+      if (!ok) return;
+    }
+  }
+  if (own) {
+    store_neuron<float>(P, p, st);
+    if (P.nspk && nsp) P.nspk[p] += nsp;
+  }
+}
+
 // ---- batch: many independent networks in one persistent launch -----------
 // Block b works on instance blk[b].inst, posts [b0, b1), and meets only the
 // other blocks of that instance (blk[b].nblk of them) at its barriers, so
@@ -865,6 +1227,8 @@ __global__ void k_batch_advance(Params *Ps, uint32_t count, uint32_t nsteps) {
 // ---- host side -------------------------------------------------------------
 struct Prod {
   bool fp64 = false;
+  bool single = false;     // runs on the single-step kernel k_prod1
+  uint32_t b1_blocks = 0;  // its blocks (one per SM at most)
   bool wide = false;  // some block's posts span several tiles: eight NMDA edges in flight
   uint32_t n = 0, sm = 148;
   Params P{};
@@ -883,7 +1247,10 @@ struct Prod {
   unsigned int *bar = nullptr;
   int *err = nullptr;
   unsigned long long *spike_total = nullptr;
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  // one event pair per launch since the last accounting: finish() adds up
+  // the device time of every launch in order, however many chunks ran
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  size_t ev_used = 0;
   double ms = 0.0;
   uint64_t kl = 0;
   uint64_t key = 0;
@@ -969,31 +1336,52 @@ int launch(Prod *p, uint32_t nsteps, bool want_bits, bool wantV, cudaStream_t st
   P.err = p->err;
   P.spike_total = p->spike_total;
   void *args[] = {&P};
-  cudaEventRecord(p->e0, st);
-  // (the FP64 pull does not take the edges-in-flight parameter)
-  const void *k = p->fp64 ? (const void *)k_prod<double, 4>
-                          : (p->wide ? (const void *)k_prod<float, 8> : (const void *)k_prod<float, 4>);
-  e = cudaLaunchCooperativeKernel(k, p->blocks, kThreads, args, 0, st);
-  cudaEventRecord(p->e1, st);
+  if (p->ev_used == p->ev.size()) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+      if (a) cudaEventDestroy(a);
+      err = "event create";
+      return FS_ERR_CUDA;
+    }
+    p->ev.push_back({a, b});
+  }
+  if (p->single && cudaMemsetAsync(P.t1_cnt, 0, 8, st) != cudaSuccess) {
+    err = "memset";
+    return FS_ERR_CUDA;
+  }
+  const auto &evp = p->ev[p->ev_used];
+  cudaEventRecord(evp.first, st);
+  if (p->single) {
+    e = cudaLaunchCooperativeKernel((const void *)k_prod1, p->b1_blocks, kT1, args, P.t1_smem, st);
+  } else {
+    // (the FP64 pull does not take the edges-in-flight parameter)
+    const void *k = p->fp64 ? (const void *)k_prod<double, 4>
+                            : (p->wide ? (const void *)k_prod<float, 8> : (const void *)k_prod<float, 4>);
+    e = cudaLaunchCooperativeKernel(k, p->blocks, kThreads, args, 0, st);
+  }
+  cudaEventRecord(evp.second, st);
   if (e != cudaSuccess) {
     err = std::string("cooperative launch: ") + cudaGetErrorString(e);
     return FS_ERR_CUDA;
   }
+  p->ev_used++;
   p->t += nsteps;
   if (launches) *launches += 1;
-  p->kl += 1;
   return FS_OK;
 }
 
 int finish(Prod *p, cudaStream_t st, std::string &err) {
-  cudaError_t e = cudaEventSynchronize(p->e1);
+  cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     err = std::string("kernel: ") + cudaGetErrorString(e);
     return FS_ERR_CUDA;
   }
-  float ms = 0;
-  cudaEventElapsedTime(&ms, p->e0, p->e1);
-  p->ms += ms;
+  for (size_t i = 0; i < p->ev_used; i++) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, p->ev[i].first, p->ev[i].second) == cudaSuccess) p->ms += ms;
+    p->kl += 1;
+  }
+  p->ev_used = 0;
   int h = 0;
   e = cudaMemcpy(&h, p->err, 4, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) {
@@ -1009,8 +1397,156 @@ int finish(Prod *p, cudaStream_t st, std::string &err) {
 
 }  // namespace
 
+// ---- plan of the single-step kernel ------------------------------------------
+// Posts are cut into at most one block per SM, in whole warps (32 posts) and
+// at most kT1 posts per block, balanced by a cost of 24 per post plus its
+// NMDA in-edges plus a quarter of its linear in-edges.  Per block: the sorted
+// presynaptic neurons of its posts' synapses, their NMDA kinetics classes,
+// their linear synapses onto the block grouped by neuron, and the NMDA
+// in-edges in CSR order with the presynaptic neuron as a tracked index.
+// Returns false (and the interval kernel runs) when a block's tables do not
+// fit in shared memory or there are more than 255 NMDA kinetics classes.
+struct Single {
+  std::vector<Blk1> blk;
+  std::vector<uint32_t> gid, lrow, lin, erow;
+  std::vector<uint8_t> cls;
+  std::vector<float> linw, ew, tab;
+  std::vector<uint16_t> eidx;
+  uint32_t smem = 0;
+};
+
+static bool plan_single(uint32_t n, uint32_t nlin, uint32_t sm_count, const std::vector<uint32_t> &in_row,
+                        const std::vector<uint32_t> &in_code, const std::vector<float> &in_w,
+                        const std::vector<uint32_t> &out_row, const std::vector<uint32_t> &out_code,
+                        const std::vector<float> &out_w, const std::vector<float> &p_dfxt,
+                        const std::vector<float> &p_dfst, const std::vector<float> &p_efas, const uint8_t *proj,
+                        Single &S1) {
+  const uint32_t units = (n + 31) / 32, per = kT1 / 32;
+  uint32_t B = std::min<uint32_t>(sm_count, units);
+  if (B == 0 || (uint64_t)B * per < units) return false;
+  // linear in-degree per post
+  std::vector<uint32_t> lin_in(n, 0);
+  for (uint32_t e = 0; e < out_code.size(); e++) lin_in[out_code[e] & 0x3fffffu]++;
+  std::vector<double> pre(units + 1, 0.0);
+  for (uint32_t u = 0; u < units; u++) {
+    double c = 0;
+    for (uint32_t q = u * 32; q < std::min(n, u * 32 + 32); q++)
+      c += 24.0 + (double)(in_row[q + 1] - in_row[q]) + 0.25 * lin_in[q];
+    pre[u + 1] = pre[u] + c;
+  }
+  std::vector<uint32_t> cut(B + 1, units);
+  cut[0] = 0;
+  for (uint32_t b = 1; b < B; b++) {
+    const double want = pre[units] * b / B;
+    uint32_t c = (uint32_t)(std::lower_bound(pre.begin(), pre.end(), want) - pre.begin());
+    c = std::max(c, cut[b - 1] + 1);
+    c = std::min(c, cut[b - 1] + per);
+    c = std::max<uint32_t>(c, units > per * (B - b) ? units - per * (B - b) : 0);
+    c = std::min(c, units);
+    cut[b] = c;
+  }
+  for (uint32_t b = 0; b < B; b++)
+    if (cut[b + 1] - cut[b] > per) return false;
+  // NMDA kinetics classes of the presynaptic neurons
+  std::vector<int> cls_of(n, -1);
+  std::vector<std::array<uint32_t, 3>> tabs;
+  for (uint32_t i = 0; i < n; i++) {
+    if (!(proj[i] & (1u << FS_NMDA))) continue;
+    std::array<uint32_t, 3> k;
+    std::memcpy(&k[0], &p_dfxt[i], 4);
+    std::memcpy(&k[1], &p_dfst[i], 4);
+    std::memcpy(&k[2], &p_efas[i], 4);
+    size_t c = 0;
+    while (c < tabs.size() && tabs[c] != k) c++;
+    if (c == tabs.size()) {
+      if (tabs.size() == 255) return false;
+      tabs.push_back(k);
+    }
+    cls_of[i] = (int)c;
+  }
+  S1.tab.clear();
+  for (auto &k : tabs)
+    for (int j = 0; j < 3; j++) {
+      float f;
+      std::memcpy(&f, &k[j], 4);
+      S1.tab.push_back(f);
+    }
+  // linear synapses grouped by the block of their post
+  std::vector<uint32_t> blk_of_unit(units);
+  for (uint32_t b = 0; b < B; b++)
+    for (uint32_t u = cut[b]; u < cut[b + 1]; u++) blk_of_unit[u] = b;
+  std::vector<std::vector<uint64_t>> lin_b(B);  // (pre << 32) | edge index
+  for (uint32_t a = 0; a < n; a++)
+    for (uint32_t e = out_row[a]; e < out_row[a + 1]; e++) {
+      const uint32_t post = out_code[e] & 0x3fffffu;
+      lin_b[blk_of_unit[post >> 5]].push_back(((uint64_t)a << 32) | e);
+    }
+  std::vector<int32_t> loc(n, -1);
+  const size_t fixed = (size_t)std::max(1u, nlin) * kT1 * 8 + S1.tab.size() * 4 + 64;
+  S1.blk.clear();
+  S1.gid.clear(); S1.lrow.clear(); S1.lin.clear(); S1.erow.clear(); S1.cls.clear();
+  S1.linw.clear(); S1.ew.clear(); S1.eidx.clear();
+  size_t smax = 0;
+  for (uint32_t b = 0; b < B; b++) {
+    const uint32_t P0 = cut[b] * 32, P1 = std::min(n, cut[b + 1] * 32);
+    std::vector<uint64_t> &L = lin_b[b];
+    std::sort(L.begin(), L.end());
+    std::vector<uint32_t> trk;
+    for (uint32_t q = P0; q < P1; q++)
+      for (uint32_t e = in_row[q]; e < in_row[q + 1]; e++) trk.push_back(in_code[e] & 0xffffffu);
+    for (uint64_t x : L) trk.push_back((uint32_t)(x >> 32));
+    std::sort(trk.begin(), trk.end());
+    trk.erase(std::unique(trk.begin(), trk.end()), trk.end());
+    if (trk.size() > 65535) return false;
+    Blk1 bk{};
+    bk.post0 = P0;
+    bk.np = P1 - P0;
+    bk.trk0 = (uint32_t)S1.gid.size();
+    bk.ntrk = (uint32_t)trk.size();
+    bk.lrow0 = (uint32_t)S1.lrow.size();
+    bk.e0 = (uint32_t)S1.ew.size();
+    bk.erow0 = (uint32_t)S1.erow.size();
+    bk.l0 = (uint32_t)S1.lin.size();
+    for (uint32_t j = 0; j < trk.size(); j++) {
+      loc[trk[j]] = (int32_t)j;
+      S1.gid.push_back(trk[j]);
+      S1.cls.push_back(255);
+    }
+    // NMDA in-edges in CSR order; the classes of the neurons they come from
+    for (uint32_t q = P0; q <= P1; q++) S1.erow.push_back(in_row[q] - in_row[P0]);
+    for (uint32_t e = in_row[P0]; e < in_row[P1]; e++) {
+      const uint32_t a = in_code[e] & 0xffffffu;
+      S1.eidx.push_back((uint16_t)loc[a]);
+      S1.ew.push_back(in_w[e]);
+      S1.cls[bk.trk0 + loc[a]] = (uint8_t)cls_of[a];
+    }
+    bk.ne = in_row[P1] - in_row[P0];
+    // linear rows per tracked neuron (L is sorted by neuron)
+    size_t k = 0;
+    for (uint32_t j = 0; j < trk.size(); j++) {
+      S1.lrow.push_back((uint32_t)(S1.lin.size() - bk.l0));
+      while (k < L.size() && (uint32_t)(L[k] >> 32) == trk[j]) {
+        const uint32_t e = (uint32_t)L[k];
+        const uint32_t post = out_code[e] & 0x3fffffu, r = (out_code[e] >> 22) & 3u;
+        S1.lin.push_back((post - P0) | (r << 16));
+        S1.linw.push_back(out_w[e]);
+        k++;
+      }
+    }
+    S1.lrow.push_back((uint32_t)(S1.lin.size() - bk.l0));
+    for (uint32_t a : trk) loc[a] = -1;
+    S1.blk.push_back(bk);
+    const size_t need = fixed + (size_t)bk.ntrk * (4 * 3 + 4 + 4 + 2) + 4 + (size_t)bk.ne * 6 + (size_t)(bk.np + 1) * 4;
+    smax = std::max(smax, need);
+  }
+  // dynamic shared memory next to the kernel's ~15 KB of static arrays
+  if (smax > (size_t)200 * 1024) return false;
+  S1.smem = (uint32_t)((smax + 15) & ~(size_t)15);
+  return true;
+}
+
 int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t sm_count, cudaStream_t st,
-                std::string &err) {
+                std::string &err, bool allow_single) {
   *out = nullptr;
   const fs_neurons &v = d->neurons;
   const uint32_t n = v.n;
@@ -1093,6 +1629,7 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
     P.mask = S - 1;
   }
   P.interval = std::max<uint32_t>(1, dmin);
+  P.dmax0 = dmax == 0 ? 1u : 0u;
   if (gap) P.interval = 1;  // a gap current reads every neuron's V of the step before
   for (int r = 0; r < 4; r++) P.lin_of_rec[r] = present[r] ? (int)(p->nlin++) : -1;
   P.nlin = p->nlin;
@@ -1215,6 +1752,42 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
     P.in_row = nullptr;
   }
   UPU(block_post, block_post.data(), block_post.size());
+  // single-step kernel: FP32, every delay 0, no gap junctions
+  if (allow_single && !p->fp64 && dmax == 0 && !gap && S.n > 0 && !(o.flags & FS_RUN_INTERVAL_KERNEL)) {
+    Single S1;
+    if (plan_single(n, p->nlin, sm_count, in_row, in_code, in_w, out_row, out_code, out_w, p_dfxt, p_dfst, p_efas,
+                    proj.data(), S1)) {
+      // the attribute is per kernel, not per handle: always the largest
+      // dynamic size any plan may take
+      int dev = 0, maxsm = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+      cudaFuncAttributes fa{};
+      cudaFuncGetAttributes(&fa, (const void *)k_prod1);
+      const int dyn_max = std::min<int>(200 * 1024, maxsm - (int)fa.sharedSizeBytes);
+      if ((int)S1.smem <= dyn_max &&
+          cudaFuncSetAttribute((const void *)k_prod1, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max) ==
+              cudaSuccess) {
+        if ((rc = dup(p, (Blk1 **)&P.b1, S1.blk.data(), S1.blk.size(), st, err))) goto fail;
+        UPU(t1_gid, S1.gid.data(), S1.gid.size());
+        UPU(t1_lrow, S1.lrow.data(), S1.lrow.size());
+        UPU(t1_lin, S1.lin.data(), S1.lin.size());
+        UPU(t1_erow, S1.erow.data(), S1.erow.size());
+        if ((rc = dup(p, (uint8_t **)&P.t1_cls, S1.cls.data(), S1.cls.size(), st, err))) goto fail;
+        UPF(t1_linw, S1.linw.data(), S1.linw.size());
+        UPF(t1_ew, S1.ew.data(), S1.ew.size());
+        UPF(t1_cls_tab, S1.tab.data(), S1.tab.size());
+        if ((rc = dup(p, (uint16_t **)&P.t1_eidx, S1.eidx.data(), S1.eidx.size(), st, err))) goto fail;
+        if ((rc = dup(p, &P.t1_cnt, (const uint32_t *)nullptr, 2, st, err))) goto fail;
+        if ((rc = dup(p, &P.t1_list, (const uint4 *)nullptr, (size_t)4 * n, st, err))) goto fail;
+        P.t1_ncls = (uint32_t)(S1.tab.size() / 3);
+        P.t1_smem = S1.smem;
+        p->single = true;
+        p->b1_blocks = (uint32_t)S1.blk.size();
+      }
+      cudaGetLastError();
+    }
+  }
   if (gap) {
     const uint32_t ng = d->compat->gap_rowptr[n];
     UPU(gap_row, d->compat->gap_rowptr, (size_t)n + 1);
@@ -1230,11 +1803,6 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
       (rc = dup(p, &p->spike_total, (const unsigned long long *)nullptr, 1, st, err)))
     goto fail;
   if (cudaMemsetAsync(p->err, 0, 4, st) != cudaSuccess) { rc = FS_ERR_CUDA; err = "memset"; goto fail; }
-  if (cudaEventCreate(&p->e0) != cudaSuccess || cudaEventCreate(&p->e1) != cudaSuccess) {
-    rc = FS_ERR_CUDA;
-    err = "event create";
-    goto fail;
-  }
   if (cudaStreamSynchronize(st) != cudaSuccess) { rc = FS_ERR_CUDA; err = "upload sync"; goto fail; }
 #undef UPF
 #undef UPI
@@ -1249,8 +1817,10 @@ fail:
 void prod_destroy(Prod *p) {
   if (!p) return;
   for (void *q : p->allocs) cudaFree(q);
-  if (p->e0) cudaEventDestroy(p->e0);
-  if (p->e1) cudaEventDestroy(p->e1);
+  for (auto &x : p->ev) {
+    cudaEventDestroy(x.first);
+    cudaEventDestroy(x.second);
+  }
   delete p;
 }
 
@@ -1309,6 +1879,7 @@ int prod_reset(Prod *p, uint32_t seed, cudaStream_t st, std::string &err) {
   p->t = 0;
   p->ms = 0.0;
   p->kl = 0;
+  p->ev_used = 0;
   return FS_OK;
 }
 
@@ -1419,8 +1990,9 @@ void prod_info(const Prod *p, ProdInfo *info) {
   info->d_max = p->d_max;
   info->slots = p->P.slots;
   info->interval = p->P.interval;
-  info->blocks = p->blocks;
-  info->threads = kThreads;
+  info->blocks = p->single ? p->b1_blocks : p->blocks;
+  info->threads = p->single ? kT1 : kThreads;
+  info->single_step = p->single ? 1 : 0;
   info->chunks = p->chunks;
   info->lin_edges = p->lin_edges;
   info->nmda_edges = p->nmda_edges;
@@ -1680,7 +2252,7 @@ int batch_create(Batch **out, uint32_t count, const fs_net_desc *const *descs, c
       rc = FS_ERR_ARG;
       break;
     }
-    rc = prod_create(&p, descs[i], o, sm_count, st, err);
+    rc = prod_create(&p, descs[i], o, sm_count, st, err, false);
     if (rc) err = "instance " + std::to_string(i) + ": " + err;
     else B->inst.push_back(p);
   }
@@ -1858,6 +2430,102 @@ int prod_barrier_probe(unsigned int limit, int *err_word, std::string &err) {
   return FS_OK;
 }
 
+// ---- checks of the drive draws --------------------------------------------
+// The device Philox on k arbitrary (counter, key) pairs, and the drive draws
+// of a step and neuron range through draw_inputs itself (the function the
+// engine's kernels call), so the CPU restatement can be compared with both.
+__global__ void k_debug_philox(const uint32_t *ctr, const uint32_t *key, uint64_t k, uint32_t *out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= k) return;
+  uint32_t c[4] = {ctr[4 * i], ctr[4 * i + 1], ctr[4 * i + 2], ctr[4 * i + 3]};
+  philox(c, key[2 * i], key[2 * i + 1]);
+  for (int w = 0; w < 4; w++) out[4 * i + w] = c[w];
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_debug_drive(const __grid_constant__ Params P, uint32_t first,
+                                                          uint32_t count, uint64_t t0, uint32_t nsteps,
+                                                          uint8_t *hits_out, double *gauss_out) {
+  constexpr uint32_t kT = TileW<T>::W;
+  __shared__ T gauss[kLB][kT];
+  __shared__ uint8_t hits[kLB][kT];
+  const uint32_t q0 = blockIdx.x * kT;
+  if (q0 >= count) return;
+  const uint32_t np = min(kT, count - q0), p0 = first + q0;
+  for (uint32_t j0 = 0; j0 < nsteps; j0 += kLB) {
+    const uint32_t L = min(kLB, nsteps - j0);
+    draw_inputs<T>(P, p0, np, t0 + j0, L, hits, gauss);
+    __syncthreads();
+    for (uint32_t idx = threadIdx.x; idx < np * L; idx += kThreads) {
+      const uint32_t j = idx / np, q = idx - j * np;
+      const size_t o = (size_t)(j0 + j) * count + q0 + q;
+      hits_out[o] = hits[j][q];
+      gauss_out[o] = (__ldg(P.act + p0 + q) & FS_ACT_INJ) ? (double)gauss[j][q] : 0.0;
+    }
+    __syncthreads();
+  }
+}
+
+int prod_debug_philox(const uint32_t *ctr, const uint32_t *key, uint64_t k, uint32_t *out, std::string &err) {
+  uint32_t *dc = nullptr, *dk = nullptr, *dout = nullptr;
+  cudaError_t e = cudaMalloc(&dc, k * 16);
+  if (e == cudaSuccess) e = cudaMalloc(&dk, k * 8);
+  if (e == cudaSuccess) e = cudaMalloc(&dout, k * 16);
+  if (e == cudaSuccess) e = cudaMemcpy(dc, ctr, k * 16, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dk, key, k * 8, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_debug_philox<<<(unsigned)((k + 255) / 256), 256>>>(dc, dk, k, dout);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, dout, k * 16, cudaMemcpyDeviceToHost);
+  if (dc) cudaFree(dc);
+  if (dk) cudaFree(dk);
+  if (dout) cudaFree(dout);
+  if (e != cudaSuccess) {
+    err = std::string("philox check: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  return FS_OK;
+}
+
+int prod_debug_drive(Prod *p, uint64_t t0, uint32_t nsteps, uint32_t first, uint32_t count, uint8_t *hits,
+                     double *gauss, cudaStream_t st, std::string &err) {
+  const size_t m = (size_t)nsteps * count;
+  uint8_t *dh = nullptr;
+  double *dg = nullptr;
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaMalloc(&dh, m);
+  if (e == cudaSuccess) e = cudaMalloc(&dg, m * 8);
+  if (e == cudaSuccess) {
+    const uint32_t W = p->fp64 ? TileW<double>::W : TileW<float>::W;
+    const unsigned blocks = (count + W - 1) / W;
+    if (p->fp64) k_debug_drive<double><<<blocks, kThreads, 0, st>>>(p->P, first, count, t0, nsteps, dh, dg);
+    else k_debug_drive<float><<<blocks, kThreads, 0, st>>>(p->P, first, count, t0, nsteps, dh, dg);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hits, dh, m, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(gauss, dg, m * 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (dh) cudaFree(dh);
+  if (dg) cudaFree(dg);
+  if (e != cudaSuccess) {
+    err = std::string("drive check: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  return FS_OK;
+}
+
+int prod_inject_wait_failure(Prod *p, cudaStream_t st, std::string &err) {
+  const int word = 2;  // the value a barrier wait that gave up stores
+  cudaError_t e = cudaMemcpyAsync(p->err, &word, 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("error word: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  return FS_OK;
+}
+
 // ---- checkpoints --------------------------------------------------------
 // The state a production engine carries from one step to the next, in the
 // order it is saved: neuron and receptor state, presynaptic gates and NMDA
@@ -1953,6 +2621,7 @@ int prod_state_load(Prod *p, const uint8_t *buf, cudaStream_t st, std::string &e
   std::memcpy(p->P.rg, h.rg, sizeof h.rg);
   p->ms = 0.0;
   p->kl = 0;
+  p->ev_used = 0;
   return FS_OK;
 }
 

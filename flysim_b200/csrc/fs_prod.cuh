@@ -9,8 +9,10 @@ namespace fsp {
 
 struct Prod;
 
+// allow_single: a network that qualifies may run on the single-step kernel
+// (batch instances never do: the batch kernel advances them)
 int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t sm_count,
-                cudaStream_t st, std::string &err);
+                cudaStream_t st, std::string &err, bool allow_single = true);
 void prod_destroy(Prod *p);
 int prod_upload_params(Prod *p, const float *pb, const uint32_t *act, const float *inj_mean,
                        const float *inj_std, cudaStream_t st, std::string &err);
@@ -28,11 +30,21 @@ struct ProdInfo {
   uint64_t lin_edges, nmda_edges;
   uint32_t lin_receptors;
   int fp64;
+  int single_step;  // the network runs on the single-step kernel
 };
 void prod_info(const Prod *p, ProdInfo *info);
 int prod_spike_counts(Prod *p, uint32_t *counts, cudaStream_t st, std::string &err);
 // Runs the bounded barrier wait to its limit (see k_barrier_probe).
 int prod_barrier_probe(unsigned int limit, int *err_word, std::string &err);
+// Checks of the drive draws: the device Philox on k (counter[4], key[2])
+// pairs, and the draws of steps [t0, t0 + nsteps) for neurons [first,
+// first + count) with the handle's key and parameters (hits [nsteps][count]
+// bit r = receptor r hit, gauss the injection current, 0 where it is off).
+int prod_debug_philox(const uint32_t *ctr, const uint32_t *key, uint64_t k, uint32_t *out, std::string &err);
+int prod_debug_drive(Prod *p, uint64_t t0, uint32_t nsteps, uint32_t first, uint32_t count, uint8_t *hits,
+                     double *gauss, cudaStream_t st, std::string &err);
+// Stores into the device error word what a bounded wait that gave up stores.
+int prod_inject_wait_failure(Prod *p, cudaStream_t st, std::string &err);
 // Checkpoint blob of the engine's step-to-step state (step counter, drive
 // stream key, gains, every state array and the delay ring).
 uint64_t prod_state_bytes(Prod *p);

@@ -26,7 +26,7 @@ namespace fsh {
 namespace {
 
 constexpr char kMagic[8] = {'F', 'S', 'B', '2', 'N', 'E', 'T', '\0'};
-constexpr uint32_t kFormat = 2;
+constexpr uint32_t kFormat = 3;  // 3: unseeded models are never stored
 constexpr uint32_t kSizes = (uint32_t)(sizeof(Receptor) | sizeof(Link) << 8 | sizeof(Event) << 16);
 
 // 64-bit streaming hash for cache keys and the payload check (not a

@@ -81,7 +81,14 @@ int fs_model_load_cached(const char *conf_path, const char *pro_path, const fs_m
   }
   // keep views valid for the model's life; options strings are not kept
   mm.opts.out_mem = mm.opts.out_spike = mm.opts.out_rate = nullptr;
-  if (use_cache) {
+  // A network seeded by std::random_device (no -udfsed, no RandomSeeds
+  // macro) gets a fresh seed, and with it fresh connectivity and drive, on
+  // every run of the reference (code/NetSimGnl2_BulPp.cpp:80-88); a cached
+  // copy would replay one draw forever, so such a model is never stored.
+  const bool random_seed = !(mm.act_ctr & FS_ACT_STD) && mm.macro_seeds.empty();
+  if (use_cache && random_seed) {
+    if (cache_status) *cache_status = FS_CACHE_UNSEEDED;
+  } else if (use_cache) {
     std::string err;
     bool stored = fsh::cache_write(cache_path, key, mm, err);
     if (!stored) g_model_err = err;

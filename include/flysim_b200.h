@@ -176,7 +176,13 @@ typedef struct fs_run_opts {
   uint64_t philox_key; /* production modes: drive stream key              */
   uint32_t blocks_per_sm; /* production modes: resident blocks per SM of the
                              persistent kernel (0 = as many as fit, <= 4)  */
+  uint32_t flags;      /* FS_RUN_* bits (0 = defaults)                     */
 } fs_run_opts;
+
+/* fs_run_opts.flags: run an FS_MODE_FP32 network whose delays are all 0 on
+ * the interval kernel rather than the single-step kernel (for checks and
+ * A/B timing; results are identical). */
+#define FS_RUN_INTERVAL_KERNEL 1u
 
 /* Per-call step outputs (host memory, caller owned; NULL = not wanted). */
 typedef struct fs_step_out {
@@ -218,7 +224,10 @@ int fs_set_drive(fs_handle *h, uint32_t first, uint32_t count, int rec, float pb
 int fs_set_act(fs_handle *h, uint32_t first, uint32_t count, uint32_t clear_mask, uint32_t set_mask);
 int fs_set_injection(fs_handle *h, uint32_t first, uint32_t count, float mean, float std);
 /* Runs nsteps steps of Activation+Spike (code/NetSimGnl2.cpp:231-264 minus
- * events and output) and returns what the output writers need. */
+ * events and output) and returns what the output writers need.  The steps
+ * run in chunks; FS_ERR_CAPACITY (spike_idx too small) is found after the
+ * chunk that overflowed has run, so the handle has then advanced past what
+ * was returned: reset it (fs_reset) or restore a checkpoint before going on. */
 int fs_step(fs_handle *h, uint32_t nsteps, fs_step_out *out);
 /* Device-resident variant for timing: runs nsteps with no host copies; the
  * per-step spike counts stay on the device. */
@@ -226,11 +235,19 @@ int fs_run(fs_handle *h, uint32_t nsteps);
 /* fs_run bracketed by CUDA events on the engine stream; returns the device
  * time of the whole call (ms) after synchronising. */
 int fs_run_timed(fs_handle *h, uint32_t nsteps, double *device_ms);
+/* Launch layout of a production-mode handle: thread blocks and threads per
+ * block of its persistent kernel, the steps between grid barriers, and
+ * whether it runs on the single-step kernel (FS_MODE_FP32 networks whose
+ * delays are all 0 and that have no gap junctions, unless
+ * FS_RUN_INTERVAL_KERNEL was given).  No counterpart in the reference. */
+int fs_engine_layout(fs_handle *h, uint32_t *blocks, uint32_t *threads, uint32_t *interval, int *single_step);
 /* Synchronise and report counters. */
 int fs_sync(fs_handle *h);
 int fs_stats(fs_handle *h, uint64_t *steps_done, uint64_t *spikes_total, uint64_t *kernel_launches);
-/* Average device duration (ms) of the dominant kernel of the last fs_run /
- * fs_step call, measured with CUDA events on the engine stream. */
+/* Average device duration (ms) of the dominant kernel over the launches
+ * since the last fs_reset that a synchronising call (fs_sync, fs_run_timed,
+ * fs_step) has accounted, measured with CUDA events on the engine stream
+ * (one event pair per launch); launches = how many. */
 int fs_kernel_time(fs_handle *h, double *ms_per_launch, uint64_t *launches);
 /* Evaluates the device's glibc-exact float exp (the NMDA Mg-block exp of
  * FS_MODE_COMPAT) on k host values, for checks against the host libm. */
@@ -259,6 +276,27 @@ int fs_debug_expf_noalloc(const float *x, float *y, uint64_t k);
  * step threads meet at condition-variable waits with no time limit
  * (code/NetSimGnl2.cpp:198-224) and are joined at the end (:348). */
 int fs_debug_barrier_timeout(uint32_t poll_limit);
+/* Checks of the production modes' external drive against a CPU restatement;
+ * no counterpart in the reference, whose drive is one sequential
+ * std::mt19937 stream (code/EqsGnl2.cpp:284-337) and ziggurat normal
+ * (code/StiExt.h:214-218).
+ * fs_debug_philox: the device Philox-4x32-10 on k blocks, ctr [k][4] and
+ * key [k][2] in, out [k][4].
+ * fs_debug_drive: the drive draws of steps [t0, t0 + nsteps) (t counted from
+ * the last fs_reset) of neurons [first, first + count) with the handle's
+ * stream key and current drive and injection parameters, computed by the
+ * function the engine's kernels call: hits [nsteps][count], bit r set when
+ * receptor r (FS_AMPA .. FS_NMDA) is hit; gauss [nsteps][count], the
+ * injection current (nA, 0 where injection is off).  Production modes. */
+int fs_debug_philox(const uint32_t *ctr, const uint32_t *key, uint64_t k, uint32_t *out);
+int fs_debug_drive(fs_handle *h, uint64_t t0, uint32_t nsteps, uint32_t first, uint32_t count, uint8_t *hits,
+                   double *gauss);
+/* Failure detection on the host side: stores into the handle's device error
+ * word what a bounded device wait that gave up stores, without running or
+ * stopping any kernel, so that the paths which must notice it (fs_sync,
+ * fs_checkpoint_save) can be checked.  Production modes; the handle's next
+ * fs_reset or fs_checkpoint_load clears it. */
+int fs_debug_inject_wait_failure(fs_handle *h);
 /* Checkpoints of a production-mode handle (FS_MODE_FP32 / FS_MODE_FP64).
  * The reference parses a SaveAllStates output and Resume event subtypes
  * (code/parser.cpp:1167-1176, :1254-1258) but implements neither; here a
@@ -271,7 +309,9 @@ int fs_debug_barrier_timeout(uint32_t poll_limit);
  * exactly as the saved handle would (bit for bit: the drive draws are a
  * function of the step counter and key).  fs_checkpoint_size gives the
  * buffer size; loading a checkpoint of another network or mode returns
- * FS_ERR_ARG; the compat mode returns FS_ERR_UNSUPPORTED. */
+ * FS_ERR_ARG; the compat mode returns FS_ERR_UNSUPPORTED.  fs_checkpoint_save
+ * first waits for the work in flight and returns FS_ERR_TIMEOUT, saving
+ * nothing, when a device wait of that work gave up. */
 int fs_checkpoint_size(fs_handle *h, uint64_t *bytes);
 int fs_checkpoint_save(fs_handle *h, void *buf, uint64_t cap, uint64_t *bytes);
 int fs_checkpoint_load(fs_handle *h, const void *buf, uint64_t bytes);
@@ -302,7 +342,11 @@ int fs_model_load(const char *conf_path, const char *pro_path, const fs_model_op
  * (re)written.  A cache that cannot be written does not fail the load.
  * cache_status (may be NULL) receives one of FS_CACHE_*.  cache_path NULL or
  * "" behaves as fs_model_load. */
-enum { FS_CACHE_OFF = 0, FS_CACHE_HIT = 1, FS_CACHE_STORED = 2, FS_CACHE_UNWRITABLE = 3 };
+enum { FS_CACHE_OFF = 0, FS_CACHE_HIT = 1, FS_CACHE_STORED = 2, FS_CACHE_UNWRITABLE = 3, FS_CACHE_UNSEEDED = 4 };
+/* FS_CACHE_UNSEEDED: the network has no fixed seed (neither -udfsed nor a
+ * RandomSeeds macro), so, as in the reference, every load draws a new seed
+ * from std::random_device and builds new connectivity from it; such a model
+ * is loaded from the text files and never cached. */
 int fs_model_load_cached(const char *conf_path, const char *pro_path, const fs_model_opts *opts,
                          const char *cache_path, fs_model **out, int *cache_status);
 int fs_model_free(fs_model *m);

@@ -11,6 +11,14 @@ reference's output files; the two log files it writes on every run
     python tests/golden/make_golden.py              # all cases from scratch
     python tests/golden/make_golden.py --logs-only  # logs.json of the committed cases
     python tests/golden/make_golden.py --case NAME  # one case (or several names)
+
+Cases at the benchmark configurations keep digests instead of files:
+config1_1s (the two-population E=800 / I=200 network of the plain method
+for its full 1 s) records the size and SHA-256 of every output file in
+digests.json; connectome20k_d0 (the 20,000-neuron connectome-shaped network
+with delays 0, 100 ms, reference run with -t 1) does the same and does not
+keep its 354 MB net.conf either: gen.json names the seeded generator call
+that rewrites it and the SHA-256 the rewritten file must have.
 """
 from __future__ import annotations
 
@@ -156,6 +164,11 @@ def cases():
         events=[{"t": 300, "type": "ChangeExtFreq", "pop": "Exc1", "f": 24000},
                 {"t": 650, "type": "ChangeMembraneNoise", "pop": "Exc1", "mean": 0.43, "std": 0.03}]), flags=[])
     c["keywords"] = dict(raw=_keywords_case, flags=["-LTP"])
+    # the benchmark configurations themselves (digests only)
+    c["config1_1s"] = dict(conf=lambda p: netgen.write_two_pop(p), pro=dict(t_end_ms=1000, seeds=(7,), outputs=OUTS),
+                           flags=[], digests=True)
+    c["connectome20k_d0"] = dict(gen=dict(n=20000, regions=58, seed=1), pro=dict(
+        t_end_ms=100, seeds=(1,), outputs=OUTS[:2]), flags=["-t", "1"], digests=True)
     # command-line options: user seed (which also switches STD on, as the
     # reference's flag parser does), a non-default time step, and the
     # -om / -os / -or outputs added on top of the .pro's
@@ -166,6 +179,35 @@ def cases():
 
 
 LOGS = ("ConfsInfo.log", "network.log")
+
+
+def write_generated_conf(gen: dict, path: str) -> None:
+    """The .conf of a generated case: connectome-shaped network, delays 0."""
+    c = netgen.connectome(n=gen["n"], regions=gen["regions"], seed=gen["seed"])
+    netgen.write_connectome(c, path, with_delays=False)
+
+
+def file_record(path: str) -> dict:
+    h = hashlib.sha256()
+    size = lines = 0
+    with open(path, "rb") as f:
+        for block in iter(lambda: f.read(1 << 22), b""):
+            h.update(block)
+            size += len(block)
+            lines += block.count(b"\n")
+    return {"bytes": size, "lines": lines, "sha256": h.hexdigest()}
+
+
+def record_digests(d, keep=("net.conf", "net.pro", "cmd.json", "logs.json", "gen.json")):
+    """Replaces the output files in d by their sizes and SHA-256 (digests.json)."""
+    rec = {}
+    for f in sorted(os.listdir(d)):
+        if f in keep or f == "digests.json":
+            continue
+        rec[f] = file_record(os.path.join(d, f))
+        os.remove(os.path.join(d, f))
+    with open(os.path.join(d, "digests.json"), "w") as f:
+        json.dump(rec, f, indent=1, sort_keys=True)
 
 
 def record_logs(d):
@@ -232,6 +274,11 @@ def main():
         os.makedirs(d)
         if "raw" in cs:
             cs["raw"](d)
+        elif "gen" in cs:
+            write_generated_conf(cs["gen"], os.path.join(d, "net.conf"))
+            netgen.write_pro(os.path.join(d, "net.pro"), **cs["pro"])
+            with open(os.path.join(d, "gen.json"), "w") as f:
+                json.dump(dict(cs["gen"], conf=file_record(os.path.join(d, "net.conf"))), f, indent=1, sort_keys=True)
         else:
             cs["conf"](os.path.join(d, "net.conf"))
             netgen.write_pro(os.path.join(d, "net.pro"), **cs["pro"])
@@ -242,7 +289,12 @@ def main():
         if r.returncode != 0:
             sys.exit("reference failed on %s: %s" % (name, r.stderr[-400:]))
         record_logs(d)
-        record_threaded_log(d, cs["flags"])
+        if "gen" not in cs:  # a second parse of a generated network is minutes of reference time
+            record_threaded_log(d, cs["flags"])
+        if cs.get("digests"):
+            record_digests(d)
+        if "gen" in cs:
+            os.remove(os.path.join(d, "net.conf"))
         outs = sorted(f for f in os.listdir(d) if f not in ("net.conf", "net.pro", "cmd.json", "logs.json"))
         print(name, outs)
 

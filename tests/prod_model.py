@@ -15,8 +15,16 @@ Synapses as the production engine defines them:
   in float32 between steps): on a spike u <- u + U(1-u), inc = u*x,
   x <- x - inc; otherwise u relaxes to U with tau_fac and x to 1 with tau_rec.
 
-Only networks without external drive and with noiseless injection are
-covered (every input is then deterministic).
+External drive and injection noise are random; they enter as inputs: the
+`drive` argument gives, per step and neuron, the hit bitmap (bit r:
+receptor r's external synapse hit) and the injection current, as the
+engine's Philox draws produce them (fs_debug_drive, itself checked bit for
+bit against the CPU restatement oracle/fs_philox.c).  The external gates
+follow BgInit (code/EqsGnl2.cpp:284-337): a linear receptor's gate st <- st+1
+on a hit, st*dfst otherwise, adding ext_g*st to its conductance; the NMDA
+drive x <- x+1 on a hit, x*dfxt otherwise, s <- dfst*s + efst*as*x*(1-s),
+adding ext_g*s.  Without `drive`, networks with drive or injection noise are
+refused.
 """
 from __future__ import annotations
 
@@ -28,15 +36,24 @@ NS_FIRE, NS_SPIKE = 1, 2
 NS_OVF, NS_UDF = 16, 32
 
 
-def simulate(na, steps: int, extra: bool = False):
+ACT_EXT = (1, 2, 32, 64)  # AMPA, GABA, ACh, GluCl drive bits of ActCtr
+
+
+def simulate(na, steps: int, extra: bool = False, drive=None):
     """Returns (spikes: list of index arrays per step, V: [steps, n] float64)
     and, with `extra`, also the receptor currents Irep [steps, 5, n] (kept
     from the last integrated step while a neuron fires,
-    code/EqsGnl2.cpp:196-206) and the LIF state word [steps, n]."""
+    code/EqsGnl2.cpp:196-206) and the LIF state word [steps, n].  drive =
+    (hits uint8 [steps, n], injection current [steps, n]) of steps 0 ..
+    steps-1 after a reset."""
     f, s = na.fields, na.syn
     n = na.n
-    assert not np.any(f["pb"]), "external drive is random: not covered"
-    assert not np.any(f["inj_std"]), "injection noise is random: not covered"
+    if drive is None:
+        assert not np.any(f["pb"]), "external drive is random: pass its draws"
+        assert not np.any(f["inj_std"]), "injection noise is random: pass its draws"
+    else:
+        hits_in, gauss_in = drive
+        assert hits_in.shape[0] >= steps and hits_in.shape[1] == n
     get = lambda k: np.asarray(f[k], np.float64)  # noqa: E731
     vrev = get("Vrev").reshape(5, n)
     dfs = get("dfst").reshape(5, n)
@@ -47,6 +64,11 @@ def simulate(na, steps: int, extra: bool = False):
     sd = np.asarray(f["SpiDy"], np.int64)
     act = np.asarray(f["act"], np.int64)
     inj = np.where(act & ACT_INJ, get("inj_mean"), 0.0)
+    extg = get("ext_g").reshape(5, n)
+    ndfxt = get("nmda_dfxt")
+    nefas = get("nmda_efst") * get("nmda_as")
+    est = np.zeros((4, n))
+    ex, es = np.zeros(n), np.zeros(n)
     pre = np.asarray(s["pre"], np.int64)
     post = np.asarray(s["post"], np.int64)
     rec = np.asarray(s["rec"], np.int64)
@@ -96,11 +118,23 @@ def simulate(na, steps: int, extra: bool = False):
         idx = t - 1 - dl[nm]
         sh = np.where(idx >= 0, s_hist[np.maximum(idx, 0), pre[nm]], 0.0)
         g[NMDA] = np.bincount(post[nm], w[nm] * sh, n)
+        isyn = inj
+        if drive is not None:
+            h = hits_in[t].astype(np.int64)
+            for r in range(4):
+                on = (act & ACT_EXT[r]) != 0
+                est[r] = np.where(on, np.where(h & (1 << r), est[r] + 1.0, est[r] * dfs[r]), est[r])
+                g[r] = np.where(on, g[r] + extg[r] * est[r], g[r])
+            on = (act & ACT_NMDA) != 0
+            ex = np.where(on, np.where(h & (1 << NMDA), ex + 1.0, ex * ndfxt), ex)
+            es = np.where(on, dfs[NMDA] * es + nefas * ex * (1.0 - es), es)
+            g[NMDA] = np.where(on, g[NMDA] + extg[NMDA] * es, g[NMDA])
+            isyn = np.where(act & ACT_INJ, gauss_in[t], 0.0)
         fire_now = (ns & NS_FIRE) != 0
         v = V.copy()
         Ir = g * (vrev - v)
         Ir[NMDA] = g[NMDA] * (vrev[NMDA] - v) / (1.0 + mg * np.exp(-0.062 * v) / 3.57)
-        I = Ir.sum(0) + inj * 1e3 + leak
+        I = Ir.sum(0) + isyn * 1e3 + leak
         I = 1e-3 * I / cm
         ovf, udf = I > dvm, I < -dvm
         ns = np.where(fire_now, ns, np.where(ovf, (ns | NS_OVF) & ~NS_UDF,

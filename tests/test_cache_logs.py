@@ -10,13 +10,17 @@
   as the reference, byte for byte, and its counts and seeds equal a fresh load.
 * Any change of the .conf, the .pro or a load option misses the cache; a
   damaged or truncated cache is rebuilt; an unwritable cache path still loads.
+* A network without a fixed seed (no -udfsed, no RandomSeeds macro) draws a
+  new seed on every load, as the reference does (code/NetSimGnl2_BulPp.cpp:
+  80-88), and is never cached.
 """
 import os
 import shutil
 
 import pytest
 
-from conftest import (GOLDEN, golden_cases, model_for, compare_outputs, golden_log_digest, file_digest)
+from conftest import (GOLDEN, golden_cases, model_for, compare_outputs, golden_log_digest, file_digest,
+                      generated_case)
 
 
 @pytest.mark.parametrize("case", golden_cases())
@@ -43,6 +47,19 @@ def test_threaded_setup_matches_reference(built, case, tmp_path):
     p = str(tmp_path / "network.log")
     m.network_log(p)
     assert file_digest(p) == golden_log_digest(case, "network.log -t 4")
+
+
+def test_logs_match_reference_at_connectome_scale(built, tmp_path):
+    # 20,000 one-neuron populations: a 329 MB ConfsInfo.log and a 93 MB
+    # network.log listing ~4.1 M synapses, both equal to the reference's
+    case = "connectome20k_d0"
+    generated_case(case, tmp_path)
+    m = model_for(built, case, conf_dir=tmp_path)
+    for f, write in (("ConfsInfo.log", m.confs_info), ("network.log", m.network_log)):
+        p = str(tmp_path / f)
+        write(p)
+        assert file_digest(p) == golden_log_digest(case, f), f
+        os.remove(p)
 
 
 def _copy_case(case, d):
@@ -131,3 +148,26 @@ def test_unwritable_cache_still_loads(built, tmp_path):
     assert m.info() == model_for(built, "small").info()
     assert "cannot write" in built.lib().fs_model_error().decode()
     assert built.Model(conf, pro).cache_status == "off"
+
+
+def test_unseeded_network_is_never_cached(built, tmp_path):
+    conf, pro = _copy_case("two_pop", tmp_path)
+    text = open(pro).read()
+    start, end = text.index("DefineMacro"), text.index("EndDefineMacro") + len("EndDefineMacro")
+    with open(pro, "w") as f:
+        f.write(text[:start] + text[end:])
+    cache = tmp_path / "c.bin"
+    seeds = set()
+    for _ in range(3):
+        m = built.Model(conf, pro, cache=str(cache))
+        assert m.cache_status == "unseeded"
+        seeds.add(m.seed(1))
+        m.close()
+    assert not cache.exists()
+    # std::random_device: three equal 32-bit draws would be a frozen seed
+    assert len(seeds) > 1
+    # the same files with a macro seed are cached as before
+    with open(pro, "w") as f:
+        f.write(text)
+    assert built.Model(conf, pro, cache=str(cache)).cache_status == "stored"
+    assert built.Model(conf, pro, cache=str(cache)).cache_status == "hit"

@@ -11,8 +11,8 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import (GOLDEN, ROOT, OracleEngine, compare_outputs, file_digest, first_diff, golden_cases,
-                      golden_log_digest, golden_outputs, model_for)
+from conftest import (GOLDEN, ROOT, OracleEngine, compare_outputs, file_digest, first_diff, generated_case,
+                      golden_cases, golden_log_digest, golden_outputs, model_for)
 
 pytestmark = pytest.mark.gpu
 
@@ -24,6 +24,19 @@ def test_gpu_compat_matches_reference_files(built, case, tmp_path):
     bad = compare_outputs(case, str(tmp_path))
     msgs = [(f, first_diff(os.path.join(GOLDEN, case, f), os.path.join(str(tmp_path), f))) for f in bad]
     assert not bad, msgs
+
+
+def test_gpu_compat_matches_reference_at_connectome_scale(built, tmp_path):
+    # 20,000 one-neuron populations, ~4.1 M synapse entries, delays 0, 100 ms:
+    # the reference's single-target path at the connectome configuration's
+    # size, byte for byte (size and SHA-256 of the reference's files)
+    case = "connectome20k_d0"
+    generated_case(case, tmp_path)
+    m = model_for(built, case, conf_dir=tmp_path)
+    out = tmp_path / "out"
+    out.mkdir()
+    m.run(str(out), mode="compat")
+    assert not compare_outputs(case, str(out))
 
 
 @pytest.mark.parametrize("case,steps", [("two_pop", 600), ("misc", 400), ("conn_ltp", 300), ("two_pop_stp", 300)])

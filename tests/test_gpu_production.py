@@ -48,6 +48,7 @@ def _small_net(fb, delays_lin, delays_gaba, delays_nmda, tm=False, dt=0.1):
 
 
 SMALL = {
+    "d0": ((0, 0, 0), (0,), (0, 0)),  # every delay 0: the single-step kernel (FP32)
     "dmin0": ((0, 7, 23), (3,), (0, 13)),
     "dmin10": ((10, 17, 49, 255), (12,), (10, 31)),
 }
@@ -146,6 +147,26 @@ def test_fp32_vs_fp64_connectome_20k(built):
     assert np.all(rates > 1.0)
     assert dr.max() < 0.02, dr
     assert dcv.max() < 0.05, dcv
+
+
+def test_fp32_vs_compat_connectome_20k_delays0(built, tmp_path):
+    # the reference-format 20k connectome (delays 0, parsed from its .conf):
+    # FP32 production (single-step kernel) against the reference-order compat
+    # path, 2 s each with independent random streams: E and I rates within
+    # 2 %, mean ISI CV within 5 %; FP32 against FP64 as on the delayed network
+    from conftest import generated_case, model_for
+    from flysim_b200 import netgen
+    generated_case("connectome20k_d0", tmp_path)
+    m = model_for(built, "connectome20k_d0", conf_dir=tmp_path)
+    c = netgen.connectome(n=20000, regions=58, seed=1)
+    groups = np.where(c.excit, 0, 1).astype(np.int64)
+    desc = m.desc()
+    _, dr, dcv, rates = _compare_modes(built, desc, 20000, groups, 20000, "fp32", "compat")
+    assert np.all(rates > 1.0)
+    assert dr.max() < 0.02 and dcv.max() < 0.05, (dr, dcv)
+    first, dr, dcv, _ = _compare_modes(built, desc, 20000, groups, 20000, "fp32", "fp64")
+    assert first >= 500, "rasters differ at step %d (< 50 ms)" % first
+    assert dr.max() < 0.02 and dcv.max() < 0.05, (dr, dcv)
 
 
 def test_two_population_fp32_vs_fp64_and_compat(built):
@@ -276,6 +297,86 @@ def test_bounded_wait_reports_timeout_and_device_stays_usable(built):
         e.reset(5)
         spk = e.step(3000)[0]
         assert sum(x.size for x in spk) > 100
+    finally:
+        e.close()
+
+
+def _both_kernels(fb, desc, steps_split, events=None, seed=5, **kw):
+    """Runs a delays-0 network on the single-step kernel and on the interval
+    kernel; returns both runs' (spikes per step, final V, spike counts)."""
+    out = []
+    for interval in (False, True):
+        e = fb.Engine(desc, "fp32", chunk_steps=700, interval_kernel=interval, **kw)
+        try:
+            assert e.layout()["single_step"] == (not interval)
+            e.reset(seed)
+            if events:
+                events(e)
+            sp = []
+            for k in steps_split:
+                sp += e.step(k)[0]
+            out.append((sp, e.state()[0].copy(), e.spike_counts()))
+        finally:
+            e.close()
+    return out
+
+
+@pytest.mark.parametrize("variant", ["plain", "tm", "events"])
+def test_single_step_kernel_equals_interval_kernel(built, variant):
+    # the 20k connectome with delays 0: shared-memory NMDA copies, deliveries
+    # by the targets' blocks and the ring hand-over between launches (calls
+    # of 1 step, chunks of 700) against the interval kernel, bit for bit
+    from flysim_b200 import netgen, network
+    c = netgen.connectome(n=20000, regions=58, seed=1)
+    na = network.connectome_net(c, with_delays=False, tm=(variant == "tm"))
+
+    def events(e):
+        e.set_drive(0, 5000, built.FS_NMDA, 0.02)
+        e.set_drive(3000, 9000, built.FS_GABA, 0.05)
+        e.set_injection(10000, 4000, 0.05, 0.3)
+    (a, Va, ca), (b, Vb, cb) = _both_kernels(built, na.desc, [1, 999, 1, 1500, 499],
+                                             events=events if variant == "events" else None)
+    assert sum(x.size for x in a) > 1000
+    for t, (x, y) in enumerate(zip(a, b)):
+        np.testing.assert_array_equal(x, y, err_msg="step %d" % t)
+    assert np.array_equal(Va.view(np.uint32), Vb.view(np.uint32))
+    np.testing.assert_array_equal(ca, cb)
+
+
+@pytest.mark.parametrize("case", ["two_pop", "two_pop_std", "two_pop_stp", "conn"])
+def test_single_step_kernel_on_reference_networks(built, case):
+    # networks read from the reference's own .conf format (delays 0, the
+    # reference's STD / STP plasticity, group and one-neuron populations)
+    from conftest import model_for
+    m = model_for(built, case)
+    (a, Va, ca), (b, Vb, cb) = _both_kernels(built, m.desc(), [1, 1200, 799])
+    assert sum(x.size for x in a) > 20
+    for t, (x, y) in enumerate(zip(a, b)):
+        np.testing.assert_array_equal(x, y, err_msg="step %d" % t)
+    assert np.array_equal(Va.view(np.uint32), Vb.view(np.uint32))
+    np.testing.assert_array_equal(ca, cb)
+
+
+def test_checkpoint_refused_after_a_wait_gave_up(built):
+    # the failure is made on the host: the handle's device error word is set
+    # as a bounded wait that gave up sets it (no kernel is stopped or hung);
+    # the state is then half an interval, so fs_sync reports the timeout and
+    # fs_checkpoint_save saves nothing; a reset clears the word
+    na = _conn_net()
+    e = built.Engine(na.desc, "fp32")
+    try:
+        e.reset(5)
+        e.run(500)
+        e.inject_wait_failure()
+        with pytest.raises(built.FsError) as ex:
+            e.checkpoint()
+        assert ex.value.code == built.FS_ERR_TIMEOUT
+        with pytest.raises(built.FsError) as ex:
+            e.sync()
+        assert ex.value.code == built.FS_ERR_TIMEOUT
+        e.reset(5)
+        e.run(500)
+        assert len(e.checkpoint()) > 0
     finally:
         e.close()
 

@@ -10,7 +10,7 @@ import os
 
 import pytest
 
-from conftest import golden_cases, model_for, compare_outputs, first_diff, GOLDEN
+from conftest import golden_cases, model_for, compare_outputs, first_diff, generated_case, GOLDEN
 
 
 @pytest.mark.parametrize("case", golden_cases())
@@ -25,6 +25,24 @@ def test_oracle_matches_reference_files(built, oracle, case, tmp_path):
     bad = compare_outputs(case, str(tmp_path))
     msgs = [(f, first_diff(os.path.join(GOLDEN, case, f), os.path.join(str(tmp_path), f))) for f in bad]
     assert not bad, msgs
+
+
+def test_oracle_matches_reference_at_connectome_scale(built, oracle, tmp_path):
+    # the 20,000-neuron connectome-shaped network with delays 0 (about 4.1 M
+    # synapse entries on the reference's single-target path,
+    # code/EqsGnl2.cpp:404-502), 100 ms, reference run with -t 1: the
+    # oracle's Spikes.dat and rate file equal the reference's (size, SHA-256)
+    case = "connectome20k_d0"
+    generated_case(case, tmp_path)
+    m = model_for(built, case, conf_dir=tmp_path)
+    out = tmp_path / "out"
+    out.mkdir()
+    ctx = oracle.oracle_create(m.desc())
+    try:
+        m.run_with(oracle.oracle_engine(), ctx, str(out))
+    finally:
+        oracle.oracle_destroy(ctx)
+    assert not compare_outputs(case, str(out))
 
 
 def test_golden_cases_cover_the_features():
