@@ -139,6 +139,7 @@ def lib() -> C.CDLL:
         "fs_debug_barrier_timeout": (C.c_int, [C.c_uint32]),
         "fs_debug_philox": (C.c_int, [_u32, _u32, C.c_uint64, _u32]),
         "fs_engine_layout": (C.c_int, [vp, _u32, _u32, _u32, C.POINTER(C.c_int)]),
+        "fs_debug_single_step_plan": (C.c_int, [C.POINTER(NetDesc), C.c_uint32, C.POINTER(C.c_uint64)]),
         "fs_debug_drive": (C.c_int, [vp, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32,
                                      C.POINTER(C.c_uint8), C.POINTER(C.c_double)]),
         "fs_debug_inject_wait_failure": (C.c_int, [vp]),
@@ -199,7 +200,8 @@ def exported_symbols() -> Sequence[str]:
                         "fs_reset", "fs_set_drive", "fs_set_act", "fs_set_injection", "fs_step", "fs_run",
                         "fs_run_timed",
                         "fs_sync", "fs_stats", "fs_kernel_time", "fs_debug_expf", "fs_debug_expf_noalloc",
-                        "fs_get_state", "fs_debug_barrier_timeout", "fs_engine_layout", "fs_debug_philox",
+                        "fs_get_state", "fs_debug_barrier_timeout", "fs_engine_layout",
+                        "fs_debug_single_step_plan", "fs_debug_philox",
                         "fs_debug_drive",
                         "fs_debug_inject_wait_failure", "fs_checkpoint_size", "fs_checkpoint_save", "fs_checkpoint_load",
                         "fs_get_syn_state", "fs_model_load", "fs_model_load_cached", "fs_model_confs_info", "fs_model_network_log",
@@ -496,6 +498,15 @@ class Engine:
 
 def device_engine_vtbl():
     return lib().fs_device_engine()
+
+
+def single_step_plan(desc, sm_count: int = 148) -> dict:
+    """Host-only check of the single-step kernel's plan for a network."""
+    st = (C.c_uint64 * 8)()
+    dp = desc if isinstance(desc, C._Pointer) else C.pointer(desc)
+    _check(lib().fs_debug_single_step_plan(dp, sm_count, st))
+    keys = ("qualifies", "blocks", "max_posts", "max_tracked", "max_edges", "smem", "lin_entries", "nmda_edges")
+    return dict(zip(keys, [int(x) for x in st]))
 
 
 def debug_philox(ctr: np.ndarray, key: np.ndarray) -> np.ndarray:

@@ -673,6 +673,15 @@ int fs_engine_layout(fs_handle *h, uint32_t *blocks, uint32_t *threads, uint32_t
   return FS_OK;
 }
 
+int fs_debug_single_step_plan(const fs_net_desc *desc, uint32_t sm_count, uint64_t *stats) {
+  if (!desc || !desc->syn || !stats || sm_count == 0)
+    return set_err(nullptr, FS_ERR_ARG, "fs_debug_single_step_plan: null argument");
+  std::string err;
+  int rc = fsp::prod_check_single_plan(desc, sm_count, stats, err);
+  if (!rc && !stats[0]) set_err(nullptr, FS_OK, err.empty() ? "not taken (delays or mode)" : err);
+  return rc ? set_err(nullptr, rc, err) : FS_OK;
+}
+
 int fs_debug_philox(const uint32_t *ctr, const uint32_t *key, uint64_t k, uint32_t *out) {
   if (k == 0) return FS_OK;
   if (!ctr || !key || !out) return set_err(nullptr, FS_ERR_ARG, "fs_debug_philox: null argument");

@@ -1397,6 +1397,110 @@ int finish(Prod *p, cudaStream_t st, std::string &err) {
 
 }  // namespace
 
+// ---- host tables of a production network -----------------------------------
+// From the flat synapse list: the receptor kinetics each presynaptic neuron
+// imposes on its gates (production modes need one per (neuron, receptor)),
+// the receptors each neuron projects with, the delay range, and the two CSR
+// tables (linear out-edges by pre: code = post | receptor << 22 | delay <<
+// 24; NMDA in-edges by post: code = pre | delay << 24) in synapse-list order.
+struct HostNet {
+  uint32_t n = 0, nlin = 0, dmin = 0, dmax = 0;
+  int lin_of_rec[4] = {-1, -1, -1, -1};
+  uint64_t nlin_e = 0, nnm_e = 0;
+  std::vector<float> pdf, p_dfxt, p_dfst, p_efas;
+  std::vector<uint8_t> proj;
+  std::vector<uint32_t> out_row, in_row, out_code, in_code;
+  std::vector<float> out_w, in_w;
+};
+
+static int host_net(const fs_net_desc *d, HostNet &H, std::string &err) {
+  const fs_neurons &v = d->neurons;
+  const uint32_t n = v.n;
+  H.n = n;
+  const fs_syn_list &S = *d->syn;
+  std::vector<float> &pdf = H.pdf, &p_dfxt = H.p_dfxt, &p_dfst = H.p_dfst, &p_efas = H.p_efas;
+  pdf.assign((size_t)4 * n, -1.0f);
+  p_dfxt.assign(n, -1.0f);
+  p_dfst.assign(n, -1.0f);
+  p_efas.assign(n, -1.0f);
+  std::vector<uint8_t> &proj = H.proj;
+  proj.assign(n, 0);
+  bool present[5] = {false, false, false, false, false};
+  uint32_t dmin = 0xffffffffu, dmax = 0;
+  uint64_t nlin_e = 0, nnm_e = 0;
+  for (uint64_t e = 0; e < S.n; e++) {
+    const uint32_t a = S.pre[e], b = S.post[e], r = S.rec[e];
+    const uint32_t dl = S.delay ? S.delay[e] : 0;
+    if (a >= n || b >= n || r >= FS_NREC) {
+      err = "synapse list: index out of range";
+      return FS_ERR_ARG;
+    }
+    if (dl > 255) {
+      err = "synapse delays above 255 steps are not supported";
+      return FS_ERR_UNSUPPORTED;
+    }
+    dmin = std::min(dmin, dl);
+    dmax = std::max(dmax, dl);
+    present[r] = true;
+    proj[a] |= (uint8_t)(1u << r);
+    auto same = [&](float &slot, float val) -> bool {
+      if (slot < 0.0f) { slot = val; return true; }
+      return slot == val;
+    };
+    bool ok;
+    if (r != FS_NMDA) {
+      ok = same(pdf[(size_t)r * n + a], v.dfst[(size_t)r * n + b]);
+      nlin_e++;
+    } else {
+      ok = same(p_dfxt[a], v.nmda_dfxt[b]) && same(p_dfst[a], v.dfst[(size_t)FS_NMDA * n + b]) &&
+           same(p_efas[a], v.nmda_efst[b] * v.nmda_as[b]);
+      nnm_e++;
+    }
+    if (!ok) {
+      err = "production modes need one receptor time constant per (presynaptic neuron, receptor); "
+            "targets of a neuron differ (use FS_MODE_COMPAT)";
+      return FS_ERR_UNSUPPORTED;
+    }
+  }
+  if (S.n == 0) dmin = 0;
+  H.dmin = dmin;
+  H.dmax = dmax;
+  H.nlin_e = nlin_e;
+  H.nnm_e = nnm_e;
+  for (int r = 0; r < 4; r++) H.lin_of_rec[r] = present[r] ? (int)(H.nlin++) : -1;
+  for (auto &x : pdf) if (x < 0) x = 0;
+  for (auto *vv : {&p_dfxt, &p_dfst, &p_efas}) for (auto &x : *vv) if (x < 0) x = 0;
+  // ---- CSR of linear out-edges (by pre) and NMDA in-edges (by post) ----
+  std::vector<uint32_t> &out_row = H.out_row, &in_row = H.in_row;
+  out_row.assign(n + 1, 0);
+  in_row.assign(n + 1, 0);
+  for (uint64_t e = 0; e < S.n; e++) {
+    if (S.rec[e] == FS_NMDA) in_row[S.post[e] + 1]++;
+    else out_row[S.pre[e] + 1]++;
+  }
+  for (uint32_t i = 0; i < n; i++) { out_row[i + 1] += out_row[i]; in_row[i + 1] += in_row[i]; }
+  H.out_code.assign(nlin_e, 0);
+  H.in_code.assign(nnm_e, 0);
+  H.out_w.assign(nlin_e, 0.0f);
+  H.in_w.assign(nnm_e, 0.0f);
+  {
+    std::vector<uint32_t> fo(out_row.begin(), out_row.end() - 1), fi(in_row.begin(), in_row.end() - 1);
+    for (uint64_t e = 0; e < S.n; e++) {
+      const uint32_t dl = S.delay ? S.delay[e] : 0;
+      if (S.rec[e] == FS_NMDA) {
+        const uint32_t q = fi[S.post[e]]++;
+        H.in_code[q] = S.pre[e] | (dl << 24);
+        H.in_w[q] = S.g[e];
+      } else {
+        const uint32_t q = fo[S.pre[e]]++;
+        H.out_code[q] = S.post[e] | ((uint32_t)S.rec[e] << 22) | (dl << 24);
+        H.out_w[q] = S.g[e];
+      }
+    }
+  }
+  return FS_OK;
+}
+
 // ---- plan of the single-step kernel ------------------------------------------
 // Posts are cut into at most one block per SM, in whole warps (32 posts) and
 // at most kT1 posts per block, balanced by a cost of 24 per post plus its
@@ -1420,10 +1524,13 @@ static bool plan_single(uint32_t n, uint32_t nlin, uint32_t sm_count, const std:
                         const std::vector<uint32_t> &out_row, const std::vector<uint32_t> &out_code,
                         const std::vector<float> &out_w, const std::vector<float> &p_dfxt,
                         const std::vector<float> &p_dfst, const std::vector<float> &p_efas, const uint8_t *proj,
-                        Single &S1) {
+                        Single &S1, std::string &why) {
   const uint32_t units = (n + 31) / 32, per = kT1 / 32;
   uint32_t B = std::min<uint32_t>(sm_count, units);
-  if (B == 0 || (uint64_t)B * per < units) return false;
+  if (B == 0 || (uint64_t)B * per < units) {
+    why = "more than 512 posts per block would be needed";
+    return false;
+  }
   // linear in-degree per post
   std::vector<uint32_t> lin_in(n, 0);
   for (uint32_t e = 0; e < out_code.size(); e++) lin_in[out_code[e] & 0x3fffffu]++;
@@ -1442,11 +1549,14 @@ static bool plan_single(uint32_t n, uint32_t nlin, uint32_t sm_count, const std:
     c = std::max(c, cut[b - 1] + 1);
     c = std::min(c, cut[b - 1] + per);
     c = std::max<uint32_t>(c, units > per * (B - b) ? units - per * (B - b) : 0);
-    c = std::min(c, units);
+    c = std::min(c, units - (B - b));  // every later block keeps at least one unit
     cut[b] = c;
   }
   for (uint32_t b = 0; b < B; b++)
-    if (cut[b + 1] - cut[b] > per) return false;
+    if (cut[b + 1] - cut[b] > per || cut[b + 1] == cut[b]) {
+      why = "no balanced cut of the posts";
+      return false;
+    }
   // NMDA kinetics classes of the presynaptic neurons
   std::vector<int> cls_of(n, -1);
   std::vector<std::array<uint32_t, 3>> tabs;
@@ -1459,7 +1569,10 @@ static bool plan_single(uint32_t n, uint32_t nlin, uint32_t sm_count, const std:
     size_t c = 0;
     while (c < tabs.size() && tabs[c] != k) c++;
     if (c == tabs.size()) {
-      if (tabs.size() == 255) return false;
+      if (tabs.size() == 255) {
+        why = "more than 255 NMDA kinetics classes";
+        return false;
+      }
       tabs.push_back(k);
     }
     cls_of[i] = (int)c;
@@ -1497,7 +1610,10 @@ static bool plan_single(uint32_t n, uint32_t nlin, uint32_t sm_count, const std:
     for (uint64_t x : L) trk.push_back((uint32_t)(x >> 32));
     std::sort(trk.begin(), trk.end());
     trk.erase(std::unique(trk.begin(), trk.end()), trk.end());
-    if (trk.size() > 65535) return false;
+    if (trk.size() > 65535) {
+      why = "a block tracks more than 65535 presynaptic neurons";
+      return false;
+    }
     Blk1 bk{};
     bk.post0 = P0;
     bk.np = P1 - P0;
@@ -1540,9 +1656,96 @@ static bool plan_single(uint32_t n, uint32_t nlin, uint32_t sm_count, const std:
     smax = std::max(smax, need);
   }
   // dynamic shared memory next to the kernel's ~15 KB of static arrays
-  if (smax > (size_t)200 * 1024) return false;
+  if (smax > (size_t)200 * 1024) {
+    why = "a block's tables need " + std::to_string(smax) + " bytes of shared memory";
+    return false;
+  }
   S1.smem = (uint32_t)((smax + 15) & ~(size_t)15);
   return true;
+}
+
+// Host-side check of a single-step plan: every index k_prod1 forms from the
+// plan stays inside the arrays and the shared memory it sizes, and the plan
+// holds each synapse of the network exactly once.
+static bool validate_single(const HostNet &H, const Single &S1, std::string &err) {
+  const uint32_t n = H.n;
+  auto fail = [&](uint32_t b, const char *what) {
+    err = "single-step plan, block " + std::to_string(b) + ": " + what;
+    return false;
+  };
+  const uint32_t ncls = (uint32_t)(S1.tab.size() / 3);
+  uint32_t next_post = 0;
+  uint64_t lin_total = 0, nmda_total = 0;
+  std::vector<uint8_t> seen;
+  for (uint32_t b = 0; b < S1.blk.size(); b++) {
+    const Blk1 &k = S1.blk[b];
+    if (k.post0 != next_post || k.post0 % 32 || k.np == 0 || k.np > kT1 || k.post0 + k.np > n)
+      return fail(b, "post range");
+    next_post = k.post0 + k.np;
+    if (k.ntrk > 65535 || (size_t)k.trk0 + k.ntrk > S1.gid.size() || (size_t)k.lrow0 + k.ntrk + 1 > S1.lrow.size() ||
+        (size_t)k.erow0 + k.np + 1 > S1.erow.size() || (size_t)k.e0 + k.ne > S1.ew.size() ||
+        (size_t)k.e0 + k.ne > S1.eidx.size())
+      return fail(b, "table range");
+    for (uint32_t j = 0; j < k.ntrk; j++) {
+      const uint32_t g = S1.gid[k.trk0 + j];
+      if (g >= n || (j && g <= S1.gid[k.trk0 + j - 1])) return fail(b, "tracked ids not sorted");
+      const uint8_t c = S1.cls[k.trk0 + j];
+      if (c != 255 && c >= ncls) return fail(b, "kinetics class");
+    }
+    const uint32_t *lr = &S1.lrow[k.lrow0];
+    if (lr[0] != 0) return fail(b, "linear rows");
+    for (uint32_t j = 0; j < k.ntrk; j++)
+      if (lr[j + 1] < lr[j]) return fail(b, "linear rows");
+    if ((size_t)k.l0 + lr[k.ntrk] > S1.lin.size() || (size_t)k.l0 + lr[k.ntrk] > S1.linw.size())
+      return fail(b, "linear entries");
+    for (uint32_t e = 0; e < lr[k.ntrk]; e++) {
+      const uint32_t code = S1.lin[k.l0 + e], r = code >> 16, q = code & 0xffffu;
+      if (q >= k.np || r > 3 || H.lin_of_rec[r] < 0) return fail(b, "linear entry");
+    }
+    lin_total += lr[k.ntrk];
+    const uint32_t *er = &S1.erow[k.erow0];
+    if (er[0] != 0 || er[k.np] != k.ne) return fail(b, "edge rows");
+    for (uint32_t q = 0; q < k.np; q++)
+      if (er[q + 1] < er[q] || er[q + 1] - er[q] != H.in_row[k.post0 + q + 1] - H.in_row[k.post0 + q])
+        return fail(b, "edge rows");
+    for (uint32_t e = 0; e < k.ne; e++) {
+      const uint16_t j = S1.eidx[k.e0 + e];
+      if (j >= k.ntrk || S1.cls[k.trk0 + j] == 255) return fail(b, "edge index");
+      if (S1.gid[k.trk0 + j] != (H.in_code[H.in_row[k.post0] + e] & 0xffffffu)) return fail(b, "edge source");
+    }
+    nmda_total += k.ne;
+    const size_t need = (size_t)std::max(1u, H.nlin) * kT1 * 8 + (size_t)k.ntrk * 12 + 3 * (size_t)ncls * 4 +
+                        (size_t)k.ne * 4 + (size_t)k.ntrk * 4 + ((size_t)k.ntrk + 1) * 4 + ((size_t)k.np + 1) * 4 +
+                        (size_t)k.ne * 2 + (size_t)k.ntrk * 2;
+    if (need > S1.smem) return fail(b, "shared memory");
+  }
+  if (next_post != n) return fail((uint32_t)S1.blk.size(), "posts not covered");
+  if (lin_total != H.nlin_e || nmda_total != H.nnm_e) return fail(0, "synapse count");
+  return true;
+}
+
+int prod_check_single_plan(const fs_net_desc *d, uint32_t sm_count, uint64_t *stats, std::string &err) {
+  HostNet H;
+  int rc = host_net(d, H, err);
+  if (rc) return rc;
+  for (int i = 0; i < 8; i++) stats[i] = 0;
+  if (H.dmax != 0) return FS_OK;
+  Single S1;
+  if (!plan_single(H.n, H.nlin, sm_count, H.in_row, H.in_code, H.in_w, H.out_row, H.out_code, H.out_w, H.p_dfxt,
+                   H.p_dfst, H.p_efas, H.proj.data(), S1, err))
+    return FS_OK;
+  if (!validate_single(H, S1, err)) return FS_ERR_ARG;
+  stats[0] = 1;
+  stats[1] = S1.blk.size();
+  for (const Blk1 &k : S1.blk) {
+    stats[2] = std::max<uint64_t>(stats[2], k.np);
+    stats[3] = std::max<uint64_t>(stats[3], k.ntrk);
+    stats[4] = std::max<uint64_t>(stats[4], k.ne);
+  }
+  stats[5] = S1.smem;
+  stats[6] = S1.lin.size();
+  stats[7] = S1.eidx.size();
+  return FS_OK;
 }
 
 int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t sm_count, cudaStream_t st,
@@ -1573,51 +1776,21 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
   P.n = n;
   for (int r = 0; r < 5; r++) P.rg[r] = 1.0f;
   const size_t nr = (size_t)FS_NREC * n;
-  const fs_syn_list &S = *d->syn;
-  // ---- receptor kinetics seen by each presynaptic neuron ----
-  std::vector<float> pdf((size_t)4 * n, -1.0f), p_dfxt(n, -1.0f), p_dfst(n, -1.0f), p_efas(n, -1.0f);
-  std::vector<uint8_t> proj(n, 0);
-  bool present[5] = {false, false, false, false, false};
-  uint32_t dmin = 0xffffffffu, dmax = 0;
-  uint64_t nlin_e = 0, nnm_e = 0;
-  for (uint64_t e = 0; e < S.n; e++) {
-    const uint32_t a = S.pre[e], b = S.post[e], r = S.rec[e];
-    const uint32_t dl = S.delay ? S.delay[e] : 0;
-    if (a >= n || b >= n || r >= FS_NREC) {
-      err = "synapse list: index out of range";
+  HostNet H;
+  {
+    int hrc = host_net(d, H, err);
+    if (hrc) {
       delete p;
-      return FS_ERR_ARG;
-    }
-    if (dl > 255) {
-      err = "synapse delays above 255 steps are not supported";
-      delete p;
-      return FS_ERR_UNSUPPORTED;
-    }
-    dmin = std::min(dmin, dl);
-    dmax = std::max(dmax, dl);
-    present[r] = true;
-    proj[a] |= (uint8_t)(1u << r);
-    auto same = [&](float &slot, float val) -> bool {
-      if (slot < 0.0f) { slot = val; return true; }
-      return slot == val;
-    };
-    bool ok;
-    if (r != FS_NMDA) {
-      ok = same(pdf[(size_t)r * n + a], v.dfst[(size_t)r * n + b]);
-      nlin_e++;
-    } else {
-      ok = same(p_dfxt[a], v.nmda_dfxt[b]) && same(p_dfst[a], v.dfst[(size_t)FS_NMDA * n + b]) &&
-           same(p_efas[a], v.nmda_efst[b] * v.nmda_as[b]);
-      nnm_e++;
-    }
-    if (!ok) {
-      err = "production modes need one receptor time constant per (presynaptic neuron, receptor); "
-            "targets of a neuron differ (use FS_MODE_COMPAT)";
-      delete p;
-      return FS_ERR_UNSUPPORTED;
+      return hrc;
     }
   }
-  if (S.n == 0) dmin = 0;
+  const uint32_t dmin = H.dmin, dmax = H.dmax;
+  const uint64_t nlin_e = H.nlin_e, nnm_e = H.nnm_e;
+  std::vector<float> &pdf = H.pdf, &p_dfxt = H.p_dfxt, &p_dfst = H.p_dfst, &p_efas = H.p_efas;
+  std::vector<uint8_t> &proj = H.proj;
+  std::vector<uint32_t> &out_row = H.out_row, &in_row = H.in_row, &out_code = H.out_code, &in_code = H.in_code;
+  std::vector<float> &out_w = H.out_w, &in_w = H.in_w;
+  const fs_syn_list &S = *d->syn;
   p->d_min = dmin;
   p->d_max = dmax;
   p->lin_edges = nlin_e;
@@ -1631,34 +1804,9 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
   P.interval = std::max<uint32_t>(1, dmin);
   P.dmax0 = dmax == 0 ? 1u : 0u;
   if (gap) P.interval = 1;  // a gap current reads every neuron's V of the step before
-  for (int r = 0; r < 4; r++) P.lin_of_rec[r] = present[r] ? (int)(p->nlin++) : -1;
+  p->nlin = H.nlin;
+  for (int r = 0; r < 4; r++) P.lin_of_rec[r] = H.lin_of_rec[r];
   P.nlin = p->nlin;
-  for (auto &x : pdf) if (x < 0) x = 0;
-  for (auto *vv : {&p_dfxt, &p_dfst, &p_efas}) for (auto &x : *vv) if (x < 0) x = 0;
-  // ---- CSR of linear out-edges (by pre) and NMDA in-edges (by post) ----
-  std::vector<uint32_t> out_row(n + 1, 0), in_row(n + 1, 0);
-  for (uint64_t e = 0; e < S.n; e++) {
-    if (S.rec[e] == FS_NMDA) in_row[S.post[e] + 1]++;
-    else out_row[S.pre[e] + 1]++;
-  }
-  for (uint32_t i = 0; i < n; i++) { out_row[i + 1] += out_row[i]; in_row[i + 1] += in_row[i]; }
-  std::vector<uint32_t> out_code(nlin_e), in_code(nnm_e);
-  std::vector<float> out_w(nlin_e), in_w(nnm_e);
-  {
-    std::vector<uint32_t> fo(out_row.begin(), out_row.end() - 1), fi(in_row.begin(), in_row.end() - 1);
-    for (uint64_t e = 0; e < S.n; e++) {
-      const uint32_t dl = S.delay ? S.delay[e] : 0;
-      if (S.rec[e] == FS_NMDA) {
-        const uint32_t q = fi[S.post[e]]++;
-        in_code[q] = S.pre[e] | (dl << 24);
-        in_w[q] = S.g[e];
-      } else {
-        const uint32_t q = fo[S.pre[e]]++;
-        out_code[q] = S.post[e] | ((uint32_t)S.rec[e] << 22) | (dl << 24);
-        out_w[q] = S.g[e];
-      }
-    }
-  }
   // ---- grid: all blocks co-resident; posts split by estimated cost ----
   int occ = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p->fp64 ? (const void *)k_prod<double, 4> : (const void *)k_prod<float, 4>,
@@ -1755,8 +1903,13 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
   // single-step kernel: FP32, every delay 0, no gap junctions
   if (allow_single && !p->fp64 && dmax == 0 && !gap && S.n > 0 && !(o.flags & FS_RUN_INTERVAL_KERNEL)) {
     Single S1;
+    std::string why;
     if (plan_single(n, p->nlin, sm_count, in_row, in_code, in_w, out_row, out_code, out_w, p_dfxt, p_dfst, p_efas,
-                    proj.data(), S1)) {
+                    proj.data(), S1, why)) {
+      if (!validate_single(H, S1, err)) {
+        rc = FS_ERR_ARG;
+        goto fail;
+      }
       // the attribute is per kernel, not per handle: always the largest
       // dynamic size any plan may take
       int dev = 0, maxsm = 0;

@@ -24,6 +24,11 @@ int prod_check(Prod *p, cudaStream_t st, uint64_t *spikes_total, std::string &er
 void prod_kernel_time(Prod *p, double *ms_per_launch, uint64_t *launches);
 int prod_get_state(Prod *p, float *V, int32_t *Count, uint32_t *NState, cudaStream_t st, std::string &err);
 
+// Builds the single-step plan of a network on the host (no device needed)
+// and checks every index the kernel derives from it; stats[0] = 1 when the
+// network qualifies, then blocks, max posts, max tracked neurons, max NMDA
+// edges per block, shared-memory bytes, linear entries, NMDA edges.
+int prod_check_single_plan(const fs_net_desc *d, uint32_t sm_count, uint64_t *stats, std::string &err);
 // Layout facts for measurement (algorithmic bytes).
 struct ProdInfo {
   uint32_t n, d_min, d_max, slots, interval, blocks, threads, chunks;

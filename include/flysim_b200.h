@@ -291,6 +291,14 @@ int fs_debug_barrier_timeout(uint32_t poll_limit);
 int fs_debug_philox(const uint32_t *ctr, const uint32_t *key, uint64_t k, uint32_t *out);
 int fs_debug_drive(fs_handle *h, uint64_t t0, uint32_t nsteps, uint32_t first, uint32_t count, uint8_t *hits,
                    double *gauss);
+/* Host-only check of the single-step kernel's plan for a network (no device
+ * needed): builds the per-block tables for sm_count blocks and verifies every
+ * index the kernel forms from them.  stats[8]: [0] 1 if the network takes
+ * the single-step kernel, [1] blocks, [2] max posts, [3] max tracked
+ * neurons, [4] max NMDA edges per block, [5] shared-memory bytes, [6]
+ * linear delivery entries, [7] NMDA edges.  FS_ERR_ARG names a violated
+ * bound.  No counterpart in the reference. */
+int fs_debug_single_step_plan(const fs_net_desc *desc, uint32_t sm_count, uint64_t *stats);
 /* Failure detection on the host side: stores into the handle's device error
  * word what a bounded device wait that gave up stores, without running or
  * stopping any kernel, so that the paths which must notice it (fs_sync,
