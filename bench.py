@@ -110,6 +110,9 @@ class ClockSampler:
 # plasticity on excitatory synapses; its working set is far beyond L2)
 WORKLOADS = {
     "connectome20k": dict(n=N_NEURONS, mean_degree=120.0, tm=False),
+    # the same network with delays 0, as the reference format expresses it
+    # (the single-step kernel; the bench line's same_network block)
+    "connectome20k_d0": dict(n=N_NEURONS, mean_degree=120.0, tm=False, delays=False),
     "scaled1m": dict(n=1_000_000, mean_degree=100.0, tm=True),
     "scaled250k": dict(n=250_000, mean_degree=100.0, tm=True),  # the same network, sized for ncu captures
 }
@@ -122,11 +125,11 @@ def build_network(rank: int, workload: str = "connectome20k", n: int = 0):
     w = dict(WORKLOADS[workload])
     if n > 0:
         w["n"] = n
-    if workload == "connectome20k":
+    if workload.startswith("connectome20k"):
         c = netgen.connectome(n=w["n"], regions=REGIONS, seed=SEED + rank)
     else:
         c = netgen.connectome_fast(n=w["n"], regions=REGIONS, mean_degree=w["mean_degree"], seed=SEED + rank)
-    return c, network.connectome_net(c, dt=DT, with_delays=True, tm=w["tm"])
+    return c, network.connectome_net(c, dt=DT, with_delays=w.get("delays", True), tm=w["tm"])
 
 
 def max_over_ranks(x: float, world: int, device: str = "cuda") -> float:

@@ -58,7 +58,7 @@ class Neurons(C.Structure):
 class RecLayout(C.Structure):
     _fields_ = [("n_gates", C.c_uint32), ("gate_pre", _u32), ("gate_post0", _u32), ("gate_g", _f),
                 ("gather_rowptr", _u32), ("gather_gate", _u32), ("n_recs", C.c_uint32), ("rec_pre", _u32),
-                ("rec_post", _u32), ("rec_g", _f), ("rec_rowptr", _u32)]
+                ("rec_post", _u32), ("rec_g", _f), ("rec_rowptr", _u32), ("rec_src", _u32)]
 
 
 class CompatLayout(C.Structure):
@@ -398,6 +398,29 @@ class Engine:
         if want_Irep or want_nstate:
             return spikes, V, I, NS
         return spikes, V
+
+    def step_gv(self, nsteps: int, gv_sel):
+        """Runs nsteps with GatingVariable outputs for the selected
+        single-target records (receptor << 28 | record index); returns
+        (spikes per step, st [nsteps, k], xt [nsteps, k])."""
+        sel = np.ascontiguousarray(gv_sel, np.uint32)
+        k = sel.size
+        counts = np.zeros(nsteps, np.uint32)
+        cap = max(1024, nsteps * self.n)
+        idx = np.zeros(cap, np.uint32)
+        gst = np.zeros((nsteps, k), np.float32)
+        gxt = np.zeros((nsteps, k), np.float32)
+        so = StepOut()
+        so.spike_count = counts.ctypes.data_as(_u32)
+        so.spike_idx = idx.ctypes.data_as(_u32)
+        so.spike_cap = cap
+        so.gv_sel = sel.ctypes.data_as(_u32)
+        so.gv_n = k
+        so.gv_st = gst.ctypes.data_as(_f)
+        so.gv_xt = gxt.ctypes.data_as(_f)
+        _check(lib().fs_step(self._h, nsteps, C.byref(so)), self._h)
+        offs = np.concatenate([[0], np.cumsum(counts.astype(np.int64))])
+        return [idx[offs[i]:offs[i + 1]].copy() for i in range(nsteps)], gst, gxt
 
     def step_csr(self, nsteps: int, spike_cap: Optional[int] = None):
         """Runs nsteps; returns the spikes as the C ABI gives them: per-step

@@ -119,6 +119,11 @@ struct Params {
   const float *t1_linw, *t1_ew, *t1_cls_tab;
   const uint16_t *t1_eidx;
   uint32_t t1_ncls, t1_smem;
+  // GatingVariable output (or null): selections of neuron p are entries
+  // [gv_row[p], gv_row[p+1]) of gv_ent (output column | receptor << 28)
+  const uint32_t *gv_row, *gv_ent;
+  uint32_t gv_n;
+  float *gv_st, *gv_xt;  // [steps][gv_n]
   uint32_t *t1_cnt;      // [2] spikes listed in the step of each parity
   uint4 *t1_list;        // [2][n][2] (id, inc, c0, c1), (c2, c3, 0, 0)
 };
@@ -734,6 +739,25 @@ __device__ __forceinline__ void spike_outputs(const Params &P, uint32_t m, bool 
   }
 }
 
+// GatingVariable columns of neuron p after step s: a single-target record's
+// gate is its presynaptic neuron's gate of the receptor; NMDA records take
+// the neuron's x and s (code/NetSimGnl2_info.cpp:701-758 prints st, and xt
+// for NMDA).
+template <class T>
+__device__ __forceinline__ void gv_write(const Params &P, uint32_t p, uint32_t s, const NeuronState<T> &st) {
+  for (uint32_t e = __ldg(P.gv_row + p), e1 = __ldg(P.gv_row + p + 1); e < e1; e++) {
+    const uint32_t code = __ldg(P.gv_ent + e), col = code & 0x0fffffffu, r = code >> 28;
+    const size_t o = (size_t)s * P.gv_n + col;
+    if (r == FS_NMDA) {
+      P.gv_st[o] = (float)st.spre;
+      P.gv_xt[o] = (float)st.xp;
+    } else {
+      P.gv_st[o] = (float)(r == 0 ? st.sp[0] : r == 1 ? st.sp[1] : r == 2 ? st.sp[2] : st.sp[3]);
+      P.gv_xt[o] = 0.0f;
+    }
+  }
+}
+
 // ---- L steps of a tile's neurons (thread per neuron), with the pushes ----
 // Per-neuron parameters and state stay in registers for the L steps; the
 // ring slots of the next PD steps are in flight while the current step
@@ -790,6 +814,7 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
     const bool spk = neuron_step<T>(P, q, st, cur, gn[j][qs], hits[j][qs], gauss[j][qs],
                                     P.gap_row ? gapI[qs] : (T)0, p, own, s, cinc, inc);
     nsp += spk ? 1u : 0u;
+    if (own && P.gv_row) gv_write<T>(P, p, s, st);
     if (own && (q.pj & (1u << FS_NMDA))) {
       if constexpr (sizeof(T) == 4) {
 #pragma unroll
@@ -1147,6 +1172,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
       float cinc[4], inc;
       const bool spk = neuron_step<float>(P, q, st, rv, gn[qs], d_hits[qs], d_gauss[qs], 0.0f, p, own, s, cinc, inc);
       nsp += spk ? 1u : 0u;
+      if (own && P.gv_row) gv_write<float>(P, p, s, st);
       const uint32_t m = __ballot_sync(fsd::kFull, spk);
       if (m) {
         spike_outputs(P, m, spk, p, s, lane);
@@ -1255,6 +1281,13 @@ struct Prod {
   uint64_t kl = 0;
   uint64_t key = 0;
   std::vector<uint32_t> host_counts;
+  // GatingVariable selections: presynaptic neuron of each record, per
+  // receptor (from the compat layout), and the device buffers of a call
+  std::vector<uint32_t> rec_src[FS_NREC];
+  uint32_t *gv_row = nullptr, *gv_ent = nullptr;
+  float *gv_st = nullptr, *gv_xt = nullptr;
+  uint64_t gv_out_cap = 0;
+  uint32_t gv_ent_cap = 0;
   std::vector<uint32_t> in_row_h;  // NMDA in-degree prefix (block partitioning)
 };
 
@@ -1312,7 +1345,7 @@ int ensure_buffers(Prod *p, uint32_t steps, bool wantV, bool wantI, bool wantNS,
 }
 
 int launch(Prod *p, uint32_t nsteps, bool want_bits, bool wantV, cudaStream_t st, uint64_t *launches,
-           std::string &err, bool wantI = false, bool wantNS = false) {
+           std::string &err, bool wantI = false, bool wantNS = false, bool wantGV = false) {
   int rc = ensure_buffers(p, nsteps, wantV, wantI, wantNS, err);
   if (rc) return rc;
   const uint32_t words = (p->n + 31) / 32;
@@ -1332,6 +1365,16 @@ int launch(Prod *p, uint32_t nsteps, bool want_bits, bool wantV, cudaStream_t st
   P.outV = wantV ? p->outV : nullptr;
   P.outI = wantI ? p->outI : nullptr;
   P.outNS = wantNS ? p->outNS : nullptr;
+  if (p->gv_out_cap && wantGV) {
+    P.gv_row = p->gv_row;
+    P.gv_ent = p->gv_ent;
+    P.gv_st = p->gv_st;
+    P.gv_xt = p->gv_xt;
+  } else {
+    P.gv_row = P.gv_ent = nullptr;
+    P.gv_st = P.gv_xt = nullptr;
+    P.gv_n = 0;
+  }
   P.bar = p->bar;
   P.err = p->err;
   P.spike_total = p->spike_total;
@@ -1900,6 +1943,12 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
     P.in_row = nullptr;
   }
   UPU(block_post, block_post.data(), block_post.size());
+  if (d->compat)
+    for (int r = 0; r < FS_NREC; r++) {
+      const fs_rec_layout &L = d->compat->rec[r];
+      const uint32_t *src = L.rec_src ? L.rec_src : L.rec_pre;
+      if (L.n_recs && src) p->rec_src[r].assign(src, src + L.n_recs);
+    }
   // single-step kernel: FP32, every delay 0, no gap junctions
   if (allow_single && !p->fp64 && dmax == 0 && !gap && S.n > 0 && !(o.flags & FS_RUN_INTERVAL_KERNEL)) {
     Single S1;
@@ -2036,6 +2085,49 @@ int prod_reset(Prod *p, uint32_t seed, cudaStream_t st, std::string &err) {
   return FS_OK;
 }
 
+// Device tables of a GatingVariable selection (out->gv_sel: receptor << 28
+// | record index): per presynaptic neuron, its output columns; output
+// buffers for chunks of up to `steps` steps.
+static int gv_prepare(Prod *p, const fs_step_out *out, uint32_t steps, cudaStream_t st, std::string &err) {
+  const uint32_t n = p->n, k = out->gv_n;
+  std::vector<uint32_t> row(n + 1, 0), ent(k);
+  std::vector<uint32_t> src(k);
+  for (uint32_t i = 0; i < k; i++) {
+    const uint32_t r = out->gv_sel[i] >> 28, e = out->gv_sel[i] & 0x0fffffffu;
+    if (r >= FS_NREC || e >= p->rec_src[r].size() || p->rec_src[r][e] >= n) {
+      err = "GatingVariable selection " + std::to_string(i) + " names no single-target record of the network";
+      return FS_ERR_ARG;
+    }
+    src[i] = p->rec_src[r][e];
+    row[src[i] + 1]++;
+  }
+  for (uint32_t i = 0; i < n; i++) row[i + 1] += row[i];
+  {
+    std::vector<uint32_t> fill(row.begin(), row.end() - 1);
+    for (uint32_t i = 0; i < k; i++) ent[fill[src[i]]++] = i | ((out->gv_sel[i] >> 28) << 28);
+  }
+  int rc;
+  if (!p->gv_row && (rc = dal(p, &p->gv_row, (size_t)n + 1, err))) return rc;
+  if (k > p->gv_ent_cap) {
+    if ((rc = dal(p, &p->gv_ent, k, err))) return rc;
+    p->gv_ent_cap = k;
+  }
+  if ((uint64_t)steps * k > p->gv_out_cap) {
+    if ((rc = dal(p, &p->gv_st, (size_t)steps * k, err)) || (rc = dal(p, &p->gv_xt, (size_t)steps * k, err)))
+      return rc;
+    p->gv_out_cap = (uint64_t)steps * k;
+  }
+  cudaError_t e = cudaMemcpyAsync(p->gv_row, row.data(), (size_t)(n + 1) * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(p->gv_ent, ent.data(), (size_t)k * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("GatingVariable tables: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  p->P.gv_n = k;
+  return FS_OK;
+}
+
 int prod_step(Prod *p, uint32_t nsteps, fs_step_out *out, uint64_t *written, cudaStream_t st, uint64_t *launches,
               uint64_t *spikes_total, std::string &err) {
   const uint32_t n = p->n, words = (n + 31) / 32;
@@ -2045,11 +2137,12 @@ int prod_step(Prod *p, uint32_t nsteps, fs_step_out *out, uint64_t *written, cud
   while (done < nsteps) {
     const uint32_t b = std::min(chunk, nsteps - done);
     const bool wantV = out && out->V, wantI = out && out->Irep, wantNS = out && out->nstate;
-    if (out && out->gv_n) {
-      err = "production modes aggregate the synapse gates: GatingVariable output needs FS_MODE_COMPAT";
-      return FS_ERR_UNSUPPORTED;
+    const bool wantGV = out && out->gv_n && out->gv_sel && out->gv_st;
+    if (wantGV && done == 0) {
+      int grc = gv_prepare(p, out, b, st, err);
+      if (grc) return grc;
     }
-    int rc = launch(p, b, true, wantV, st, launches, err, wantI, wantNS);
+    int rc = launch(p, b, true, wantV, st, launches, err, wantI, wantNS, wantGV);
     if (rc) return rc;
     cudaError_t e = fsd::spikes_compact(p->bits, b, words, p->counts, p->offsets, p->idx, st, launches);
     if (e != cudaSuccess) { err = cudaGetErrorString(e); return FS_ERR_CUDA; }
@@ -2078,6 +2171,14 @@ int prod_step(Prod *p, uint32_t nsteps, fs_step_out *out, uint64_t *written, cud
     }
     if (wantNS) {
       e = cudaMemcpy(out->nstate + (size_t)done * n, p->outNS, (size_t)b * n * 4, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) { err = cudaGetErrorString(e); return FS_ERR_CUDA; }
+    }
+    if (wantGV) {
+      e = cudaMemcpy(out->gv_st + (size_t)done * out->gv_n, p->gv_st, (size_t)b * out->gv_n * 4,
+                     cudaMemcpyDeviceToHost);
+      if (e == cudaSuccess && out->gv_xt)
+        e = cudaMemcpy(out->gv_xt + (size_t)done * out->gv_n, p->gv_xt, (size_t)b * out->gv_n * 4,
+                       cudaMemcpyDeviceToHost);
       if (e != cudaSuccess) { err = cudaGetErrorString(e); return FS_ERR_CUDA; }
     }
     *written += total;

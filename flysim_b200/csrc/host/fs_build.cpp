@@ -368,6 +368,7 @@ void build_network(Model &m) {
       srec_src[r][e] = t[e].src;
       rec_delay[r][e] = t[e].d;
     }
+    ra.rec_src = srec_src[r];
     ra.rec_rowptr.assign(n + 1, 0);
     for (size_t e = 0; e < t.size(); e++) ra.rec_rowptr[t[e].post + 1]++;
     for (uint32_t x = 0; x < n; x++) ra.rec_rowptr[x + 1] += ra.rec_rowptr[x];
@@ -494,6 +495,7 @@ void Network::make_views(float dt, uint32_t act_ctr) {
     L.n_recs = (uint32_t)ra.rec_pre.size();
     L.rec_pre = ra.rec_pre.data(); L.rec_post = ra.rec_post.data(); L.rec_g = ra.rec_g.data();
     L.rec_rowptr = ra.rec_rowptr.data();
+    L.rec_src = ra.rec_src.empty() ? nullptr : ra.rec_src.data();
   }
   compat.gap_rowptr = gap_rowptr.empty() ? nullptr : gap_rowptr.data();
   compat.gap_other = gap_other.data();

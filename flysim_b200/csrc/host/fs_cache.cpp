@@ -26,7 +26,7 @@ namespace fsh {
 namespace {
 
 constexpr char kMagic[8] = {'F', 'S', 'B', '2', 'N', 'E', 'T', '\0'};
-constexpr uint32_t kFormat = 3;  // 3: unseeded models are never stored
+constexpr uint32_t kFormat = 4;  // 3: unseeded models are never stored; 4: record sources
 constexpr uint32_t kSizes = (uint32_t)(sizeof(Receptor) | sizeof(Link) << 8 | sizeof(Event) << 16);
 
 // 64-bit streaming hash for cache keys and the payload check (not a
@@ -210,7 +210,7 @@ template <class A> void visit_model(A &a, Model &m) {
   for (int r = 0; r < FS_NREC; r++) {
     Network::RecArrays &ra = n.rec[r];
     a(ra.gate_pre); a(ra.gate_post0); a(ra.gate_g); a(ra.gather_rowptr); a(ra.gather_gate);
-    a(ra.rec_pre); a(ra.rec_post); a(ra.rec_g); a(ra.rec_rowptr); a(ra.seg_post); a(ra.seg_len);
+    a(ra.rec_pre); a(ra.rec_post); a(ra.rec_g); a(ra.rec_rowptr); a(ra.seg_post); a(ra.seg_len); a(ra.rec_src);
   }
   a(n.gap_rowptr); a(n.gap_other); a(n.gap_g);
   a(n.gap1_pre); a(n.gap1_post); a(n.gap_ngroup); a(n.gap1_g);

@@ -94,6 +94,7 @@ struct Network {
     std::vector<uint32_t> rec_pre, rec_post;
     std::vector<float> rec_g;
     std::vector<uint32_t> rec_rowptr;
+    std::vector<uint32_t> rec_src;  // presynaptic neuron of each record
     // group segments in the reference's order (posts ascending; for GluCl the
     // post read through the Ach map): segment s holds seg_len[s] gather
     // entries of post seg_post[s].  Only network.log reads these.

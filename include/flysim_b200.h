@@ -128,6 +128,9 @@ typedef struct fs_rec_layout {
   const uint32_t *rec_pre, *rec_post;
   const float *rec_g;
   const uint32_t *rec_rowptr;    /* [n+1] records of post i: [rowptr[i], rowptr[i+1]) */
+  /* the presynaptic NEURON of each record (the production modes' gate of a
+   * record is that neuron's); NULL: rec_pre read as a neuron index */
+  const uint32_t *rec_src;
 } fs_rec_layout;
 
 typedef struct fs_compat_layout {
@@ -194,7 +197,11 @@ typedef struct fs_step_out {
   float *Irep;             /* [nsteps*FS_NREC*n] receptor currents (Nets.Irep) */
   uint32_t *nstate;        /* [nsteps*n] NState after the step             */
   /* gating variables of selected single-target records (GatingVariable
-   * output, code/NetSimGnl2_info.cpp:701-758); FS_MODE_COMPAT only */
+   * output, code/NetSimGnl2_info.cpp:701-758).  In the production modes a
+   * record's st is its presynaptic neuron's gate for the receptor (every
+   * record of one neuron and receptor obeys the same recurrence) and an
+   * NMDA record's (xt, st) are that neuron's NMDA x and s; the selection
+   * needs the compat layout of the description (fs_net_desc.compat). */
   const uint32_t *gv_sel;  /* (receptor << 28) | record index in fs_rec_layout order */
   uint32_t gv_n;
   float *gv_st;            /* [nsteps*gv_n] st after the step              */

@@ -357,6 +357,47 @@ def test_single_step_kernel_on_reference_networks(built, case):
     np.testing.assert_array_equal(ca, cb)
 
 
+@pytest.mark.parametrize("mode", ["fp64", "fp32"])
+def test_gating_variables_equal_compat(built, mode):
+    # GatingVariable output in the production modes: a single-target
+    # record's gate is its presynaptic neuron's gate (NMDA: x and s).  On a
+    # deterministic drive (no Poisson input, noiseless injection) the
+    # production modes follow the reference-order compat path spike for spike
+    # and the records' st / xt agree to float rounding
+    from conftest import model_for
+    m = model_for(built, "conn")
+    d = m.desc()
+    lay = d.contents.compat.contents
+    sel = []
+    for r in range(5):
+        L = lay.rec[r]
+        for e in range(L.n_recs):
+            if L.rec_pre[e] in (1, 7, 30):
+                sel.append((r << 28) | e)
+    assert len(sel) > 20 and any(x >> 28 == built.FS_NMDA for x in sel)
+    n = d.contents.neurons.n
+    steps = 2000
+    out = {}
+    for md in ("compat", mode):
+        e = built.Engine(d, md, chunk_steps=700)
+        try:
+            e.reset(m.seed())
+            for r in range(5):
+                e.set_drive(0, n, r, 0.0)
+            e.set_injection(0, n, 0.45, 0.0)
+            out[md] = e.step_gv(steps, sel)
+        finally:
+            e.close()
+    (sa, gs_a, gx_a), (sb, gs_b, gx_b) = out["compat"], out[mode]
+    assert sum(x.size for x in sa) > 100
+    for t in range(steps):
+        np.testing.assert_array_equal(sa[t], sb[t], err_msg="spikes differ at step %d" % t)
+    assert np.abs(gs_a).max() > 0.1 and np.abs(gx_a).max() > 0.1
+    tol = 1e-5 if mode == "fp64" else 1e-4
+    np.testing.assert_allclose(gs_b, gs_a, rtol=tol, atol=tol * np.abs(gs_a).max())
+    np.testing.assert_allclose(gx_b, gx_a, rtol=tol, atol=tol * np.abs(gx_a).max())
+
+
 def test_checkpoint_refused_after_a_wait_gave_up(built):
     # the failure is made on the host: the handle's device error word is set
     # as a bounded wait that gave up sets it (no kernel is stopped or hung);
