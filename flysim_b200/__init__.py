@@ -26,7 +26,7 @@ FS_OK, FS_ERR_ARG, FS_ERR_CUDA, FS_ERR_NOMEM, FS_ERR_CAPACITY, FS_ERR_PARSE, FS_
     FS_ERR_TIMEOUT, FS_ERR_IO, FS_ERR_NODEVICE = range(10)
 FS_AMPA, FS_GABA, FS_ACH, FS_GCL, FS_NMDA, FS_NREC = 0, 1, 2, 3, 4, 5
 FS_MODE_COMPAT, FS_MODE_FP32, FS_MODE_FP64 = 0, 1, 2
-FS_RUN_INTERVAL_KERNEL = 1
+FS_RUN_INTERVAL_KERNEL, FS_RUN_TILE_KERNELS = 1, 2
 MODES = {"compat": FS_MODE_COMPAT, "fp32": FS_MODE_FP32, "fp64": FS_MODE_FP64}
 ACT = dict(AMPA=1, GABA=2, NMDA=4, GAP=8, ACH=32, GCL=64, INJ=128, LIF=256, LTP=8192, STD=16384, STP=32768)
 NS_FIRE, NS_SPIKE = 1, 2
@@ -97,7 +97,7 @@ class ModelOpts(C.Structure):
 
 class BatchPlan(C.Structure):
     _fields_ = [("blocks", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("candidates", C.c_uint32),
-                ("cost_update", C.c_float), ("sample_ms", C.c_double)]
+                ("tile_posts", C.c_uint32), ("edges_in_flight", C.c_uint32), ("sample_ms", C.c_double)]
 
 
 class EngineVtbl(C.Structure):
@@ -330,11 +330,11 @@ class Engine:
     """One network instance on one GPU (fs_create ... fs_destroy)."""
 
     def __init__(self, desc, mode: str = "compat", device: int = 0, chunk_steps: int = 0, philox_key: int = 0,
-                 blocks_per_sm: int = 0, interval_kernel: bool = False):
+                 blocks_per_sm: int = 0, interval_kernel: bool = False, tile_kernels: bool = False):
         L = lib()
         self._keep = getattr(desc, "_keep", None)
         o = RunOpts(MODES[mode], device, chunk_steps, philox_key, blocks_per_sm,
-                    FS_RUN_INTERVAL_KERNEL if interval_kernel else 0)
+                    (FS_RUN_INTERVAL_KERNEL if interval_kernel else 0) | (FS_RUN_TILE_KERNELS if tile_kernels else 0))
         h = C.c_void_p()
         dp = desc if isinstance(desc, C._Pointer) else C.pointer(desc)
         rc = L.fs_create(dp, C.byref(o), C.byref(h))
@@ -455,10 +455,13 @@ class Engine:
 
     def layout(self):
         """Launch layout (production modes): blocks, threads, interval and
-        whether the single-step kernel runs the network."""
-        b, t, i, sgl = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_int()
-        _check(lib().fs_engine_layout(self._h, C.byref(b), C.byref(t), C.byref(i), C.byref(sgl)), self._h)
-        return dict(blocks=b.value, threads=t.value, interval=i.value, single_step=bool(sgl.value))
+        the kernels that run the network ("interval", "single_step" or
+        "tiles")."""
+        b, t, i, k = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_int()
+        _check(lib().fs_engine_layout(self._h, C.byref(b), C.byref(t), C.byref(i), C.byref(k)), self._h)
+        kind = {0: "interval", 1: "single_step", 2: "tiles"}[k.value]
+        return dict(blocks=b.value, threads=t.value, interval=i.value, kernel=kind,
+                    single_step=kind == "single_step")
 
     def kernel_time(self):
         ms, n = C.c_double(), C.c_uint64()
@@ -586,7 +589,7 @@ class Batch:
         p = BatchPlan()
         self._ok(lib().fs_batch_tune(self._h, sample_steps, C.byref(p)))
         return dict(blocks=p.blocks, blocks_per_sm=p.blocks_per_sm, candidates=p.candidates,
-                    cost_update=p.cost_update, sample_ms=p.sample_ms)
+                    tile_posts=p.tile_posts, edges_in_flight=p.edges_in_flight, sample_ms=p.sample_ms)
 
     def run(self, nsteps: int) -> float:
         ms = C.c_double()

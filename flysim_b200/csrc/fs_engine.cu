@@ -660,7 +660,7 @@ int fs_debug_barrier_timeout(uint32_t poll_limit) {
   return FS_OK;
 }
 
-int fs_engine_layout(fs_handle *h, uint32_t *blocks, uint32_t *threads, uint32_t *interval, int *single_step) {
+int fs_engine_layout(fs_handle *h, uint32_t *blocks, uint32_t *threads, uint32_t *interval, int *kernel) {
   if (!h) return set_err(nullptr, FS_ERR_ARG, "null handle");
   if (h->mode == FS_MODE_COMPAT || !h->prod)
     return set_err(h, FS_ERR_UNSUPPORTED, "fs_engine_layout: production modes only");
@@ -669,7 +669,7 @@ int fs_engine_layout(fs_handle *h, uint32_t *blocks, uint32_t *threads, uint32_t
   if (blocks) *blocks = pi.blocks;
   if (threads) *threads = pi.threads;
   if (interval) *interval = pi.interval;
-  if (single_step) *single_step = pi.single_step;
+  if (kernel) *kernel = pi.single_step ? 1 : pi.tiles ? 2 : 0;
   return FS_OK;
 }
 
@@ -1045,7 +1045,8 @@ int fs_batch_tune(fs_batch *b, uint32_t sample_steps, fs_batch_plan *plan) {
     plan->blocks = p.blocks;
     plan->blocks_per_sm = p.blocks_per_sm;
     plan->candidates = p.candidates;
-    plan->cost_update = (float)p.cost_update;
+    plan->tile_posts = p.tile_posts;
+    plan->edges_in_flight = p.edges_in_flight;
     plan->sample_ms = p.sample_ms;
   }
   return FS_OK;

@@ -121,6 +121,7 @@ struct Params {
   uint32_t t1_ncls, t1_smem;
   // GatingVariable output (or null): selections of neuron p are entries
   // [gv_row[p], gv_row[p+1]) of gv_ent (output column | receptor << 28)
+  void *gn_buf;          // tile kernels: NMDA sums of a batch of steps, [L][n]
   const uint32_t *gv_row, *gv_ent;
   uint32_t gv_n;
   float *gv_st, *gv_xt;  // [steps][gv_n]
@@ -861,26 +862,94 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
   }
 }
 
+// Shared-memory buffers of one tile (the posts a block advances together).
+template <class T>
+struct TileBufs {
+  static constexpr uint32_t kT = TileW<T>::W;
+  static constexpr uint32_t kCap = sizeof(T) == 4 ? 448 : 192;
+  T gn[kLB][kT];
+  T gauss[kLB][kT];
+  T gapI[kT];
+  uint8_t hits[kLB][kT];
+  uint32_t l_n, l_p[kCap];
+  uint16_t l_tm[kCap];
+  T l_c[kCap][4];
+};
+
+// NMDA sums of L steps for a tile's posts into B.gn.
+template <class T, int PU>
+__device__ __forceinline__ void tile_pull(const Params &P, uint32_t tp0, uint32_t np, uint32_t bs, uint32_t L,
+                                          TileBufs<T> &B) {
+  const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if constexpr (sizeof(T) == 4) {
+    if (P.dmax0) nmda_pull1_f32(P, tp0, np, P.t0 + bs, (float (*)[kTile])B.gn, wid, lane);
+    else nmda_pull_f32<PU>(P, tp0, np, P.t0 + bs, L, (float (*)[kTile])B.gn, wid, lane);
+  } else {
+    nmda_pull<T>(P, tp0, np, P.t0 + bs, L, B.gn, wid, lane);
+  }
+}
+
+// The rest of a tile's batch of L steps once its NMDA sums are in B.gn: the
+// drive draws, gap currents, the neurons' steps and the spikes' pushes.
+template <class T, int PD>
+__device__ __forceinline__ void tile_steps(const Params &P, uint32_t tp0, uint32_t np, uint32_t bs, uint32_t L,
+                                           TileBufs<T> &B) {
+  constexpr uint32_t kCap = TileBufs<T>::kCap;
+  const SpikeList<T> lst{&B.l_n, B.l_p, B.l_tm, B.l_c, kCap};
+  const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  draw_inputs<T>(P, tp0, np, P.t0 + bs, L, B.hits, B.gauss);
+  if (P.gap_row) {
+    // gap currents of this step (interval 1): g (V_other - V_self) over
+    // V at the end of the previous step (none before the first step)
+    const uint64_t t = P.t0 + bs;
+    for (uint32_t q = tid; q < np; q += kThreads) {
+      T acc = (T)0;
+      if (t > 0) {
+        const T *vp = (const T *)P.Vg + (size_t)((t - 1u) & 1u) * P.n;
+        const uint32_t pq = tp0 + q;
+        const T vs = __ldcg(vp + pq);
+        for (uint32_t e = __ldg(P.gap_row + pq), e1 = __ldg(P.gap_row + pq + 1); e < e1; e++)
+          acc = acc + (T)__ldg(P.gap_w + e) * (__ldcg(vp + __ldg(P.gap_other + e)) - vs);
+      }
+      B.gapI[q] = acc;
+    }
+  }
+  __syncthreads();
+  // warps without neurons in this tile skip the steps
+  if ((tid & ~31u) < np) neuron_steps<T, PD>(P, tp0, np, bs, L, B.gn, B.hits, B.gauss, lst, B.gapI);
+  __syncthreads();
+  // the batch's spikes: with fewer spikes than warps the whole block
+  // walks each spike's out-edges (a hub's hundreds of edges in one or
+  // two rounds); with more, one spike per warp, eight in flight
+  const uint32_t nl = min(B.l_n, kCap);
+  if (nl < kThreads / 32) {
+    for (uint32_t k = 0; k < nl; k++) {
+      T cj[4];
+#pragma unroll
+      for (int r = 0; r < 4; r++) cj[r] = B.l_c[k][r];
+      push_spike<T>(P, B.l_p[k], B.l_tm[k], cj, tid, kThreads);
+    }
+  } else {
+    for (uint32_t k = wid; k < nl; k += kThreads / 32) {
+      T cj[4];
+#pragma unroll
+      for (int r = 0; r < 4; r++) cj[r] = B.l_c[k][r];
+      push_spike<T>(P, B.l_p[k], B.l_tm[k], cj, lane, 32);
+    }
+  }
+  __syncthreads();
+  if (tid == 0) B.l_n = 0;
+}
+
 // The steps of one block: posts [B0, B1) of the network P, whose blocks
 // (nblk of them) meet at a barrier after every interval.  PU: NMDA edges in
 // flight per lane in the pull; PD: ring slots in flight per neuron in the
 // steps (results depend on neither).
 template <class T, int PU, int PD>
 __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32_t B1, uint32_t nblk) {
-  // FP64 tiles are half as wide so the per-tile buffers stay in static
-  // shared memory
   constexpr uint32_t kT = TileW<T>::W;
-  constexpr uint32_t kCap = sizeof(T) == 4 ? 448 : 192;
-  __shared__ T gn[kLB][kT];
-  __shared__ T gauss[kLB][kT];
-  __shared__ T gapI[kT];
-  __shared__ uint8_t hits[kLB][kT];
-  __shared__ uint32_t l_n, l_p[kCap];
-  __shared__ uint16_t l_tm[kCap];
-  __shared__ T l_c[kCap][4];
-  const SpikeList<T> lst{&l_n, l_p, l_tm, l_c, kCap};
-  const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  if (tid == 0) l_n = 0;
+  __shared__ TileBufs<T> B;
+  if (threadIdx.x == 0) B.l_n = 0;
   __syncthreads();
   uint32_t s = 0;
   while (s < P.nsteps) {
@@ -889,53 +958,8 @@ __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32
       const uint32_t L = min(kLB, iv_end - bs);
       for (uint32_t tp0 = B0; tp0 < B1; tp0 += kT) {
         const uint32_t np = min(kT, B1 - tp0);
-        if constexpr (sizeof(T) == 4) {
-          if (P.dmax0) nmda_pull1_f32(P, tp0, np, P.t0 + bs, (float (*)[kTile])gn, wid, lane);
-          else nmda_pull_f32<PU>(P, tp0, np, P.t0 + bs, L, (float (*)[kTile])gn, wid, lane);
-        }
-        else nmda_pull<T>(P, tp0, np, P.t0 + bs, L, gn, wid, lane);
-        draw_inputs<T>(P, tp0, np, P.t0 + bs, L, hits, gauss);
-        if (P.gap_row) {
-          // gap currents of this step (interval 1): g (V_other - V_self) over
-          // V at the end of the previous step (none before the first step)
-          const uint64_t t = P.t0 + bs;
-          for (uint32_t q = tid; q < np; q += kThreads) {
-            T acc = (T)0;
-            if (t > 0) {
-              const T *vp = (const T *)P.Vg + (size_t)((t - 1u) & 1u) * P.n;
-              const uint32_t pq = tp0 + q;
-              const T vs = __ldcg(vp + pq);
-              for (uint32_t e = __ldg(P.gap_row + pq), e1 = __ldg(P.gap_row + pq + 1); e < e1; e++)
-                acc = acc + (T)__ldg(P.gap_w + e) * (__ldcg(vp + __ldg(P.gap_other + e)) - vs);
-            }
-            gapI[q] = acc;
-          }
-        }
-        __syncthreads();
-        // warps without neurons in this tile skip the steps
-        if ((tid & ~31u) < np) neuron_steps<T, PD>(P, tp0, np, bs, L, gn, hits, gauss, lst, gapI);
-        __syncthreads();
-        // the batch's spikes: with fewer spikes than warps the whole block
-        // walks each spike's out-edges (a hub's hundreds of edges in one or
-        // two rounds); with more, one spike per warp, eight in flight
-        const uint32_t nl = min(l_n, kCap);
-        if (nl < kThreads / 32) {
-          for (uint32_t k = 0; k < nl; k++) {
-            T cj[4];
-#pragma unroll
-            for (int r = 0; r < 4; r++) cj[r] = l_c[k][r];
-            push_spike<T>(P, l_p[k], l_tm[k], cj, tid, kThreads);
-          }
-        } else {
-          for (uint32_t k = wid; k < nl; k += kThreads / 32) {
-            T cj[4];
-#pragma unroll
-            for (int r = 0; r < 4; r++) cj[r] = l_c[k][r];
-            push_spike<T>(P, l_p[k], l_tm[k], cj, lane, 32);
-          }
-        }
-        __syncthreads();
-        if (tid == 0) l_n = 0;
+        tile_pull<T, PU>(P, tp0, np, bs, L, B);
+        tile_steps<T, PD>(P, tp0, np, bs, L, B);
       }
     }
     s = iv_end;
@@ -1222,38 +1246,78 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
   }
 }
 
-// ---- batch: many independent networks in one persistent launch -----------
-// Block b works on instance blk[b].inst, posts [b0, b1), and meets only the
-// other blocks of that instance (blk[b].nblk of them) at its barriers, so
-// instances of different sizes and intervals advance independently.
-struct BatchBlock {
-  uint32_t inst, b0, b1, nblk;
+// ---- tile kernels: networks too large for one persistent launch, batches --
+// A launch pair advances every tile (up to TileW posts of one network) by a
+// batch of L steps: k_tile_pull writes the tiles' NMDA sums of the batch to
+// gn_buf, k_tile_step draws the drive, runs the neurons' steps and pushes
+// the spikes.  The kernel boundary is the barrier between batches, so
+// blocks are scheduled freely over the tiles of all networks (no block
+// waits for another), the pull runs at the occupancy its registers allow,
+// and L never exceeds the smallest interval of the networks (every value a
+// batch reads was final before it began).  A chunk of steps is one CUDA
+// graph of these pairs.  Per post the arithmetic and the order of every sum
+// are those of the persistent kernel, so the results are identical.
+struct IvTile {
+  uint32_t inst, p0, np, pad;
 };
 
-template <class T>
-__global__ void __launch_bounds__(kThreads) k_prod_batch(const Params *__restrict__ Ps,
-                                                         const BatchBlock *__restrict__ blk) {
+__device__ __forceinline__ void params_to_smem(Params &Psh, const Params *__restrict__ Ps, uint32_t inst) {
+  const uint32_t *src = (const uint32_t *)(Ps + inst);
+  uint32_t *dst = (uint32_t *)&Psh;
+  for (uint32_t i = threadIdx.x; i < sizeof(Params) / 4; i += blockDim.x) dst[i] = src[i];
+}
+
+template <class T, int U>
+__global__ void __launch_bounds__(kThreads, 3) k_tile_pull(const Params *__restrict__ Ps,
+                                                          const IvTile *__restrict__ tiles, uint32_t bs,
+                                                          uint32_t L) {
   __shared__ __align__(16) Params Psh;
-  const BatchBlock me = blk[blockIdx.x];
-  {
-    const uint32_t *src = (const uint32_t *)(Ps + me.inst);
-    uint32_t *dst = (uint32_t *)&Psh;
-    for (uint32_t i = threadIdx.x; i < sizeof(Params) / 4; i += blockDim.x) dst[i] = src[i];
+  __shared__ T gn[kLB][TileW<T>::W];
+  const IvTile tl = tiles[blockIdx.x];
+  params_to_smem(Psh, Ps, tl.inst);
+  __syncthreads();
+  const Params &P = Psh;
+  const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if constexpr (sizeof(T) == 4) {
+    if (P.dmax0) nmda_pull1_f32(P, tl.p0, tl.np, P.t0 + bs, (float (*)[kTile])gn, wid, lane);
+    else nmda_pull_f32<U>(P, tl.p0, tl.np, P.t0 + bs, L, (float (*)[kTile])gn, wid, lane);
+  } else {
+    nmda_pull<T>(P, tl.p0, tl.np, P.t0 + bs, L, gn, wid, lane);
   }
   __syncthreads();
-  prod_blocks<T, 8, 1>(Psh, me.b0, me.b1, me.nblk);
+  T *out = (T *)P.gn_buf;
+  for (uint32_t i = tid; i < tl.np * L; i += kThreads) {
+    const uint32_t j = i / tl.np, q = i - j * tl.np;
+    out[(size_t)j * P.n + tl.p0 + q] = gn[j][q];
+  }
 }
 
-// Advances every instance's step counter after a batch launch (graph node).
-__global__ void k_batch_advance(Params *Ps, uint32_t count, uint32_t nsteps) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < count) Ps[i].t0 += nsteps;
+template <class T, int PD>
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) k_tile_step(const Params *__restrict__ Ps,
+                                                                              const IvTile *__restrict__ tiles,
+                                                                              uint32_t bs, uint32_t L) {
+  __shared__ __align__(16) Params Psh;
+  __shared__ TileBufs<T> B;
+  const IvTile tl = tiles[blockIdx.x];
+  params_to_smem(Psh, Ps, tl.inst);
+  if (threadIdx.x == 0) B.l_n = 0;
+  __syncthreads();
+  const Params &P = Psh;
+  const T *in = (const T *)P.gn_buf;
+  for (uint32_t i = threadIdx.x; i < tl.np * L; i += kThreads) {
+    const uint32_t j = i / tl.np, q = i - j * tl.np;
+    B.gn[j][q] = in[(size_t)j * P.n + tl.p0 + q];
+  }
+  tile_steps<T, PD>(P, tl.p0, tl.np, bs, L, B);  // its first barrier orders the loads above
 }
+
 
 // ---- host side -------------------------------------------------------------
+struct Tiles;
 struct Prod {
   bool fp64 = false;
   bool single = false;     // runs on the single-step kernel k_prod1
+  struct Tiles *tiles = nullptr;  // runs on the tile kernels (large networks)
   uint32_t b1_blocks = 0;  // its blocks (one per SM at most)
   bool wide = false;  // some block's posts span several tiles: eight NMDA edges in flight
   uint32_t n = 0, sm = 148;
@@ -1344,6 +1408,16 @@ int ensure_buffers(Prod *p, uint32_t steps, bool wantV, bool wantI, bool wantNS,
   return FS_OK;
 }
 
+}  // namespace
+
+// tile runner of a single network (defined with the tile runner below)
+int tiles_solo_launch(Prod *p, const Params &P, uint32_t nsteps, cudaStream_t st, uint64_t *kernels,
+                      std::string &err);
+void tiles_delete(Tiles *T);
+int tiles_solo_create(Prod *p, std::string &err);
+
+namespace {
+
 int launch(Prod *p, uint32_t nsteps, bool want_bits, bool wantV, cudaStream_t st, uint64_t *launches,
            std::string &err, bool wantI = false, bool wantNS = false, bool wantGV = false) {
   int rc = ensure_buffers(p, nsteps, wantV, wantI, wantNS, err);
@@ -1394,6 +1468,16 @@ int launch(Prod *p, uint32_t nsteps, bool want_bits, bool wantV, cudaStream_t st
   }
   const auto &evp = p->ev[p->ev_used];
   cudaEventRecord(evp.first, st);
+  if (p->tiles) {
+    uint64_t k = 0;
+    int trc = tiles_solo_launch(p, P, nsteps, st, &k, err);
+    cudaEventRecord(evp.second, st);
+    if (trc) return trc;
+    p->ev_used++;
+    p->t += nsteps;
+    if (launches) *launches += k;
+    return FS_OK;
+  }
   if (p->single) {
     e = cudaLaunchCooperativeKernel((const void *)k_prod1, p->b1_blocks, kT1, args, P.t1_smem, st);
   } else {
@@ -1990,6 +2074,12 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
       cudaGetLastError();
     }
   }
+  // tile kernels: networks whose blocks would each walk more than two tiles
+  // of posts per batch (at 2 blocks per SM: above ~150,000 neurons)
+  if (allow_single && !p->single && !(o.flags & FS_RUN_INTERVAL_KERNEL) &&
+      ((o.flags & FS_RUN_TILE_KERNELS) || (uint64_t)n > (uint64_t)p->blocks * 2 * (p->fp64 ? TileW<double>::W : kTile))) {
+    if ((rc = tiles_solo_create(p, err))) goto fail;
+  }
   if (gap) {
     const uint32_t ng = d->compat->gap_rowptr[n];
     UPU(gap_row, d->compat->gap_rowptr, (size_t)n + 1);
@@ -2018,6 +2108,7 @@ fail:
 
 void prod_destroy(Prod *p) {
   if (!p) return;
+  if (p->tiles) tiles_delete(p->tiles);
   for (void *q : p->allocs) cudaFree(q);
   for (auto &x : p->ev) {
     cudaEventDestroy(x.first);
@@ -2247,6 +2338,7 @@ void prod_info(const Prod *p, ProdInfo *info) {
   info->blocks = p->single ? p->b1_blocks : p->blocks;
   info->threads = p->single ? kT1 : kThreads;
   info->single_step = p->single ? 1 : 0;
+  info->tiles = p->tiles ? 1 : 0;
   info->chunks = p->chunks;
   info->lin_edges = p->lin_edges;
   info->nmda_edges = p->nmda_edges;
@@ -2265,28 +2357,22 @@ int prod_spike_counts(Prod *p, uint32_t *counts, cudaStream_t st, std::string &e
   return FS_OK;
 }
 
-// ---- batch of independent networks ------------------------------------------
-struct Batch {
+// ---- tile runner (batches; single networks too large for one launch) ---------
+// Device tile plan and parameter array over one or more production
+// networks, and the CUDA graph of a chunk of steps.
+struct Tiles {
   bool fp64 = false;
-  uint32_t sm = 148, occ = 1;
-  std::vector<Prod *> inst;
-  std::vector<uint32_t> seeds;
-  Params *dP = nullptr;          // [count] parameters as the kernel reads them
-  BatchBlock *dB = nullptr;      // [blocks]
-  uint32_t dB_cap = 0;
-  unsigned int *bars = nullptr;  // [count][64]
-  int *errs = nullptr;           // [count]
-  uint32_t blocks = 0, per_sm = 0;
-  double upd = 24.0;
-  uint32_t chunk = 10000;
-  uint32_t dev_nsteps = 0;       // nsteps the device parameter array holds (0: stale)
+  uint32_t count = 0;
+  Params *dP = nullptr;        // [count] parameters as the kernels read them
+  IvTile *dT = nullptr;        // [ntiles]
+  uint32_t ntiles = 0, dT_cap = 0;
+  uint32_t tile_w = kTile;     // posts per tile
+  int U = 8;                   // NMDA edges in flight per lane in the pull
+  uint32_t Lmax = 1;           // steps per launch pair
+  uint32_t dev_nsteps = 0;     // nsteps the device parameters hold (0: stale)
   cudaGraphExec_t exec = nullptr;
   uint32_t graph_steps = 0;
-  bool graph_ok = true;          // capture works for this launch
-  bool graph_used = false;
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  double ms = 0.0;
-  uint64_t launches = 0;
+  bool graph_ok = true, graph_used = false;
 };
 
 namespace {
@@ -2296,82 +2382,152 @@ cudaError_t bal(X **p, size_t count) {
   return cudaMalloc((void **)p, count * sizeof(X));
 }
 
-// cost-balanced split of an instance's posts into k contiguous ranges
-void split_posts(const Prod *p, uint32_t k, double upd, std::vector<uint32_t> &bp) {
-  const uint32_t n = p->n;
-  bp.assign(k + 1, n);
-  bp[0] = 0;
-  const std::vector<uint32_t> &in = p->in_row_h;
-  const double total = (double)p->nmda_edges + upd * n;
-  double acc = 0;
-  uint32_t b = 1;
-  for (uint32_t q = 0; q < n && b < k; q++) {
-    acc += upd + (double)(in[q + 1] - in[q]);
-    while (b < k && acc >= total * b / k) bp[b++] = q + 1;
-  }
-  for (; b < k; b++) bp[b] = n;
+void tiles_free(Tiles &T) {
+  if (T.exec) cudaGraphExecDestroy(T.exec);
+  if (T.dP) cudaFree(T.dP);
+  if (T.dT) cudaFree(T.dT);
+  T = Tiles();
 }
 
-int batch_plan(Batch *B, uint32_t per_sm, double upd, std::string &err) {
-  const uint32_t count = (uint32_t)B->inst.size();
-  const uint32_t total = B->sm * per_sm;
-  if (count > total) {
-    err = "batch of " + std::to_string(count) + " instances exceeds the " + std::to_string(total) +
-          " co-resident blocks of one launch";
-    return FS_ERR_CAPACITY;
+// Tiles of tile_w posts, network by network (a network's tiles run
+// together and share its s history in L2).
+int tiles_plan(Tiles &T, const std::vector<Prod *> &inst, uint32_t tile_w, int U, std::string &err) {
+  const uint32_t W = T.fp64 ? TileW<double>::W : TileW<float>::W;
+  tile_w = std::max<uint32_t>(32, std::min(tile_w, W));
+  std::vector<IvTile> plan;
+  uint32_t L = kLB;
+  for (uint32_t i = 0; i < inst.size(); i++) {
+    for (uint32_t p0 = 0; p0 < inst[i]->n; p0 += tile_w)
+      plan.push_back(IvTile{i, p0, std::min(tile_w, inst[i]->n - p0), 0});
+    L = std::min(L, inst[i]->P.interval);
   }
-  std::vector<double> c(count);
-  double sum = 0;
-  for (uint32_t i = 0; i < count; i++) sum += (c[i] = upd * B->inst[i]->n + (double)B->inst[i]->nmda_edges);
-  // one block each, the rest by cost (largest remainder), at most n/8 blocks
-  std::vector<uint32_t> k(count, 1);
-  std::vector<std::pair<double, uint32_t>> rem;
-  uint32_t used = count;
-  for (uint32_t i = 0; i < count; i++) {
-    const double want = (double)(total - count) * c[i] / sum;
-    const uint32_t cap = std::max<uint32_t>(1, (B->inst[i]->n + 7) / 8);
-    const uint32_t add = std::min<uint32_t>((uint32_t)want, cap - 1);
-    k[i] += add;
-    used += add;
-    rem.push_back({want - (double)add, i});
-  }
-  std::sort(rem.begin(), rem.end(), [](const std::pair<double, uint32_t> &a, const std::pair<double, uint32_t> &b) {
-    return a.first > b.first || (a.first == b.first && a.second < b.second);
-  });
-  for (size_t r = 0; r < rem.size() && used < total; r++) {
-    const uint32_t i = rem[r].second;
-    if (k[i] < std::max<uint32_t>(1, (B->inst[i]->n + 7) / 8)) { k[i]++; used++; }
-  }
-  std::vector<BatchBlock> plan;
-  std::vector<uint32_t> bp;
-  for (uint32_t i = 0; i < count; i++) {
-    split_posts(B->inst[i], k[i], upd, bp);
-    for (uint32_t j = 0; j < k[i]; j++) plan.push_back(BatchBlock{i, bp[j], bp[j + 1], k[i]});
-  }
-  if (plan.size() > B->dB_cap) {
-    if (B->dB) cudaFree(B->dB);
-    B->dB = nullptr;
-    B->dB_cap = 0;
-    cudaError_t e = bal(&B->dB, plan.size());
+  if (plan.size() > T.dT_cap) {
+    if (T.dT) cudaFree(T.dT);
+    T.dT = nullptr;
+    T.dT_cap = 0;
+    cudaError_t e = bal(&T.dT, plan.size());
     if (e != cudaSuccess) {
       err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
       return FS_ERR_NOMEM;
     }
-    B->dB_cap = (uint32_t)plan.size();
+    T.dT_cap = (uint32_t)plan.size();
   }
-  cudaError_t e = cudaMemcpy(B->dB, plan.data(), plan.size() * sizeof(BatchBlock), cudaMemcpyHostToDevice);
+  cudaError_t e = cudaMemcpy(T.dT, plan.data(), plan.size() * sizeof(IvTile), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
-    err = std::string("plan upload: ") + cudaGetErrorString(e);
+    err = std::string("tile plan upload: ") + cudaGetErrorString(e);
     return FS_ERR_CUDA;
   }
-  B->blocks = (uint32_t)plan.size();
-  B->per_sm = per_sm;
-  B->upd = upd;
-  if (B->exec) cudaGraphExecDestroy(B->exec);
-  B->exec = nullptr;
-  B->graph_steps = 0;
+  T.ntiles = (uint32_t)plan.size();
+  T.tile_w = tile_w;
+  T.U = U;
+  T.Lmax = std::max<uint32_t>(1, L);
+  if (T.exec) cudaGraphExecDestroy(T.exec);
+  T.exec = nullptr;
+  T.graph_steps = 0;
   return FS_OK;
 }
+
+int tiles_upload(Tiles &T, const Params *hp, uint32_t count, uint32_t nsteps, cudaStream_t st, std::string &err) {
+  if (!T.dP || count != T.count) {
+    if (T.dP) cudaFree(T.dP);
+    T.dP = nullptr;
+    cudaError_t e = bal(&T.dP, count);
+    if (e != cudaSuccess) {
+      err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+      return FS_ERR_NOMEM;
+    }
+    T.count = count;
+  }
+  cudaError_t e = cudaMemcpyAsync(T.dP, hp, count * sizeof(Params), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("parameter upload: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  T.dev_nsteps = nsteps;
+  return FS_OK;
+}
+
+// Advances every instance's step counter after a chunk (graph node).
+__global__ void k_tiles_advance(Params *Ps, uint32_t count, uint32_t nsteps) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < count) Ps[i].t0 += nsteps;
+}
+
+cudaError_t tiles_enqueue(const Tiles &T, uint32_t nsteps, cudaStream_t st) {
+  for (uint32_t bs = 0; bs < nsteps; bs += T.Lmax) {
+    const uint32_t L = std::min(T.Lmax, nsteps - bs);
+    if (T.fp64) {
+      k_tile_pull<double, 4><<<T.ntiles, kThreads, 0, st>>>(T.dP, T.dT, bs, L);
+      k_tile_step<double, 1><<<T.ntiles, kThreads, 0, st>>>(T.dP, T.dT, bs, L);
+    } else {
+      if (T.U == 4) k_tile_pull<float, 4><<<T.ntiles, kThreads, 0, st>>>(T.dP, T.dT, bs, L);
+      else k_tile_pull<float, 8><<<T.ntiles, kThreads, 0, st>>>(T.dP, T.dT, bs, L);
+      k_tile_step<float, 2><<<T.ntiles, kThreads, 0, st>>>(T.dP, T.dT, bs, L);
+    }
+  }
+  k_tiles_advance<<<(T.count + 255) / 256, 256, 0, st>>>(T.dP, T.count, nsteps);
+  return cudaGetLastError();
+}
+
+// kernels of one chunk
+uint64_t tiles_kernels(const Tiles &T, uint32_t nsteps) { return 2ull * ((nsteps + T.Lmax - 1) / T.Lmax) + 1; }
+
+// One chunk of nsteps: a replay of the captured graph when one exists for
+// this step count, else a direct launch.
+int tiles_launch(Tiles &T, uint32_t nsteps, cudaStream_t st, std::string &err) {
+  cudaError_t e = cudaSuccess;
+  if (T.graph_ok && T.graph_steps != nsteps) {
+    if (T.exec) cudaGraphExecDestroy(T.exec);
+    T.exec = nullptr;
+    T.graph_steps = 0;
+    cudaGraph_t g = nullptr;
+    e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      cudaError_t le = tiles_enqueue(T, nsteps, st);
+      e = cudaStreamEndCapture(st, &g);
+      if (le != cudaSuccess) e = le;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&T.exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e == cudaSuccess) {
+      T.graph_steps = nsteps;
+    } else {
+      cudaGetLastError();
+      T.graph_ok = false;
+      if (T.exec) cudaGraphExecDestroy(T.exec);
+      T.exec = nullptr;
+    }
+  }
+  if (T.exec && T.graph_steps == nsteps) {
+    e = cudaGraphLaunch(T.exec, st);
+    T.graph_used = true;
+  } else {
+    e = tiles_enqueue(T, nsteps, st);
+  }
+  if (e != cudaSuccess) {
+    err = std::string("tile launch: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  return FS_OK;
+}
+
+}  // namespace
+
+// ---- batch of independent networks ------------------------------------------
+struct Batch {
+  bool fp64 = false;
+  uint32_t sm = 148;
+  std::vector<Prod *> inst;
+  std::vector<uint32_t> seeds;
+  Tiles T;
+  uint32_t chunk = 10000;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  double ms = 0.0;
+  uint64_t launches = 0;
+};
+
+namespace {
 
 int batch_upload(Batch *B, uint32_t nsteps, cudaStream_t st, std::string &err) {
   const uint32_t count = (uint32_t)B->inst.size();
@@ -2383,72 +2539,22 @@ int batch_upload(Batch *B, uint32_t nsteps, cudaStream_t st, std::string &err) {
     P.bits = nullptr;
     P.counts = nullptr;
     P.outV = nullptr;
-    P.bar = B->bars + 64 * (size_t)i;
-    P.err = B->errs + i;
+    P.outI = nullptr;
+    P.outNS = nullptr;
+    P.gv_row = P.gv_ent = nullptr;
+    P.gv_st = P.gv_xt = nullptr;
     P.spike_total = B->inst[i]->spike_total;
     hp[i] = P;
   }
-  cudaError_t e = cudaMemcpyAsync(B->dP, hp.data(), count * sizeof(Params), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) {
-    err = std::string("batch parameter upload: ") + cudaGetErrorString(e);
-    return FS_ERR_CUDA;
-  }
-  B->dev_nsteps = nsteps;
-  return FS_OK;
+  return tiles_upload(B->T, hp.data(), count, nsteps, st, err);
 }
 
-cudaError_t batch_enqueue(Batch *B, uint32_t nsteps, cudaStream_t st) {
-  void *args[] = {&B->dP, &B->dB};
-  cudaError_t e = B->fp64 ? cudaLaunchCooperativeKernel((void *)k_prod_batch<double>, B->blocks, kThreads, args, 0, st)
-                          : cudaLaunchCooperativeKernel((void *)k_prod_batch<float>, B->blocks, kThreads, args, 0, st);
-  if (e != cudaSuccess) return e;
-  const uint32_t count = (uint32_t)B->inst.size();
-  k_batch_advance<<<(count + 255) / 256, 256, 0, st>>>(B->dP, count, nsteps);
-  return cudaGetLastError();
-}
-
-// one launch of nsteps for every instance: a replay of the captured graph
-// when one exists for this step count, else a direct launch
 int batch_launch(Batch *B, uint32_t nsteps, cudaStream_t st, std::string &err) {
   int rc;
-  if (B->dev_nsteps != nsteps && (rc = batch_upload(B, nsteps, st, err))) return rc;
-  cudaError_t e = cudaSuccess;
-  if (B->graph_ok && B->graph_steps != nsteps) {
-    if (B->exec) cudaGraphExecDestroy(B->exec);
-    B->exec = nullptr;
-    B->graph_steps = 0;
-    cudaGraph_t g = nullptr;
-    e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
-      cudaError_t le = batch_enqueue(B, nsteps, st);
-      e = cudaStreamEndCapture(st, &g);
-      if (le != cudaSuccess) e = le;
-    }
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&B->exec, g, 0);
-    if (g) cudaGraphDestroy(g);
-    if (e == cudaSuccess) {
-      B->graph_steps = nsteps;
-    } else {
-      // this launch form cannot be captured here: launch it directly
-      cudaGetLastError();
-      B->graph_ok = false;
-      if (B->exec) cudaGraphExecDestroy(B->exec);
-      B->exec = nullptr;
-    }
-  }
-  if (B->exec && B->graph_steps == nsteps) {
-    e = cudaGraphLaunch(B->exec, st);
-    B->graph_used = true;
-  } else {
-    e = batch_enqueue(B, nsteps, st);
-  }
-  if (e != cudaSuccess) {
-    err = std::string("batch launch: ") + cudaGetErrorString(e);
-    return FS_ERR_CUDA;
-  }
+  if (B->T.dev_nsteps != nsteps && (rc = batch_upload(B, nsteps, st, err))) return rc;
+  if ((rc = tiles_launch(B->T, nsteps, st, err))) return rc;
   for (Prod *p : B->inst) p->t += nsteps;
-  B->launches++;
+  B->launches += tiles_kernels(B->T, nsteps);
   return FS_OK;
 }
 
@@ -2458,17 +2564,6 @@ int batch_check(Batch *B, cudaStream_t st, std::string &err) {
     err = std::string("batch kernel: ") + cudaGetErrorString(e);
     return FS_ERR_CUDA;
   }
-  std::vector<int> h(B->inst.size());
-  e = cudaMemcpy(h.data(), B->errs, h.size() * 4, cudaMemcpyDeviceToHost);
-  if (e != cudaSuccess) {
-    err = std::string("error words: ") + cudaGetErrorString(e);
-    return FS_ERR_CUDA;
-  }
-  for (size_t i = 0; i < h.size(); i++)
-    if (h[i]) {
-      err = "instance " + std::to_string(i) + ": barrier wait gave up (device error word set)";
-      return FS_ERR_TIMEOUT;
-    }
   return FS_OK;
 }
 
@@ -2477,11 +2572,7 @@ int batch_check(Batch *B, cudaStream_t st, std::string &err) {
 void batch_destroy(Batch *B) {
   if (!B) return;
   for (Prod *p : B->inst) prod_destroy(p);
-  if (B->exec) cudaGraphExecDestroy(B->exec);
-  if (B->dP) cudaFree(B->dP);
-  if (B->dB) cudaFree(B->dB);
-  if (B->bars) cudaFree(B->bars);
-  if (B->errs) cudaFree(B->errs);
+  tiles_free(B->T);
   if (B->e0) cudaEventDestroy(B->e0);
   if (B->e1) cudaEventDestroy(B->e1);
   delete B;
@@ -2496,6 +2587,7 @@ int batch_create(Batch **out, uint32_t count, const fs_net_desc *const *descs, c
   }
   Batch *B = new Batch();
   B->fp64 = (o.mode == FS_MODE_FP64);
+  B->T.fp64 = B->fp64;
   B->sm = sm_count;
   B->chunk = o.chunk_steps ? o.chunk_steps : 10000;
   int rc = FS_OK;
@@ -2508,31 +2600,20 @@ int batch_create(Batch **out, uint32_t count, const fs_net_desc *const *descs, c
     }
     rc = prod_create(&p, descs[i], o, sm_count, st, err, false);
     if (rc) err = "instance " + std::to_string(i) + ": " + err;
-    else B->inst.push_back(p);
-  }
-  int occ = 0;
-  if (rc == FS_OK) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &occ, B->fp64 ? (const void *)k_prod_batch<double> : (const void *)k_prod_batch<float>, kThreads, 0);
-    B->occ = (uint32_t)std::max(1, occ);
-    cudaError_t e = bal(&B->dP, count);
-    if (e == cudaSuccess) e = bal(&B->bars, (size_t)count * 64);
-    if (e == cudaSuccess) e = bal(&B->errs, count);
-    if (e == cudaSuccess) e = cudaMemset(B->bars, 0, (size_t)count * 64 * 4);
-    if (e == cudaSuccess) e = cudaMemset(B->errs, 0, (size_t)count * 4);
-    if (e == cudaSuccess) e = cudaEventCreate(&B->e0);
-    if (e == cudaSuccess) e = cudaEventCreate(&B->e1);
-    if (e != cudaSuccess) {
-      err = std::string("batch buffers: ") + cudaGetErrorString(e);
-      rc = FS_ERR_NOMEM;
+    else {
+      B->inst.push_back(p);
+      rc = prod_tile_buffers(p, st, err);
     }
   }
   if (rc == FS_OK) {
-    uint32_t per_sm = std::min<uint32_t>(B->occ, 2);
-    if (o.blocks_per_sm) per_sm = std::min<uint32_t>(B->occ, o.blocks_per_sm);
-    while (per_sm < B->occ && B->sm * per_sm < count) per_sm++;
-    rc = batch_plan(B, per_sm, 24.0, err);
+    cudaError_t e = cudaEventCreate(&B->e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&B->e1);
+    if (e != cudaSuccess) {
+      err = std::string("batch events: ") + cudaGetErrorString(e);
+      rc = FS_ERR_CUDA;
+    }
   }
+  if (rc == FS_OK) rc = tiles_plan(B->T, B->inst, B->fp64 ? TileW<double>::W : kTile, 8, err);
   if (rc) {
     batch_destroy(B);
     return rc;
@@ -2552,14 +2633,7 @@ int batch_reset(Batch *B, const uint32_t *seeds, cudaStream_t st, std::string &e
       return rc;
     }
   }
-  cudaError_t e = cudaMemsetAsync(B->bars, 0, B->inst.size() * 64 * 4, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(B->errs, 0, B->inst.size() * 4, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) {
-    err = std::string("batch reset: ") + cudaGetErrorString(e);
-    return FS_ERR_CUDA;
-  }
-  B->dev_nsteps = 0;
+  B->T.dev_nsteps = 0;
   B->ms = 0.0;
   return FS_OK;
 }
@@ -2583,38 +2657,42 @@ int batch_run(Batch *B, uint32_t nsteps, cudaStream_t st, double *device_ms, std
   return FS_OK;
 }
 
+// Autotuner: times a sample of the batch for each tile width (posts per
+// block) and number of NMDA edges in flight per lane, keeps the fastest and
+// resets every instance (its seed unchanged).  Results never depend on the
+// choice.
 int batch_tune(Batch *B, uint32_t sample_steps, cudaStream_t st, BatchPlan *out, std::string &err) {
   if (!sample_steps) sample_steps = 200;
   double best = -1.0;
-  uint32_t best_ps = B->per_sm;
-  double best_upd = B->upd;
-  const double upds[3] = {8.0, 24.0, 64.0};
+  uint32_t best_w = B->T.tile_w;
+  int best_u = B->T.U;
   uint32_t tried = 0;
-  for (uint32_t ps = 1; ps <= std::min<uint32_t>(B->occ, 4); ps++) {
-    if (B->sm * ps < B->inst.size()) continue;
-    for (double u : upds) {
-      int rc = batch_plan(B, ps, u, err);
+  const uint32_t widths[3] = {64, 128, 256};
+  const int us[2] = {4, 8};
+  for (uint32_t w : widths) {
+    if (B->fp64 && w > TileW<double>::W) continue;
+    for (int u : us) {
+      if (B->fp64 && u != 4) continue;  // the FP64 pull has no edges-in-flight parameter
+      int rc = tiles_plan(B->T, B->inst, w, u, err);
       if (rc) return rc;
       if ((rc = batch_reset(B, nullptr, st, err))) return rc;
       double ms = 0;
-      if ((rc = batch_run(B, sample_steps, st, nullptr, err))) return rc;   // warm-up (graph capture)
+      if ((rc = batch_run(B, sample_steps, st, nullptr, err))) return rc;  // warm-up (graph capture)
       if ((rc = batch_run(B, sample_steps, st, &ms, err))) return rc;
       tried++;
       if (best < 0 || ms < best) {
         best = ms;
-        best_ps = ps;
-        best_upd = u;
+        best_w = w;
+        best_u = u;
       }
     }
   }
-  int rc = batch_plan(B, best_ps, best_upd, err);
+  int rc = tiles_plan(B->T, B->inst, best_w, best_u, err);
   if (rc == FS_OK) rc = batch_reset(B, nullptr, st, err);
   if (rc) return rc;
   B->ms = 0.0;
   if (out) {
-    out->blocks = B->blocks;
-    out->blocks_per_sm = B->per_sm;
-    out->cost_update = best_upd;
+    batch_info(B, out);
     out->sample_ms = best;
     out->candidates = tried;
   }
@@ -2622,12 +2700,16 @@ int batch_tune(Batch *B, uint32_t sample_steps, cudaStream_t st, BatchPlan *out,
 }
 
 void batch_info(const Batch *B, BatchPlan *out) {
-  out->blocks = B->blocks;
-  out->blocks_per_sm = B->per_sm;
-  out->cost_update = B->upd;
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &occ, B->fp64 ? (const void *)k_tile_step<double, 1> : (const void *)k_tile_step<float, 2>, kThreads, 0);
+  out->blocks = B->T.ntiles;
+  out->blocks_per_sm = (uint32_t)std::max(0, occ);
+  out->tile_posts = B->T.tile_w;
+  out->edges_in_flight = (uint32_t)B->T.U;
   out->sample_ms = 0.0;
   out->candidates = 0;
-  out->graph = B->graph_used ? 1 : 0;
+  out->graph = B->T.graph_used ? 1 : 0;
   out->launches = B->launches;
   out->total_ms = B->ms;
 }
@@ -2655,6 +2737,36 @@ int batch_spike_totals(Batch *B, uint64_t *totals, cudaStream_t st, std::string 
 }
 
 uint32_t batch_size(const Batch *B) { return (uint32_t)B->inst.size(); }
+
+int prod_tile_buffers(Prod *p, cudaStream_t st, std::string &err) {
+  (void)st;
+  if (p->P.gn_buf) return FS_OK;
+  return dal(p, (uint8_t **)&p->P.gn_buf, (size_t)kLB * p->n * (p->fp64 ? 8 : 4), err);
+}
+
+int tiles_solo_create(Prod *p, std::string &err) {
+  int rc = prod_tile_buffers(p, nullptr, err);
+  if (rc) return rc;
+  p->tiles = new Tiles();
+  p->tiles->fp64 = p->fp64;
+  std::vector<Prod *> one{p};
+  return tiles_plan(*p->tiles, one, p->fp64 ? TileW<double>::W : kTile, 8, err);
+}
+
+void tiles_delete(Tiles *T) {
+  if (!T) return;
+  tiles_free(*T);
+  delete T;
+}
+
+int tiles_solo_launch(Prod *p, const Params &P, uint32_t nsteps, cudaStream_t st, uint64_t *kernels,
+                      std::string &err) {
+  int rc = tiles_upload(*p->tiles, &P, 1, nsteps, st, err);
+  if (rc) return rc;
+  if ((rc = tiles_launch(*p->tiles, nsteps, st, err))) return rc;
+  if (kernels) *kernels = tiles_kernels(*p->tiles, nsteps);
+  return FS_OK;
+}
 
 // ---- failure detection check ---------------------------------------------
 // One block waits at a barrier of two blocks that the second never reaches:
@@ -2899,7 +3011,7 @@ int batch_set_gains(Batch *B, uint32_t i, const float *g, std::string &err) {
     return FS_ERR_ARG;
   }
   prod_set_gains(B->inst[i], g);
-  B->dev_nsteps = 0;  // the device copy of the parameters is stale
+  B->T.dev_nsteps = 0;  // the device copy of the parameters is stale
   return FS_OK;
 }
 

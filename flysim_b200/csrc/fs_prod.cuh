@@ -13,6 +13,8 @@ struct Prod;
 // (batch instances never do: the batch kernel advances them)
 int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t sm_count,
                 cudaStream_t st, std::string &err, bool allow_single = true);
+// NMDA-sum buffer of the tile kernels (allocated once per network)
+int prod_tile_buffers(Prod *p, cudaStream_t st, std::string &err);
 void prod_destroy(Prod *p);
 int prod_upload_params(Prod *p, const float *pb, const uint32_t *act, const float *inj_mean,
                        const float *inj_std, cudaStream_t st, std::string &err);
@@ -36,6 +38,7 @@ struct ProdInfo {
   uint32_t lin_receptors;
   int fp64;
   int single_step;  // the network runs on the single-step kernel
+  int tiles;        // the network runs on the tile kernels
 };
 void prod_info(const Prod *p, ProdInfo *info);
 int prod_spike_counts(Prod *p, uint32_t *counts, cudaStream_t st, std::string &err);
@@ -59,8 +62,8 @@ int prod_state_load(Prod *p, const uint8_t *buf, cudaStream_t st, std::string &e
 // Batch: independent production networks advanced by one persistent launch.
 struct Batch;
 struct BatchPlan {
-  uint32_t blocks, blocks_per_sm, candidates;
-  double cost_update, sample_ms;
+  uint32_t blocks, blocks_per_sm, candidates, tile_posts, edges_in_flight;
+  double sample_ms;
   int graph;
   uint64_t launches;
   double total_ms;

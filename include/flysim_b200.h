@@ -15,7 +15,8 @@
  *                  (code/NetSimGnl2_BulPp.cpp:27-727) do.  No GPU needed.
  *   - fs_create / fs_step / ...  device side: one handle owns all device
  *                  memory of one network instance on one GPU.
- *   - fs_batch_*   many independent instances in one persistent launch.
+ *   - fs_batch_*   many independent instances advanced together (one CUDA
+ *                  graph of tile-kernel launches per chunk of steps).
  *
  * Conventions: every call returns an int status (FS_OK = 0, >0 error codes
  * below); fs_last_error() gives a message.  No exceptions cross the ABI.
@@ -186,6 +187,11 @@ typedef struct fs_run_opts {
  * the interval kernel rather than the single-step kernel (for checks and
  * A/B timing; results are identical). */
 #define FS_RUN_INTERVAL_KERNEL 1u
+/* fs_run_opts.flags: run the network on the tile kernels (one launch pair
+ * per batch of steps, blocks scheduled freely over tiles of posts), which
+ * networks above ~150,000 neurons take by default; results are identical
+ * to the persistent kernel's. */
+#define FS_RUN_TILE_KERNELS 2u
 
 /* Per-call step outputs (host memory, caller owned; NULL = not wanted). */
 typedef struct fs_step_out {
@@ -244,10 +250,11 @@ int fs_run(fs_handle *h, uint32_t nsteps);
 int fs_run_timed(fs_handle *h, uint32_t nsteps, double *device_ms);
 /* Launch layout of a production-mode handle: thread blocks and threads per
  * block of its persistent kernel, the steps between grid barriers, and
- * whether it runs on the single-step kernel (FS_MODE_FP32 networks whose
- * delays are all 0 and that have no gap junctions, unless
- * FS_RUN_INTERVAL_KERNEL was given).  No counterpart in the reference. */
-int fs_engine_layout(fs_handle *h, uint32_t *blocks, uint32_t *threads, uint32_t *interval, int *single_step);
+ * which kernels run it (kernel): 0 the persistent interval kernel, 1 the
+ * single-step kernel (FS_MODE_FP32 networks whose delays are all 0 and that
+ * have no gap junctions), 2 the tile kernels (large networks).  No
+ * counterpart in the reference. */
+int fs_engine_layout(fs_handle *h, uint32_t *blocks, uint32_t *threads, uint32_t *interval, int *kernel);
 /* Synchronise and report counters. */
 int fs_sync(fs_handle *h);
 int fs_stats(fs_handle *h, uint64_t *steps_done, uint64_t *spikes_total, uint64_t *kernel_launches);
@@ -407,34 +414,38 @@ const fs_engine_vtbl *fs_device_engine(void);
  * these (code/NetSimGnl2_info.cpp:660-700). */
 int fs_spike_counts(fs_handle *h, uint32_t *counts);
 
-/* ---- batches: many independent networks in one persistent launch -------
+/* ---- batches: many independent networks advanced together --------------
  * The generalisation of the reference's repeat loop (-rp, code/main.cpp:
  * 251-252) to instances that differ in size, parameters and seed, as the
  * seizure-like E/I-gain scans need.  Every instance is a production-mode
- * network (FP32 or FP64) with its own state; one cooperative launch advances
- * all of them, each instance's blocks meeting only at its own barriers, and
- * the launch is captured once into a CUDA graph and replayed per chunk of
- * steps.  An instance's results are identical to running it alone with
- * fs_create / fs_run (same seed and philox_key). */
+ * network (FP32 or FP64) with its own state.  All instances' posts are cut
+ * into tiles; each batch of steps (at most the smallest interval of the
+ * instances, and 16) is one pair of launches over every tile of every
+ * instance (NMDA pull, then the neurons' steps and spike pushes), the blocks
+ * scheduled freely over the tiles, and a chunk of steps is captured once
+ * into a CUDA graph and replayed.  Any number of instances fits.  An
+ * instance's results are identical to running it alone with fs_create /
+ * fs_run (same seed and philox_key). */
 typedef struct fs_batch fs_batch;
 typedef struct fs_batch_plan {
-  uint32_t blocks;        /* thread blocks of the launch                     */
-  uint32_t blocks_per_sm; /* resident blocks per SM                          */
+  uint32_t blocks;        /* thread blocks of each launch: tiles of posts    */
+  uint32_t blocks_per_sm; /* resident step-kernel blocks per SM              */
   uint32_t candidates;    /* configurations the tuner timed                  */
-  float cost_update;      /* per-neuron cost weight of the block partition,
-                             in units of one NMDA in-edge                   */
+  uint32_t tile_posts;    /* posts per tile                                  */
+  uint32_t edges_in_flight; /* NMDA edges in flight per lane in the pull     */
   double sample_ms;       /* device time of the chosen plan's sample run     */
 } fs_batch_plan;
 /* opts: mode FS_MODE_FP32 (default) or FS_MODE_FP64, device, chunk_steps
- * (steps per graph replay, default 10000), philox_key, blocks_per_sm. */
+ * (steps per graph replay, default 10000), philox_key. */
 int fs_batch_create(uint32_t count, const fs_net_desc *const *descs, const fs_run_opts *opts, fs_batch **out);
 int fs_batch_destroy(fs_batch *b);
 const char *fs_batch_error(const fs_batch *b); /* b may be NULL */
 /* seeds: one per instance (NULL = the previous seeds, initially 1). */
 int fs_batch_reset(fs_batch *b, const uint32_t *seeds);
-/* Autotuner: times sample_steps (0 = 200) for each candidate block plan
- * (blocks per SM x partition cost weight), keeps the fastest and resets
- * every instance (its seed unchanged).  Results never depend on the plan. */
+/* Autotuner: times sample_steps (0 = 200) for each candidate plan (posts
+ * per tile 64 / 128 / 256 x NMDA edges in flight per lane 4 / 8), keeps the
+ * fastest and resets every instance (its seed unchanged).  Results never
+ * depend on the plan. */
 int fs_batch_tune(fs_batch *b, uint32_t sample_steps, fs_batch_plan *plan);
 /* Advances every instance by nsteps; device_ms = device time of the call. */
 int fs_batch_run(fs_batch *b, uint32_t nsteps, double *device_ms);

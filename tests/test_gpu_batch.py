@@ -1,5 +1,5 @@
-"""Batched engine (fs_batch_*): many independent production networks in one
-persistent launch.  The bar is identity: every instance's per-neuron spike
+"""Batched engine (fs_batch_*): many independent production networks advanced
+together by the tile kernels.  The bar is identity: every instance's per-neuron spike
 counts equal those of the same network run alone on the plain engine (same
 seed, same Philox key), whatever the block plan, the call split or the
 tuner's choice."""
@@ -64,15 +64,16 @@ def test_batch_equals_single_runs(built, mode):
 def test_tuner_and_plans_do_not_change_results(built):
     inst = _instances(SPECS[:4])
     res = []
-    for tune, bps in ((False, 1), (False, 2), (True, 0)):
-        b = built.Batch([na.desc for _, na in inst], blocks_per_sm=bps)
+    for tune in (False, True):
+        b = built.Batch([na.desc for _, na in inst])
         try:
             plan = b.tune(100) if tune else None
             b.reset([s for s, _ in inst])
             b.run(2500)
             res.append([b.spike_counts(i) for i in range(len(inst))])
             if tune:
-                assert plan["candidates"] >= 2 and plan["blocks"] >= len(inst)
+                assert plan["candidates"] == 6 and plan["blocks"] >= len(inst)
+                assert plan["tile_posts"] in (64, 128, 256) and plan["edges_in_flight"] in (4, 8)
         finally:
             b.close()
     for r in res[1:]:
@@ -91,7 +92,18 @@ def test_sweep_driver_matches_looped_engine(built):
     np.testing.assert_array_equal(a["hyper"], b["hyper"])
 
 
-def test_too_many_instances_is_a_capacity_error(built):
-    inst = _instances([(64, 1.0, 2000.0, 100 + i, True) for i in range(600)])
-    with pytest.raises(built.FsError, match="co-resident"):
-        built.Batch([na.desc for _, na in inst])
+def test_many_small_instances(built):
+    # more instances than the GPU holds blocks: the tile kernels schedule
+    # blocks freely, so 600 instances run; two of them equal their solo runs
+    inst = _instances([(64 + 3 * i, 1.0, 3000.0, 100 + i, True) for i in range(600)])
+    b = built.Batch([na.desc for _, na in inst], chunk_steps=1000)
+    try:
+        b.reset([s for s, _ in inst])
+        b.run(1500)
+        counts = [b.spike_counts(i) for i in (0, 599)]
+        assert b.info()["blocks"] >= 600
+    finally:
+        b.close()
+    for k, i in enumerate((0, 599)):
+        ref, _ = _single(built, inst[i][1], inst[i][0], 1500)
+        np.testing.assert_array_equal(counts[k], ref)

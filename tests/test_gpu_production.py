@@ -398,6 +398,33 @@ def test_gating_variables_equal_compat(built, mode):
     np.testing.assert_allclose(gx_b, gx_a, rtol=tol, atol=tol * np.abs(gx_a).max())
 
 
+@pytest.mark.parametrize("mode", ["fp32", "fp64"])
+def test_tile_kernels_equal_persistent_kernel(built, mode):
+    # the tile kernels (one launch pair per batch of steps, as large networks
+    # and batches run) against the persistent interval kernel: identical
+    # spikes and membrane potentials, Tsodyks-Markram plasticity included
+    from flysim_b200 import netgen, network
+    c = netgen.connectome_fast(n=30000, regions=87, seed=4)
+    na = network.connectome_net(c, tm=True)
+    out = []
+    for tiles in (False, True):
+        e = built.Engine(na.desc, mode, chunk_steps=600, tile_kernels=tiles, interval_kernel=not tiles)
+        try:
+            assert e.layout()["kernel"] == ("tiles" if tiles else "interval")
+            e.reset(3)
+            sp = []
+            for k in (1, 777, 3, 1219):
+                sp += e.step(k)[0]
+            out.append((sp, e.state()[0].copy()))
+        finally:
+            e.close()
+    (a, Va), (b, Vb) = out
+    assert sum(x.size for x in a) > 1000
+    for t, (x, y) in enumerate(zip(a, b)):
+        np.testing.assert_array_equal(x, y, err_msg="step %d" % t)
+    assert np.array_equal(Va.view(np.uint32), Vb.view(np.uint32))
+
+
 def test_checkpoint_refused_after_a_wait_gave_up(built):
     # the failure is made on the host: the handle's device error word is set
     # as a bounded wait that gave up sets it (no kernel is stopped or hung);
