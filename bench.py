@@ -264,6 +264,45 @@ def same_network_block(c, args, world, rank, flush, barrier, cap_hint: float):
         eng.close()
 
 
+def run_compat(args, rank):
+    """--mode compat: the reference-order engine (the mode whose files equal
+    the reference's byte for byte) on the 20k network with delays 0, read
+    from its .conf like the reference reads it; --ltp adds long-term
+    plasticity, which only this mode runs.  One step = 1 s simulated."""
+    import flysim_b200 as fb
+    from flysim_b200 import netgen
+    if rank != 0:
+        return 0
+    c, _ = build_network(0, "connectome20k_d0")
+    tmp = tempfile.mkdtemp()
+    try:
+        conf, pro = os.path.join(tmp, "net.conf"), os.path.join(tmp, "net.pro")
+        netgen.write_connectome(c, conf, with_delays=False)
+        netgen.write_pro(pro, 1000.0, seeds=(SEED,), outputs=())
+        m = fb.Model(conf, pro, ltp=args.ltp)
+        eng = fb.Engine(m.desc(), "compat", chunk_steps=1000)
+        eng.reset(m.seed())
+        for _ in range(args.warmup):
+            eng.run_timed(STEPS_PER_BENCH_STEP // 10)
+        ms = [eng.run_timed(STEPS_PER_BENCH_STEP) for _ in range(args.steps)]
+        st = eng.stats()
+        eng.close()
+        m.close()
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    tot = float(np.sum(ms))
+    sim_s = args.steps * STEPS_PER_BENCH_STEP * DT * 1e-3
+    print(json.dumps({
+        "metric": METRIC + ", compat mode" + (" with LTP" if args.ltp else ""), "value": sim_s / (tot * 1e-3),
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tot / args.steps, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "connectome-shaped network, 20000 neurons, delays 0, read from its .conf; "
+                               "compat mode (reference operation order and random streams)%s; one step = 1 s "
+                               "simulated" % (", -LTP" if args.ltp else "")},
+        "gpu_launches": st["launches"], "spikes": st["spikes"]}))
+    return 0
+
+
 def run_reference(args, rank):
     """--impl reference: the reference binary on the same network (delays 0).
 
@@ -335,7 +374,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--mode", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--mode", default="fp32", choices=["fp32", "fp64", "compat"],
+                    help="compat: the reference-order engine on the delays-0 network read from its .conf "
+                         "(a measurement line of its own, not the headline)")
+    ap.add_argument("--ltp", action="store_true", help="with --mode compat: run the network with -LTP")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-same-network", action="store_true",
                     help="skip the delays-0 measurement of the network the reference arm runs")
@@ -349,6 +391,8 @@ def main():
     if args.impl == "reference":
         return run_reference(args, rank)
 
+    if args.mode == "compat":
+        return run_compat(args, rank)
     import torch
     import torch.distributed as dist
     import flysim_b200 as fb
