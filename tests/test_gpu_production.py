@@ -384,7 +384,8 @@ def test_gating_variables_equal_compat(built, mode):
             e.reset(m.seed())
             for r in range(5):
                 e.set_drive(0, n, r, 0.0)
-            e.set_injection(0, n, 0.45, 0.0)
+            for k in range(0, n, 40):  # 0.52 .. 0.88 nA: thresholds crossed at different rates
+                e.set_injection(k, min(40, n - k), 0.52 + 0.04 * ((k // 40) % 10), 0.0)
             out[md] = e.step_gv(steps, sel)
         finally:
             e.close()
