@@ -334,6 +334,7 @@ def test_single_step_kernel_equals_interval_kernel(built, variant):
         e.set_drive(0, 5000, built.FS_NMDA, 0.02)
         e.set_drive(3000, 9000, built.FS_GABA, 0.05)
         e.set_injection(10000, 4000, 0.05, 0.3)
+        e.set_act(10000, 4000, 0, built.ACT["INJ"])
     (a, Va, ca), (b, Vb, cb) = _both_kernels(built, na.desc, [1, 999, 1, 1500, 499],
                                              events=events if variant == "events" else None)
     assert sum(x.size for x in a) > 1000
@@ -386,6 +387,7 @@ def test_gating_variables_equal_compat(built, mode):
                 e.set_drive(0, n, r, 0.0)
             for k in range(0, n, 40):  # 0.52 .. 0.88 nA: thresholds crossed at different rates
                 e.set_injection(k, min(40, n - k), 0.52 + 0.04 * ((k // 40) % 10), 0.0)
+            e.set_act(0, n, 0, built.ACT["INJ"])  # as the protocol driver's injection event does
             out[md] = e.step_gv(steps, sel)
         finally:
             e.close()

@@ -172,6 +172,7 @@ def _events(fb, e, f, n):
     lo, hi = n // 3, (2 * n) // 3
     mean, std = np.float32(0.05), np.float32(0.4)
     e.set_injection(lo, hi - lo, float(mean), float(std))
+    e.set_act(lo, hi - lo, 0, fb.ACT["INJ"])
     f["act"] = f["act"].copy()
     f["act"][lo:hi] |= fb.ACT["INJ"]
     f["inj_mean"] = f["inj_mean"].copy()
