@@ -373,7 +373,7 @@ def test_gating_variables_equal_compat(built, mode):
     for r in range(5):
         L = lay.rec[r]
         for e in range(L.n_recs):
-            if L.rec_pre[e] in (1, 7, 30):
+            if L.rec_pre[e] in (361, 367, 390):
                 sel.append((r << 28) | e)
     assert len(sel) > 20 and any(x >> 28 == built.FS_NMDA for x in sel)
     n = d.contents.neurons.n
@@ -385,8 +385,8 @@ def test_gating_variables_equal_compat(built, mode):
             e.reset(m.seed())
             for r in range(5):
                 e.set_drive(0, n, r, 0.0)
-            for k in range(0, n, 40):  # 0.52 .. 0.88 nA: thresholds crossed at different rates
-                e.set_injection(k, min(40, n - k), 0.52 + 0.04 * ((k // 40) % 10), 0.0)
+            for k in range(0, n, 40):  # 0.75 .. 1.11 nA, well above threshold: sharp crossings
+                e.set_injection(k, min(40, n - k), 0.75 + 0.04 * ((k // 40) % 10), 0.0)
             e.set_act(0, n, 0, built.ACT["INJ"])  # as the protocol driver's injection event does
             out[md] = e.step_gv(steps, sel)
         finally:

@@ -17,8 +17,9 @@ mode keeps the reference's own streams.  The chain is checked link by link:
 3. GPU: the device Philox equals the restatement on arbitrary counters and
    keys, bit for bit; the engine's drive draws (fs_debug_drive, the function
    its kernels call) equal the restatement: hit bitmaps bit for bit, the
-   injection current within 2 ulp of its state type (the device's log and
-   cospi and glibc's log and cos may differ in the last bit of the double).
+   injection current within 4 units of rounding of its state type (the
+   device's log and cospi and glibc's log and cos may differ in the last bit
+   of the double).
 4. GPU: a network with external drive on every receptor and injection noise,
    run by the engine, equals the float64 step-by-step restatement
    (tests/prod_model.py) fed with those draws: identical spikes for 3,000
@@ -201,8 +202,13 @@ def test_device_drive_matches_oracle(phil, built, mode):
             inj = (f["act"][first:first + count] & built.ACT["INJ"]) != 0
             assert np.all(gd[:, ~inj] == 0) and np.all(go[:, ~inj] == 0)
             if inj.any():
-                ulp = np.spacing(np.abs(go[:, inj]).astype(np.float32 if mode == "fp32" else np.float64))
-                assert np.all(np.abs(gd[:, inj] - go[:, inj]) <= 2 * ulp)
+                # mean + std z: within 4 units of rounding of the larger of
+                # its two terms (a result near 0 cancels; its own ulp is no
+                # measure of the inputs' rounding)
+                eps = np.finfo(np.float32 if mode == "fp32" else np.float64).eps
+                mean = f["inj_mean"][first:first + count][inj].astype(np.float64)
+                scale = np.maximum(np.abs(mean), np.abs(go[:, inj] - mean))
+                assert np.all(np.abs(gd[:, inj] - go[:, inj]) <= 4 * eps * scale)
                 assert np.mean(gd[:, inj] == go[:, inj]) > 0.99
     finally:
         e.close()
