@@ -384,6 +384,8 @@ def main():
     ap.add_argument("--workload", default="connectome20k", choices=sorted(WORKLOADS))
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="run this many timesteps once and exit (for ncu captures)")
+    ap.add_argument("--phase-clock", action="store_true",
+                    help="with --profile-steps: report SM cycles per timestep in each kernel phase")
     args = ap.parse_args()
     world = _env_int("WORLD_SIZE", 1)
     rank = _env_int("RANK", 0)
@@ -405,9 +407,22 @@ def main():
     eng = fb.Engine(na.desc, args.mode, device=local, chunk_steps=STEPS_PER_BENCH_STEP)
     eng.reset(SEED + rank)
     if args.profile_steps:
+        if args.phase_clock:
+            eng.run(args.profile_steps // 4)  # warm caches
+            eng.sync()
+            eng.phase_clock(True)
         eng.run(args.profile_steps)
         eng.sync()
-        print(json.dumps({"profile_steps": args.profile_steps, "stats": eng.stats()}))
+        line = {"profile_steps": args.profile_steps, "stats": eng.stats(), "layout": eng.layout()}
+        if args.phase_clock:
+            ph = eng.phase_times().astype(np.float64) / args.profile_steps
+            names = (["lists+deliveries", "nmda copies", "nmda sums", "neuron steps", "barrier", "set-up"]
+                     if eng.layout()["kernel"] == "single_step" else
+                     ["nmda pull", "drive draws", "neuron steps", "pushes", "barrier", "-"])
+            line["cycles_per_timestep"] = {nm: {"mean": round(float(ph[:, k].mean()), 1),
+                                                "max": round(float(ph[:, k].max()), 1)}
+                                           for k, nm in enumerate(names) if nm != "-"}
+        print(json.dumps(line))
         return 0
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2

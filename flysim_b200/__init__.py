@@ -143,6 +143,8 @@ def lib() -> C.CDLL:
         "fs_debug_drive": (C.c_int, [vp, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32,
                                      C.POINTER(C.c_uint8), C.POINTER(C.c_double)]),
         "fs_debug_inject_wait_failure": (C.c_int, [vp]),
+        "fs_debug_phase_clock": (C.c_int, [vp, C.c_int]),
+        "fs_debug_phase_times": (C.c_int, [vp, C.POINTER(C.c_uint64), C.c_uint32, _u32]),
         "fs_checkpoint_size": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
         "fs_checkpoint_save": (C.c_int, [vp, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
         "fs_checkpoint_load": (C.c_int, [vp, C.c_void_p, C.c_uint64]),
@@ -203,7 +205,8 @@ def exported_symbols() -> Sequence[str]:
                         "fs_get_state", "fs_debug_barrier_timeout", "fs_engine_layout",
                         "fs_debug_single_step_plan", "fs_debug_philox",
                         "fs_debug_drive",
-                        "fs_debug_inject_wait_failure", "fs_checkpoint_size", "fs_checkpoint_save", "fs_checkpoint_load",
+                        "fs_debug_inject_wait_failure", "fs_debug_phase_clock", "fs_debug_phase_times",
+                        "fs_checkpoint_size", "fs_checkpoint_save", "fs_checkpoint_load",
                         "fs_get_syn_state", "fs_model_load", "fs_model_load_cached", "fs_model_confs_info", "fs_model_network_log",
                         "fs_model_free", "fs_model_error",
                         "fs_model_desc", "fs_model_info", "fs_model_seed", "fs_model_run",
@@ -510,6 +513,21 @@ class Engine:
         _check(lib().fs_debug_drive(self._h, t0, nsteps, first, count, hits.ctypes.data_as(C.POINTER(C.c_uint8)),
                                     gauss.ctypes.data_as(C.POINTER(C.c_double))), self._h)
         return hits, gauss
+
+    def phase_clock(self, enable: bool = True):
+        """Switches the persistent kernels' per-block phase clock on (zeroed)
+        or off."""
+        _check(lib().fs_debug_phase_clock(self._h, 1 if enable else 0), self._h)
+
+    def phase_times(self) -> np.ndarray:
+        """SM cycles per block and phase since the clock was switched on,
+        [blocks, 8]."""
+        nb = C.c_uint32()
+        _check(lib().fs_debug_phase_times(self._h, None, 0, C.byref(nb)), self._h)
+        out = np.zeros(nb.value * 8, np.uint64)
+        _check(lib().fs_debug_phase_times(self._h, out.ctypes.data_as(C.POINTER(C.c_uint64)), out.size,
+                                          C.byref(nb)), self._h)
+        return out.reshape(nb.value, 8)
 
     def inject_wait_failure(self):
         """Sets the device error word as a bounded wait that gave up would."""

@@ -707,6 +707,24 @@ int fs_debug_drive(fs_handle *h, uint64_t t0, uint32_t nsteps, uint32_t first, u
   return rc ? set_err(h, rc, h->err) : FS_OK;
 }
 
+int fs_debug_phase_clock(fs_handle *h, int enable) {
+  if (!h) return set_err(nullptr, FS_ERR_ARG, "null handle");
+  if (h->mode == FS_MODE_COMPAT || !h->prod)
+    return set_err(h, FS_ERR_UNSUPPORTED, "fs_debug_phase_clock: production modes only");
+  CK(cudaSetDevice(h->device));
+  int rc = fsp::prod_phase_clock(h->prod, enable, h->st, h->err);
+  return rc ? set_err(h, rc, h->err) : FS_OK;
+}
+
+int fs_debug_phase_times(fs_handle *h, uint64_t *out, uint32_t cap, uint32_t *blocks) {
+  if (!h) return set_err(nullptr, FS_ERR_ARG, "null handle");
+  if (h->mode == FS_MODE_COMPAT || !h->prod)
+    return set_err(h, FS_ERR_UNSUPPORTED, "fs_debug_phase_times: production modes only");
+  CK(cudaSetDevice(h->device));
+  int rc = fsp::prod_phase_times(h->prod, out, cap, blocks, h->st, h->err);
+  return rc ? set_err(h, rc, h->err) : FS_OK;
+}
+
 int fs_debug_inject_wait_failure(fs_handle *h) {
   if (!h) return set_err(nullptr, FS_ERR_ARG, "null handle");
   if (h->mode == FS_MODE_COMPAT || !h->prod)

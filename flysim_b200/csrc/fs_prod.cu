@@ -122,6 +122,7 @@ struct Params {
   // GatingVariable output (or null): selections of neuron p are entries
   // [gv_row[p], gv_row[p+1]) of gv_ent (output column | receptor << 28)
   void *gn_buf;          // tile kernels: NMDA sums of a batch of steps, [L][n]
+  unsigned long long *phase;  // phase clock: [blocks][8] SM cycles per phase, or null
   const uint32_t *gv_row, *gv_ent;
   uint32_t gv_n;
   float *gv_st, *gv_xt;  // [steps][gv_n]
@@ -484,6 +485,25 @@ __device__ __forceinline__ void draw_inputs(const Params &P, uint32_t p0, uint32
     gauss[j][q] = gv;
   }
 }
+
+// ---- phase clock (debug aid) -------------------------------------------------
+// When P.phase is set, thread 0 of each block adds the SM cycles between
+// consecutive marks to its block's counter k (a relaxed add per mark).
+struct PhaseClock {
+  unsigned long long *out;
+  long long t;
+  __device__ __forceinline__ void start(const Params &P) {
+    out = (P.phase && threadIdx.x == 0) ? P.phase + (size_t)blockIdx.x * 8 : nullptr;
+    if (out) t = clock64();
+  }
+  __device__ __forceinline__ void mark(int k) {
+    if (out) {
+      const long long now = clock64();
+      atomicAdd(out + k, (unsigned long long)(now - t));
+      t = now;
+    }
+  }
+};
 
 // ---- one neuron's step (shared by every kernel) ----------------------------
 // Parameters and state of one neuron, held in registers while its thread
@@ -893,7 +913,7 @@ __device__ __forceinline__ void tile_pull(const Params &P, uint32_t tp0, uint32_
 // drive draws, gap currents, the neurons' steps and the spikes' pushes.
 template <class T, int PD>
 __device__ __forceinline__ void tile_steps(const Params &P, uint32_t tp0, uint32_t np, uint32_t bs, uint32_t L,
-                                           TileBufs<T> &B) {
+                                           TileBufs<T> &B, PhaseClock &pc) {
   constexpr uint32_t kCap = TileBufs<T>::kCap;
   const SpikeList<T> lst{&B.l_n, B.l_p, B.l_tm, B.l_c, kCap};
   const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -915,9 +935,11 @@ __device__ __forceinline__ void tile_steps(const Params &P, uint32_t tp0, uint32
     }
   }
   __syncthreads();
+  pc.mark(1);
   // warps without neurons in this tile skip the steps
   if ((tid & ~31u) < np) neuron_steps<T, PD>(P, tp0, np, bs, L, B.gn, B.hits, B.gauss, lst, B.gapI);
   __syncthreads();
+  pc.mark(2);
   // the batch's spikes: with fewer spikes than warps the whole block
   // walks each spike's out-edges (a hub's hundreds of edges in one or
   // two rounds); with more, one spike per warp, eight in flight
@@ -938,6 +960,7 @@ __device__ __forceinline__ void tile_steps(const Params &P, uint32_t tp0, uint32
     }
   }
   __syncthreads();
+  pc.mark(3);
   if (tid == 0) B.l_n = 0;
 }
 
@@ -949,6 +972,8 @@ template <class T, int PU, int PD>
 __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32_t B1, uint32_t nblk) {
   constexpr uint32_t kT = TileW<T>::W;
   __shared__ TileBufs<T> B;
+  PhaseClock pc;
+  pc.start(P);
   if (threadIdx.x == 0) B.l_n = 0;
   __syncthreads();
   uint32_t s = 0;
@@ -959,12 +984,14 @@ __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32
       for (uint32_t tp0 = B0; tp0 < B1; tp0 += kT) {
         const uint32_t np = min(kT, B1 - tp0);
         tile_pull<T, PU>(P, tp0, np, bs, L, B);
-        tile_steps<T, PD>(P, tp0, np, bs, L, B);
+        pc.mark(0);
+        tile_steps<T, PD>(P, tp0, np, bs, L, B, pc);
       }
     }
     s = iv_end;
     if (s < P.nsteps) {
       if (!grid_sync(P.bar, P.err, nblk)) return;
+      pc.mark(4);
     }
   }
 }
@@ -1109,20 +1136,30 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
     d_hits[tid] = (uint8_t)draw_one<float>(P, p, P.t0, gv);
     d_gauss[tid] = gv;
   }
+  PhaseClock pc;
+  pc.start(P);
   __syncthreads();
+  pc.mark(5);
   for (uint32_t s = 0; s < P.nsteps; s++) {
     const uint64_t t = P.t0 + s;
     if (s > 0) {
       // ---- spikes of step t - 1: deliveries, then the NMDA copies ----
       const uint32_t par = (uint32_t)(t - 1u) & 1u;
-      const uint32_t cnt = __ldcg(P.t1_cnt + par);
       const uint4 *lst = P.t1_list + (size_t)par * n * 2;
+      // the first pass's entries are loaded with the count (one round trip;
+      // entries past the count are ignored)
+      uint4 a0 = make_uint4(0u, 0u, 0u, 0u), b0 = a0;
+      if (tid < n) {
+        a0 = __ldcg(lst + 2 * (size_t)tid);
+        b0 = __ldcg(lst + 2 * (size_t)tid + 1);
+      }
+      const uint32_t cnt = __ldcg(P.t1_cnt + par);
       for (uint32_t c0 = 0; c0 < cnt; c0 += kT1F) {
         if (tid == 0) f_n = 0;
         __syncthreads();
         const uint32_t i = c0 + tid;
         if (tid < kT1F && i < cnt) {
-          const uint4 a = __ldcg(lst + 2 * (size_t)i), b = __ldcg(lst + 2 * (size_t)i + 1);
+          const uint4 a = c0 == 0 ? a0 : __ldcg(lst + 2 * (size_t)i), b = c0 == 0 ? b0 : __ldcg(lst + 2 * (size_t)i + 1);
           const int j = find_sorted(gid, NT, a.x);
           if (j >= 0) {
             flag[j] = 1;
@@ -1152,6 +1189,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
         }
         __syncthreads();
       }
+      pc.mark(0);
       for (uint32_t j = tid; j < NT; j += kT1) {
         const uint8_t c = cls[j];
         if (c != 255) {
@@ -1164,16 +1202,31 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
         flag[j] = 0;
       }
       __syncthreads();
+      pc.mark(1);
     }
     // ---- NMDA sums of the block's posts (order of nmda_pull1_f32) ----
     for (uint32_t qq = wid; qq < np; qq += kT1 / 32) {
       float a = 0.0f;
-      for (uint32_t e = erow[qq] + lane; e < erow[qq + 1]; e += 32) a = __fmaf_rn(ew[e], ts[eidx[e]], a);
+      const uint32_t e1 = erow[qq + 1];
+      // four of the lane's edges loaded before their sums (same order)
+      for (uint32_t e = erow[qq] + lane; e < e1; e += 128) {
+        float w[4], v[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const uint32_t ee = e + 32u * u;
+          w[u] = ee < e1 ? ew[ee] : 0.0f;
+          v[u] = ee < e1 ? ts[eidx[ee]] : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (e + 32u * u < e1) a = __fmaf_rn(w[u], v[u], a);
+      }
 #pragma unroll
       for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(fsd::kFull, a, o);
       if (lane == 0) gn[qq] = a;
     }
     __syncthreads();
+    pc.mark(2);
     // ---- the neurons' step ----
     if (active) {
       long long rv[4];
@@ -1227,6 +1280,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
         }
       }
     }
+    pc.mark(3);
     if (s + 1 < P.nsteps) {
       // the next step's drive draws are made while the barrier is awaited
       const uint64_t tn = t + 1;
@@ -1238,6 +1292,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
         }
       });
       if (!ok) return;
+      pc.mark(4);
     }
   }
   if (own) {
@@ -1308,7 +1363,9 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) k_tile_step(
     const uint32_t j = i / tl.np, q = i - j * tl.np;
     B.gn[j][q] = in[(size_t)j * P.n + tl.p0 + q];
   }
-  tile_steps<T, PD>(P, tl.p0, tl.np, bs, L, B);  // its first barrier orders the loads above
+  PhaseClock pc;
+  pc.out = nullptr;
+  tile_steps<T, PD>(P, tl.p0, tl.np, bs, L, B, pc);  // its first barrier orders the loads above
 }
 
 
@@ -1319,6 +1376,7 @@ struct Prod {
   bool single = false;     // runs on the single-step kernel k_prod1
   struct Tiles *tiles = nullptr;  // runs on the tile kernels (large networks)
   uint32_t b1_blocks = 0;  // its blocks (one per SM at most)
+  unsigned long long *phase_buf = nullptr;  // phase clock counters (debug aid)
   bool wide = false;  // some block's posts span several tiles: eight NMDA edges in flight
   uint32_t n = 0, sm = 148;
   Params P{};
@@ -2876,6 +2934,48 @@ int prod_debug_drive(Prod *p, uint64_t t0, uint32_t nsteps, uint32_t first, uint
   if (dg) cudaFree(dg);
   if (e != cudaSuccess) {
     err = std::string("drive check: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  return FS_OK;
+}
+
+// Phase clock: per block, SM cycles spent in each phase of the persistent
+// kernels since it was switched on (k_prod1: 0 spike lists and deliveries,
+// 1 NMDA copies, 2 NMDA sums, 3 neuron steps and spike lists, 4 grid
+// barrier; k_prod: 0 NMDA pull, 1 drive draws, 2 neuron steps, 3 pushes,
+// 4 grid barrier).
+int prod_phase_clock(Prod *p, int enable, cudaStream_t st, std::string &err) {
+  const uint32_t nb = std::max(p->blocks, p->b1_blocks);
+  if (!enable) {
+    p->P.phase = nullptr;
+    return FS_OK;
+  }
+  if (!p->phase_buf) {
+    int rc = dal(p, &p->phase_buf, (size_t)nb * 8, err);
+    if (rc) return rc;
+  }
+  cudaError_t e = cudaMemsetAsync(p->phase_buf, 0, (size_t)nb * 8 * 8, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("phase clock: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  p->P.phase = p->phase_buf;
+  return FS_OK;
+}
+
+int prod_phase_times(Prod *p, uint64_t *out, uint32_t cap, uint32_t *blocks, cudaStream_t st, std::string &err) {
+  const uint32_t nb = p->single ? p->b1_blocks : p->blocks;
+  if (blocks) *blocks = nb;
+  if (!p->phase_buf) {
+    err = "phase clock was never switched on";
+    return FS_ERR_ARG;
+  }
+  const size_t k = std::min<size_t>(cap, (size_t)nb * 8);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess && k) e = cudaMemcpy(out, p->phase_buf, k * 8, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    err = std::string("phase clock: ") + cudaGetErrorString(e);
     return FS_ERR_CUDA;
   }
   return FS_OK;

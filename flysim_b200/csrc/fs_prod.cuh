@@ -51,6 +51,10 @@ int prod_barrier_probe(unsigned int limit, int *err_word, std::string &err);
 int prod_debug_philox(const uint32_t *ctr, const uint32_t *key, uint64_t k, uint32_t *out, std::string &err);
 int prod_debug_drive(Prod *p, uint64_t t0, uint32_t nsteps, uint32_t first, uint32_t count, uint8_t *hits,
                      double *gauss, cudaStream_t st, std::string &err);
+// Phase clock of the persistent kernels (debug aid): per block, SM cycles
+// per phase; out holds [blocks][8].
+int prod_phase_clock(Prod *p, int enable, cudaStream_t st, std::string &err);
+int prod_phase_times(Prod *p, uint64_t *out, uint32_t cap, uint32_t *blocks, cudaStream_t st, std::string &err);
 // Stores into the device error word what a bounded wait that gave up stores.
 int prod_inject_wait_failure(Prod *p, cudaStream_t st, std::string &err);
 // Checkpoint blob of the engine's step-to-step state (step counter, drive

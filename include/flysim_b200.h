@@ -313,6 +313,16 @@ int fs_debug_drive(fs_handle *h, uint64_t t0, uint32_t nsteps, uint32_t first, u
  * linear delivery entries, [7] NMDA edges.  FS_ERR_ARG names a violated
  * bound.  No counterpart in the reference. */
 int fs_debug_single_step_plan(const fs_net_desc *desc, uint32_t sm_count, uint64_t *stats);
+/* Phase clock of the persistent kernels (a profiling aid; no counterpart in
+ * the reference).  fs_debug_phase_clock(h, 1) zeroes and switches on
+ * per-block counters of SM cycles per phase, 0 switches them off;
+ * fs_debug_phase_times copies up to cap counters, [blocks][8], and the
+ * block count.  Phases: single-step kernel 0 spike lists and deliveries,
+ * 1 NMDA copies, 2 NMDA sums, 3 neuron steps, 4 grid barrier, 5 set-up;
+ * interval kernel 0 NMDA pull, 1 drive draws, 2 neuron steps, 3 pushes,
+ * 4 grid barrier.  The tile kernels have no phase clock. */
+int fs_debug_phase_clock(fs_handle *h, int enable);
+int fs_debug_phase_times(fs_handle *h, uint64_t *out, uint32_t cap, uint32_t *blocks);
 /* Failure detection on the host side: stores into the handle's device error
  * word what a bounded device wait that gave up stores, without running or
  * stopping any kernel, so that the paths which must notice it (fs_sync,
