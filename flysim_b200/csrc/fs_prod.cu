@@ -40,6 +40,7 @@
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 #include <cuda_runtime.h>
 #include "fs_prod.cuh"
@@ -1084,25 +1085,27 @@ __device__ __forceinline__ bool grid_sync_work(unsigned int *bar, int *err, uint
 
 __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params P) {
   extern __shared__ __align__(16) unsigned char sm1[];
-  __shared__ float gn[kT1], d_gauss[kT1], f_c[kT1F][4];
+  __shared__ float gn[kT1], d_gauss[kT1], f_c[kT1F][4], nf_inc[kT1F];
   __shared__ uint8_t d_hits[kT1];
-  __shared__ uint32_t f_j[kT1F], f_n;
+  __shared__ uint32_t f_j[kT1F], f_n, nf_j[kT1F], nf_n;
   const Blk1 me = P.b1[blockIdx.x];
   const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const uint32_t n = P.n, S = P.slots, mask = P.mask, NT = me.ntrk, np = me.np;
-  // shared-memory layout (16-byte aligned pieces first)
-  long long *acc = (long long *)sm1;                        // [nlin][kT1]
-  float *tx = (float *)(acc + (size_t)max(1u, P.nlin) * kT1);  // [NT] NMDA x copies
-  float *ts = tx + NT;                                      // [NT] NMDA s copies
-  float *tinc = ts + NT;                                    // [NT] increment of a listed spike
-  float *ctab = tinc + NT;                                  // [ncls][3]
-  float *ew = ctab + 3 * P.t1_ncls;                         // [ne]
-  uint32_t *gid = (uint32_t *)(ew + me.ne);                 // [NT]
-  uint32_t *lrow = gid + NT;                                // [NT + 1]
-  uint32_t *erow = lrow + NT + 1;                           // [np + 1]
-  uint16_t *eidx = (uint16_t *)(erow + np + 1);             // [ne]
-  uint8_t *cls = (uint8_t *)(eidx + me.ne);                 // [NT]
-  uint8_t *flag = cls + NT;                                 // [NT] listed this step
+  // shared-memory layout (16-byte aligned pieces first); the NMDA copies are
+  // double-buffered by step parity: buffer s & 1 holds the values after
+  // step t0 + s - 1
+  long long *acc = (long long *)sm1;                           // [nlin][kT1]
+  float *const cx0 = (float *)(acc + (size_t)max(1u, P.nlin) * kT1);  // [NT] NMDA x copies
+  float *const cs0 = cx0 + NT;                                 // [NT] NMDA s copies
+  float *const cx1 = cs0 + NT;
+  float *const cs1 = cx1 + NT;
+  float *ctab = cs1 + NT;                                      // [ncls][3]
+  float *ew = ctab + 3 * P.t1_ncls;                            // [ne]
+  uint32_t *gid = (uint32_t *)(ew + me.ne);                    // [NT]
+  uint32_t *lrow = gid + NT;                                   // [NT + 1]
+  uint32_t *erow = lrow + NT + 1;                              // [np + 1]
+  uint16_t *eidx = (uint16_t *)(erow + np + 1);                // [ne]
+  uint8_t *cls = (uint8_t *)(eidx + me.ne);                    // [NT]
   // ---- tables ----
   for (uint32_t i = tid; i < max(1u, P.nlin) * kT1; i += kT1) acc[i] = 0ll;
   for (uint32_t i = tid; i < 3 * P.t1_ncls; i += kT1) ctab[i] = __ldg(P.t1_cls_tab + i);
@@ -1111,11 +1114,10 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
     const uint8_t c = __ldg(P.t1_cls + me.trk0 + j);
     gid[j] = g;
     cls[j] = c;
-    flag[j] = 0;
     // the copies start from the owners' values after the last step before
     // this launch (written back by the previous launch)
-    tx[j] = c != 255 ? __ldcg((const float *)P.x_pre + g) : 0.0f;
-    ts[j] = c != 255 ? __ldcg((const float *)P.s_pre + g) : 0.0f;
+    cx0[j] = c != 255 ? __ldcg((const float *)P.x_pre + g) : 0.0f;
+    cs0[j] = c != 255 ? __ldcg((const float *)P.s_pre + g) : 0.0f;
   }
   for (uint32_t j = tid; j <= NT; j += kT1) lrow[j] = __ldg(P.t1_lrow + me.lrow0 + j);
   for (uint32_t q = tid; q <= np; q += kT1) erow[q] = __ldg(P.t1_erow + me.erow0 + q);
@@ -1142,8 +1144,14 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
   pc.mark(5);
   for (uint32_t s = 0; s < P.nsteps; s++) {
     const uint64_t t = P.t0 + s;
+    float *X = (s & 1u) ? cx1 : cx0, *Sv = (s & 1u) ? cs1 : cs0;
     if (s > 0) {
-      // ---- spikes of step t - 1: deliveries, then the NMDA copies ----
+      // ---- spikes of step t - 1 ----
+      // the buffer of this step already holds every copy advanced as if its
+      // neuron had not spiked (made during the barrier wait); the listed
+      // spikes are redone from the previous buffer, and their linear
+      // synapses onto this block are delivered
+      const float *Xo = (s & 1u) ? cx0 : cx1, *So = (s & 1u) ? cs0 : cs1;
       const uint32_t par = (uint32_t)(t - 1u) & 1u;
       const uint4 *lst = P.t1_list + (size_t)par * n * 2;
       // the first pass's entries are loaded with the count (one round trip;
@@ -1155,15 +1163,21 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
       }
       const uint32_t cnt = __ldcg(P.t1_cnt + par);
       for (uint32_t c0 = 0; c0 < cnt; c0 += kT1F) {
-        if (tid == 0) f_n = 0;
+        if (tid == 0) {
+          f_n = 0;
+          nf_n = 0;
+        }
         __syncthreads();
         const uint32_t i = c0 + tid;
         if (tid < kT1F && i < cnt) {
           const uint4 a = c0 == 0 ? a0 : __ldcg(lst + 2 * (size_t)i), b = c0 == 0 ? b0 : __ldcg(lst + 2 * (size_t)i + 1);
           const int j = find_sorted(gid, NT, a.x);
           if (j >= 0) {
-            flag[j] = 1;
-            tinc[j] = __uint_as_float(a.y);
+            if (cls[j] != 255) {
+              const uint32_t k = atomicAdd(&nf_n, 1u);
+              nf_j[k] = (uint32_t)j;
+              nf_inc[k] = __uint_as_float(a.y);
+            }
             if (lrow[j + 1] > lrow[j]) {
               const uint32_t k = atomicAdd(&f_n, 1u);
               f_j[k] = (uint32_t)j;
@@ -1175,6 +1189,14 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
           }
         }
         __syncthreads();
+        // the NMDA copies of the listed neurons, from their previous values
+        for (uint32_t k = tid; k < nf_n; k += kT1) {
+          const uint32_t j = nf_j[k], c = cls[j];
+          float xv = Xo[j], sv = So[j];
+          nmda_pre_step<float>(xv, sv, true, nf_inc[k], ctab[3 * c], ctab[3 * c + 1], ctab[3 * c + 2]);
+          X[j] = xv;
+          Sv[j] = sv;
+        }
         // one warp per listed spike walks its synapses onto this block
         for (uint32_t k = wid; k < f_n; k += kT1 / 32) {
           const uint32_t j = f_j[k];
@@ -1190,40 +1212,42 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
         __syncthreads();
       }
       pc.mark(0);
-      for (uint32_t j = tid; j < NT; j += kT1) {
-        const uint8_t c = cls[j];
-        if (c != 255) {
-          const bool spk = flag[j] != 0;
-          float xv = tx[j], sv = ts[j];
-          nmda_pre_step<float>(xv, sv, spk, spk ? tinc[j] : 1.0f, ctab[3 * c], ctab[3 * c + 1], ctab[3 * c + 2]);
-          tx[j] = xv;
-          ts[j] = sv;
-        }
-        flag[j] = 0;
-      }
-      __syncthreads();
       pc.mark(1);
     }
     // ---- NMDA sums of the block's posts (order of nmda_pull1_f32) ----
-    for (uint32_t qq = wid; qq < np; qq += kT1 / 32) {
-      float a = 0.0f;
-      const uint32_t e1 = erow[qq + 1];
-      // four of the lane's edges loaded before their sums (same order)
-      for (uint32_t e = erow[qq] + lane; e < e1; e += 128) {
-        float w[4], v[4];
+    // a warp takes two posts at once, each summed lane-strided with four
+    // edges loaded ahead, then both butterflies
+    for (uint32_t qa = wid; qa < np; qa += kT1 / 16) {
+      const uint32_t qb = qa + kT1 / 32;
+      const uint32_t ea0 = erow[qa], ea1 = erow[qa + 1];
+      const uint32_t eb0 = qb < np ? erow[qb] : 0u, eb1 = qb < np ? erow[qb + 1] : 0u;
+      const uint32_t len = max(ea1 - ea0, eb1 - eb0);
+      float aa = 0.0f, ab = 0.0f;
+      for (uint32_t o = lane; o < len; o += 128) {
+        float wa[4], va[4], wb[4], vb[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-          const uint32_t ee = e + 32u * u;
-          w[u] = ee < e1 ? ew[ee] : 0.0f;
-          v[u] = ee < e1 ? ts[eidx[ee]] : 0.0f;
+          const uint32_t xa = ea0 + o + 32u * u, xb = eb0 + o + 32u * u;
+          wa[u] = xa < ea1 ? ew[xa] : 0.0f;
+          va[u] = xa < ea1 ? Sv[eidx[xa]] : 0.0f;
+          wb[u] = xb < eb1 ? ew[xb] : 0.0f;
+          vb[u] = xb < eb1 ? Sv[eidx[xb]] : 0.0f;
         }
 #pragma unroll
-        for (int u = 0; u < 4; u++)
-          if (e + 32u * u < e1) a = __fmaf_rn(w[u], v[u], a);
+        for (int u = 0; u < 4; u++) {
+          if (ea0 + o + 32u * u < ea1) aa = __fmaf_rn(wa[u], va[u], aa);
+          if (eb0 + o + 32u * u < eb1) ab = __fmaf_rn(wb[u], vb[u], ab);
+        }
       }
 #pragma unroll
-      for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(fsd::kFull, a, o);
-      if (lane == 0) gn[qq] = a;
+      for (int o = 16; o; o >>= 1) {
+        aa += __shfl_xor_sync(fsd::kFull, aa, o);
+        ab += __shfl_xor_sync(fsd::kFull, ab, o);
+      }
+      if (lane == 0) {
+        gn[qa] = aa;
+        if (qb < np) gn[qb] = ab;
+      }
     }
     __syncthreads();
     pc.mark(2);
@@ -1282,13 +1306,25 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
     }
     pc.mark(3);
     if (s + 1 < P.nsteps) {
-      // the next step's drive draws are made while the barrier is awaited
+      // while the barrier is awaited: the next step's drive draws, and every
+      // NMDA copy advanced into the other buffer as if its neuron had not
+      // spiked (the listed spikes are redone after the barrier)
       const uint64_t tn = t + 1;
+      float *Xn = (s & 1u) ? cx0 : cx1, *Sn = (s & 1u) ? cs0 : cs1;
       const bool ok = grid_sync_work(P.bar, P.err, gridDim.x, P.t1_cnt + ((uint32_t)(t + 1u) & 1u), [&]() {
         for (uint32_t qq = tid - 32; qq < np; qq += kT1 - 32) {
           float gv = 0.0f;
           d_hits[qq] = (uint8_t)draw_one<float>(P, me.post0 + qq, tn, gv);
           d_gauss[qq] = gv;
+        }
+        for (uint32_t j = tid - 32; j < NT; j += kT1 - 32) {
+          const uint32_t c = cls[j];
+          if (c != 255) {
+            float xv = X[j], sv = Sv[j];
+            nmda_pre_step<float>(xv, sv, false, 1.0f, ctab[3 * c], ctab[3 * c + 1], ctab[3 * c + 2]);
+            Xn[j] = xv;
+            Sn[j] = sv;
+          }
         }
       });
       if (!ok) return;
@@ -1837,7 +1873,7 @@ static bool plan_single(uint32_t n, uint32_t nlin, uint32_t sm_count, const std:
     S1.lrow.push_back((uint32_t)(S1.lin.size() - bk.l0));
     for (uint32_t a : trk) loc[a] = -1;
     S1.blk.push_back(bk);
-    const size_t need = fixed + (size_t)bk.ntrk * (4 * 3 + 4 + 4 + 2) + 4 + (size_t)bk.ne * 6 + (size_t)(bk.np + 1) * 4;
+    const size_t need = fixed + (size_t)bk.ntrk * (4 * 4 + 4 + 4 + 1) + 4 + (size_t)bk.ne * 6 + (size_t)(bk.np + 1) * 4;
     smax = std::max(smax, need);
   }
   // dynamic shared memory next to the kernel's ~15 KB of static arrays
@@ -1899,9 +1935,11 @@ static bool validate_single(const HostNet &H, const Single &S1, std::string &err
       if (S1.gid[k.trk0 + j] != (H.in_code[H.in_row[k.post0] + e] & 0xffffffu)) return fail(b, "edge source");
     }
     nmda_total += k.ne;
-    const size_t need = (size_t)std::max(1u, H.nlin) * kT1 * 8 + (size_t)k.ntrk * 12 + 3 * (size_t)ncls * 4 +
+    // the kernel's layout: acc | x, s copies x2 | class table | edge weights |
+    // ids | linear rows | edge rows | edge indices | classes
+    const size_t need = (size_t)std::max(1u, H.nlin) * kT1 * 8 + (size_t)k.ntrk * 16 + 3 * (size_t)ncls * 4 +
                         (size_t)k.ne * 4 + (size_t)k.ntrk * 4 + ((size_t)k.ntrk + 1) * 4 + ((size_t)k.np + 1) * 4 +
-                        (size_t)k.ne * 2 + (size_t)k.ntrk * 2;
+                        (size_t)k.ne * 2 + (size_t)k.ntrk;
     if (need > S1.smem) return fail(b, "shared memory");
   }
   if (next_post != n) return fail((uint32_t)S1.blk.size(), "posts not covered");
@@ -1933,8 +1971,17 @@ int prod_check_single_plan(const fs_net_desc *d, uint32_t sm_count, uint64_t *st
   return FS_OK;
 }
 
+static int prod_create_from(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t sm_count,
+                            cudaStream_t st, std::string &err, bool allow_single, HostNet *pre);
+
 int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t sm_count, cudaStream_t st,
                 std::string &err, bool allow_single) {
+  return prod_create_from(out, d, o, sm_count, st, err, allow_single, nullptr);
+}
+
+// pre: host tables already built by host_net (moved from), or null
+static int prod_create_from(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t sm_count,
+                            cudaStream_t st, std::string &err, bool allow_single, HostNet *pre) {
   *out = nullptr;
   const fs_neurons &v = d->neurons;
   const uint32_t n = v.n;
@@ -1962,7 +2009,9 @@ int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t
   for (int r = 0; r < 5; r++) P.rg[r] = 1.0f;
   const size_t nr = (size_t)FS_NREC * n;
   HostNet H;
-  {
+  if (pre) {
+    H = std::move(*pre);
+  } else {
     int hrc = host_net(d, H, err);
     if (hrc) {
       delete p;
@@ -2649,18 +2698,37 @@ int batch_create(Batch **out, uint32_t count, const fs_net_desc *const *descs, c
   B->sm = sm_count;
   B->chunk = o.chunk_steps ? o.chunk_steps : 10000;
   int rc = FS_OK;
-  for (uint32_t i = 0; i < count && rc == FS_OK; i++) {
-    Prod *p = nullptr;
+  for (uint32_t i = 0; i < count && rc == FS_OK; i++)
     if (!descs[i]) {
       err = "batch: null network description " + std::to_string(i);
       rc = FS_ERR_ARG;
-      break;
     }
-    rc = prod_create(&p, descs[i], o, sm_count, st, err, false);
-    if (rc) err = "instance " + std::to_string(i) + ": " + err;
-    else {
-      B->inst.push_back(p);
-      rc = prod_tile_buffers(p, st, err);
+  // the host tables of a wave of instances are built on all host threads,
+  // then the instances are uploaded one by one
+  const uint32_t wave = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  for (uint32_t i0 = 0; i0 < count && rc == FS_OK; i0 += wave) {
+    const uint32_t k = std::min(wave, count - i0);
+    std::vector<HostNet> hn(k);
+    std::vector<int> hrc(k, FS_OK);
+    std::vector<std::string> herr(k);
+    std::vector<std::thread> th;
+    for (uint32_t j = 0; j < k; j++)
+      th.emplace_back([&, j]() { hrc[j] = host_net(descs[i0 + j], hn[j], herr[j]); });
+    for (auto &x : th) x.join();
+    for (uint32_t j = 0; j < k && rc == FS_OK; j++) {
+      const uint32_t i = i0 + j;
+      Prod *p = nullptr;
+      if (hrc[j]) {
+        rc = hrc[j];
+        err = "instance " + std::to_string(i) + ": " + herr[j];
+        break;
+      }
+      rc = prod_create_from(&p, descs[i], o, sm_count, st, err, false, &hn[j]);
+      if (rc) err = "instance " + std::to_string(i) + ": " + err;
+      else {
+        B->inst.push_back(p);
+        rc = prod_tile_buffers(p, st, err);
+      }
     }
   }
   if (rc == FS_OK) {

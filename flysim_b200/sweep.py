@@ -77,7 +77,7 @@ def run_batched(points: Sequence[SweepPoint], seconds: float = 2.0, dt: float = 
     steps = int(round(seconds * 1e3 / dt))
     t0 = time.perf_counter()
     b = Batch([na.desc for na in nets], mode=mode)
-    plan = b.tune() if tune else None
+    plan = b.tune(100) if tune else None
     b.reset([p.seed for p in points])
     dev_ms = b.run(steps)
     counts = [b.spike_counts(i) for i in range(len(points))]
