@@ -153,6 +153,13 @@ __device__ __forceinline__ void philox(uint32_t c[4], uint32_t k0, uint32_t k1) 
 }
 __device__ __forceinline__ float u24(uint32_t x) { return (float)(x >> 8) * 5.9604644775390625e-08f; }
 
+// Delay ring slot of (linear receptor index ri, post, slot): slot-major,
+// [ri][slot][post], so the posts a warp advances read one slot's
+// consecutive words.
+__device__ __forceinline__ unsigned long long *ring_at(const Params &P, int ri, uint32_t post, uint32_t slot) {
+  return P.ring + ((size_t)ri * P.slots + slot) * P.n + post;
+}
+
 // ---- bounded grid barrier ---------------------------------------------------
 // Over the `count` blocks that share `bar` (the whole grid, or the blocks of
 // one network instance in a batch).  bar[0] counts arrivals, bar[32] (its
@@ -409,7 +416,7 @@ __device__ __forceinline__ void nmda_pull(const Params &P, uint32_t p0, uint32_t
 template <class T>
 __device__ __forceinline__ void push_spike(const Params &P, uint32_t q, uint32_t tm, const T (&cj)[4],
                                            uint32_t start, uint32_t stride) {
-  const uint32_t n = P.n, S = P.slots, mask = P.mask;
+  const uint32_t mask = P.mask;
   const uint32_t ob = __ldg(P.out_row + q), oe = __ldg(P.out_row + q + 1);
   for (uint32_t e = ob + start; e < oe; e += 4 * stride) {
     uint32_t code[4];
@@ -427,7 +434,7 @@ __device__ __forceinline__ void push_spike(const Params &P, uint32_t q, uint32_t
         const T cv = ((r == 0) ? cj[0] : (r == 1) ? cj[1] : (r == 2) ? cj[2] : cj[3]) * (T)P.rg[r];
         const long long fx = __double2ll_rn((double)((T)w[u] * cv) * kFix);
         const int ri = P.lin_of_rec[r];
-        atomicAdd(P.ring + ((size_t)ri * n + post) * S + ((tm + d) & mask), (unsigned long long)fx);
+        atomicAdd(ring_at(P, ri, post, (tm + d) & mask), (unsigned long long)fx);
       }
     }
   }
@@ -807,8 +814,8 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
 #pragma unroll
     for (int r = 0; r < 4; r++) {
       const int ri = P.lin_of_rec[r];
-      rv[r] = (ri >= 0 && own) ? (long long)__ldcg(P.ring + ((size_t)ri * n + p) * S + tprev) : 0ll;
-      rv2[r] = (PD == 2 && ri >= 0 && own && L > 1) ? (long long)__ldcg(P.ring + ((size_t)ri * n + p) * S + tn) : 0ll;
+      rv[r] = (ri >= 0 && own) ? (long long)__ldcg(ring_at(P, ri, p, tprev)) : 0ll;
+      rv2[r] = (PD == 2 && ri >= 0 && own && L > 1) ? (long long)__ldcg(ring_at(P, ri, p, tn)) : 0ll;
     }
   }
   for (uint32_t j = 0; j < L; j++) {
@@ -822,12 +829,12 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
       cur[r] = rv[r];
       const int ri = P.lin_of_rec[r];
       if (ri >= 0) {
-        if (own && rv[r]) __stcg(P.ring + ((size_t)ri * n + p) * S + tprev, 0ull);
+        if (own && rv[r]) __stcg(ring_at(P, ri, p, tprev), 0ull);
         if constexpr (PD == 2) {
           rv[r] = rv2[r];
-          rv2[r] = (own && j + 2 < L) ? (long long)__ldcg(P.ring + ((size_t)ri * n + p) * S + ((tm + 1u) & mask)) : 0ll;
+          rv2[r] = (own && j + 2 < L) ? (long long)__ldcg(ring_at(P, ri, p, (tm + 1u) & mask)) : 0ll;
         } else {
-          rv[r] = (own && j + 1 < L) ? (long long)__ldcg(P.ring + ((size_t)ri * n + p) * S + tm) : 0ll;
+          rv[r] = (own && j + 1 < L) ? (long long)__ldcg(ring_at(P, ri, p, tm)) : 0ll;
         }
       }
     }
@@ -1090,7 +1097,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
   __shared__ uint32_t f_j[kT1F], f_n, nf_j[kT1F], nf_n;
   const Blk1 me = P.b1[blockIdx.x];
   const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  const uint32_t n = P.n, S = P.slots, mask = P.mask, NT = me.ntrk, np = me.np;
+  const uint32_t n = P.n, mask = P.mask, NT = me.ntrk, np = me.np;
   // shared-memory layout (16-byte aligned pieces first); the NMDA copies are
   // double-buffered by step parity: buffer s & 1 holds the values after
   // step t0 + s - 1
@@ -1260,7 +1267,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
         const int ri = P.lin_of_rec[r];
         if (ri >= 0 && own) {
           if (s == 0) {  // deliveries of the step before this launch: the ring
-            long long *slot = (long long *)P.ring + ((size_t)ri * n + p) * S + ((uint32_t)(t - 1u) & mask);
+            long long *slot = (long long *)ring_at(P, ri, p, (uint32_t)(t - 1u) & mask);
             rv[r] = __ldcg(slot);
             if (rv[r]) __stcg(slot, 0ll);
           } else {
@@ -1359,7 +1366,7 @@ __device__ __forceinline__ void params_to_smem(Params &Psh, const Params *__rest
 }
 
 template <class T, int U>
-__global__ void __launch_bounds__(kThreads, 3) k_tile_pull(const Params *__restrict__ Ps,
+__global__ void __launch_bounds__(kThreads, U == 4 ? 4 : 3) k_tile_pull(const Params *__restrict__ Ps,
                                                           const IvTile *__restrict__ tiles, uint32_t bs,
                                                           uint32_t L) {
   __shared__ __align__(16) Params Psh;
