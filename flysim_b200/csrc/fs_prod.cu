@@ -127,7 +127,7 @@ struct Params {
   const uint32_t *gv_row, *gv_ent;
   uint32_t gv_n;
   float *gv_st, *gv_xt;  // [steps][gv_n]
-  uint32_t *t1_cnt;      // [2] spikes listed in the step of each parity
+  uint32_t *t1_cnt;      // [4] spikes listed in step t, slot t mod 4
   uint4 *t1_list;        // [2][n][2] (id, inc, c0, c1), (c2, c3, 0, 0)
 };
 
@@ -161,55 +161,47 @@ __device__ __forceinline__ unsigned long long *ring_at(const Params &P, int ri, 
 }
 
 // ---- bounded grid barrier ---------------------------------------------------
-// Over the `count` blocks that share `bar` (the whole grid, or the blocks of
-// one network instance in a batch).  bar[0] counts arrivals, bar[32] (its
-// own 128-byte line) is the generation the waiting blocks poll; the last
-// block to arrive resets the count and advances the generation.  Ordering
-// (PTX memory model): after bar.sync, thread 0's acq_rel arrival releases
-// the whole block's writes (release is cumulative) and, for the last block,
-// acquires every earlier arrival's; the last block publishes the count reset
-// and all writes with a release add on the generation, which the others
-// observe with relaxed polls followed by one acquire fence; the closing
-// bar.sync hands that on to the block.  Every wait is bounded: after ~2^24
-// polls the block sets the error word and all blocks leave.
-__device__ __forceinline__ unsigned int ld_relaxed_gpu(const unsigned int *p) {
-  unsigned int v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+// Over the `count` blocks that share `bar` (the whole grid).  The first 8
+// bytes of bar are a 64-bit arrival counter that the host zeroes before each
+// launch and that only grows: barrier k of a launch is passed when the
+// counter reaches k * count.  Each block's thread 0, after bar.sync (which
+// orders the block's writes before it), adds its arrival with a release
+// reduction and polls the counter with acquire loads; a load that sees the
+// full count synchronises with every arrival (the reductions form one
+// release sequence), and the closing bar.sync hands that on to the block.
+// No block resets anything and there is no second hop through a
+// generation word.  Every wait is bounded: after ~2^24 polls the block sets
+// the error word and all blocks leave.  `target` is thread 0's count of the
+// arrivals expected so far.
+__device__ __forceinline__ unsigned long long ld_acquire_gpu(const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ unsigned int atom_add_acq_rel_gpu(unsigned int *p, unsigned int v) {
-  unsigned int old;
-  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-  return old;
+__device__ __forceinline__ void red_release_gpu(unsigned long long *p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
-__device__ __forceinline__ void red_release_gpu(unsigned int *p, unsigned int v) {
-  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ void fence_acquire_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
-__device__ __forceinline__ bool grid_sync(unsigned int *bar, int *err, uint32_t count,
-                                          unsigned int limit = 1u << 24) {
-  __syncthreads();
-  if (count <= 1) return *(volatile int *)err == 0;
-  if (threadIdx.x == 0) {
-    unsigned int *gen = bar + 32;
-    const unsigned int g = ld_relaxed_gpu(gen);
-    const unsigned int arrived = atom_add_acq_rel_gpu(bar, 1u);
-    if (arrived == count - 1) {
-      atomicExch(bar, 0u);
-      red_release_gpu(gen, 1u);
-    } else {
-      unsigned int spins = 0;
-      while (ld_relaxed_gpu(gen) == g) {
-        if (*(volatile int *)err) break;
-        if (++spins > limit) {
-          atomicExch(err, 2);
-          break;
-        }
-      }
-      fence_acquire_gpu();
+__device__ __forceinline__ bool arrive_and_wait(unsigned int *bar, int *err, uint32_t count,
+                                                unsigned long long &target, unsigned int limit) {
+  unsigned long long *ctr = (unsigned long long *)bar;
+  target += count;
+  red_release_gpu(ctr, 1ull);
+  unsigned int spins = 0;
+  while (ld_acquire_gpu(ctr) < target) {
+    if (*(volatile int *)err) return false;
+    if (++spins > limit) {
+      atomicExch(err, 2);
+      return false;
     }
   }
+  return true;
+}
+
+__device__ __forceinline__ bool grid_sync(unsigned int *bar, int *err, uint32_t count, unsigned long long &target,
+                                          unsigned int limit = 1u << 24) {
+  __syncthreads();
+  if (count > 1 && threadIdx.x == 0) arrive_and_wait(bar, err, count, target, limit);
   __syncthreads();
   return *(volatile int *)err == 0;
 }
@@ -982,6 +974,7 @@ __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32
   __shared__ TileBufs<T> B;
   PhaseClock pc;
   pc.start(P);
+  unsigned long long target = 0;  // barrier arrivals so far (thread 0)
   if (threadIdx.x == 0) B.l_n = 0;
   __syncthreads();
   uint32_t s = 0;
@@ -998,7 +991,7 @@ __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32
     }
     s = iv_end;
     if (s < P.nsteps) {
-      if (!grid_sync(P.bar, P.err, nblk)) return;
+      if (!grid_sync(P.bar, P.err, nblk, target)) return;
       pc.mark(4);
     }
   }
@@ -1054,35 +1047,15 @@ __device__ __forceinline__ int find_sorted(const uint32_t *a, uint32_t n, uint32
   return (lo < n && a[lo] == x) ? (int)lo : -1;
 }
 
-// Grid barrier of k_prod1: as grid_sync, and the last block to arrive also
-// zeroes *reset (the spike count of the step after next) before releasing
-// the others; threads of warps 1.. run work() while thread 0 waits.
+// Grid barrier of k_prod1: as grid_sync, with threads of warps 1.. running
+// work() while thread 0 waits.
 template <class F>
-__device__ __forceinline__ bool grid_sync_work(unsigned int *bar, int *err, uint32_t count, uint32_t *reset,
-                                               F &&work, unsigned int limit = 1u << 24) {
+__device__ __forceinline__ bool grid_sync_work(unsigned int *bar, int *err, uint32_t count,
+                                               unsigned long long &target, F &&work,
+                                               unsigned int limit = 1u << 24) {
   __syncthreads();
-  if (count <= 1) {
-    if (threadIdx.x == 0) *reset = 0u;
-    else if (threadIdx.x >= 32) work();
-  } else if (threadIdx.x == 0) {
-    unsigned int *gen = bar + 32;
-    const unsigned int g = ld_relaxed_gpu(gen);
-    const unsigned int arrived = atom_add_acq_rel_gpu(bar, 1u);
-    if (arrived == count - 1) {
-      *(volatile uint32_t *)reset = 0u;
-      atomicExch(bar, 0u);
-      red_release_gpu(gen, 1u);
-    } else {
-      unsigned int spins = 0;
-      while (ld_relaxed_gpu(gen) == g) {
-        if (*(volatile int *)err) break;
-        if (++spins > limit) {
-          atomicExch(err, 2);
-          break;
-        }
-      }
-      fence_acquire_gpu();
-    }
+  if (threadIdx.x == 0) {
+    if (count > 1) arrive_and_wait(bar, err, count, target, limit);
   } else if (threadIdx.x >= 32) {
     work();
   }
@@ -1147,11 +1120,16 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
   }
   PhaseClock pc;
   pc.start(P);
+  unsigned long long target = 0;  // barrier arrivals so far (thread 0)
   __syncthreads();
   pc.mark(5);
   for (uint32_t s = 0; s < P.nsteps; s++) {
     const uint64_t t = P.t0 + s;
     float *X = (s & 1u) ? cx1 : cx0, *Sv = (s & 1u) ? cs1 : cs0;
+    // spike counts rotate over four slots: the slot of step t + 2 was last
+    // read in step t - 1, so it can be emptied now (every append to it comes
+    // after two more barriers)
+    if (blockIdx.x == 0 && tid == 0) __stcg(P.t1_cnt + ((uint32_t)(t + 2u) & 3u), 0u);
     if (s > 0) {
       // ---- spikes of step t - 1 ----
       // the buffer of this step already holds every copy advanced as if its
@@ -1161,6 +1139,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
       const float *Xo = (s & 1u) ? cx0 : cx1, *So = (s & 1u) ? cs0 : cs1;
       const uint32_t par = (uint32_t)(t - 1u) & 1u;
       const uint4 *lst = P.t1_list + (size_t)par * n * 2;
+      const uint32_t cslot = (uint32_t)(t - 1u) & 3u;
       // the first pass's entries are loaded with the count (one round trip;
       // entries past the count are ignored)
       uint4 a0 = make_uint4(0u, 0u, 0u, 0u), b0 = a0;
@@ -1168,7 +1147,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
         a0 = __ldcg(lst + 2 * (size_t)tid);
         b0 = __ldcg(lst + 2 * (size_t)tid + 1);
       }
-      const uint32_t cnt = __ldcg(P.t1_cnt + par);
+      const uint32_t cnt = __ldcg(P.t1_cnt + cslot);
       for (uint32_t c0 = 0; c0 < cnt; c0 += kT1F) {
         if (tid == 0) {
           f_n = 0;
@@ -1287,7 +1266,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
         const uint32_t par = (uint32_t)t & 1u;
         const int leader = __ffs(m) - 1;
         uint32_t base = 0;
-        if ((int)lane == leader) base = atomicAdd(P.t1_cnt + par, (uint32_t)__popc(m));
+        if ((int)lane == leader) base = atomicAdd(P.t1_cnt + ((uint32_t)t & 3u), (uint32_t)__popc(m));
         base = __shfl_sync(fsd::kFull, base, leader);
         if (spk) {
           uint4 *e = P.t1_list + ((size_t)par * n + base + __popc(m & ((1u << lane) - 1u))) * 2;
@@ -1318,7 +1297,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
       // spiked (the listed spikes are redone after the barrier)
       const uint64_t tn = t + 1;
       float *Xn = (s & 1u) ? cx0 : cx1, *Sn = (s & 1u) ? cs0 : cs1;
-      const bool ok = grid_sync_work(P.bar, P.err, gridDim.x, P.t1_cnt + ((uint32_t)(t + 1u) & 1u), [&]() {
+      const bool ok = grid_sync_work(P.bar, P.err, gridDim.x, target, [&]() {
         for (uint32_t qq = tid - 32; qq < np; qq += kT1 - 32) {
           float gv = 0.0f;
           d_hits[qq] = (uint8_t)draw_one<float>(P, me.post0 + qq, tn, gv);
@@ -1563,7 +1542,7 @@ int launch(Prod *p, uint32_t nsteps, bool want_bits, bool wantV, cudaStream_t st
     }
     p->ev.push_back({a, b});
   }
-  if (p->single && cudaMemsetAsync(P.t1_cnt, 0, 8, st) != cudaSuccess) {
+  if (p->single && cudaMemsetAsync(P.t1_cnt, 0, 16, st) != cudaSuccess) {
     err = "memset";
     return FS_ERR_CUDA;
   }
@@ -2178,7 +2157,7 @@ static int prod_create_from(Prod **out, const fs_net_desc *d, const fs_run_opts 
         UPF(t1_ew, S1.ew.data(), S1.ew.size());
         UPF(t1_cls_tab, S1.tab.data(), S1.tab.size());
         if ((rc = dup(p, (uint16_t **)&P.t1_eidx, S1.eidx.data(), S1.eidx.size(), st, err))) goto fail;
-        if ((rc = dup(p, &P.t1_cnt, (const uint32_t *)nullptr, 2, st, err))) goto fail;
+        if ((rc = dup(p, &P.t1_cnt, (const uint32_t *)nullptr, 4, st, err))) goto fail;
         if ((rc = dup(p, &P.t1_list, (const uint4 *)nullptr, (size_t)4 * n, st, err))) goto fail;
         P.t1_ncls = (uint32_t)(S1.tab.size() / 3);
         P.t1_smem = S1.smem;
@@ -2905,7 +2884,10 @@ int tiles_solo_launch(Prod *p, const Params &P, uint32_t nsteps, cudaStream_t st
 // One block waits at a barrier of two blocks that the second never reaches:
 // the bounded wait gives up after `limit` polls, sets the error word and
 // returns, and the context stays usable.
-__global__ void k_barrier_probe(unsigned int *bar, int *err, unsigned int limit) { grid_sync(bar, err, 2, limit); }
+__global__ void k_barrier_probe(unsigned int *bar, int *err, unsigned int limit) {
+  unsigned long long target = 0;
+  grid_sync(bar, err, 2, target, limit);
+}
 
 int prod_barrier_probe(unsigned int limit, int *err_word, std::string &err) {
   unsigned int *bar = nullptr;
