@@ -1047,6 +1047,27 @@ __device__ __forceinline__ int find_sorted(const uint32_t *a, uint32_t n, uint32
   return (lo < n && a[lo] == x) ? (int)lo : -1;
 }
 
+// Deliveries of a pass of listed spikes onto a block (k_prod1): warp w of
+// nw takes listed spikes w, w + nw, ... and walks the spike's synapse row
+// onto the block's posts, adding w * c (receptor gain applied) as 2^-40
+// fixed point into the per-post accumulators.
+constexpr uint32_t kDelW = 4;  // warps that deliver the last pass
+__device__ __forceinline__ void deliver_listed(const Params &P, const Blk1 &me, uint32_t nf, const uint32_t *f_j,
+                                               const float (*f_c)[4], const uint32_t *lrow, long long *acc,
+                                               uint32_t w, uint32_t lane, uint32_t nw) {
+  for (uint32_t k = w; k < nf; k += nw) {
+    const uint32_t j = f_j[k];
+    for (uint32_t e = lrow[j] + lane; e < lrow[j + 1]; e += 32) {
+      const uint32_t code = __ldg(P.t1_lin + me.l0 + e);
+      const float wt = __ldg(P.t1_linw + me.l0 + e);
+      const uint32_t r = code >> 16, ql = code & 0xffffu;
+      const float cv = f_c[k][r] * P.rg[r];
+      const long long fx = __double2ll_rn((double)(wt * cv) * kFix);
+      atomicAdd((unsigned long long *)&acc[(size_t)P.lin_of_rec[r] * kT1 + ql], (unsigned long long)fx);
+    }
+  }
+}
+
 // Grid barrier of k_prod1: as grid_sync, with threads of warps 1.. running
 // work() while thread 0 waits.
 template <class F>
@@ -1067,7 +1088,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
   extern __shared__ __align__(16) unsigned char sm1[];
   __shared__ float gn[kT1], d_gauss[kT1], f_c[kT1F][4], nf_inc[kT1F];
   __shared__ uint8_t d_hits[kT1];
-  __shared__ uint32_t f_j[kT1F], f_n, nf_j[kT1F], nf_n;
+  __shared__ uint32_t f_j[kT1F], f_n, nf_j[kT1F], nf_n, next_post;
   const Blk1 me = P.b1[blockIdx.x];
   const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const uint32_t n = P.n, mask = P.mask, NT = me.ntrk, np = me.np;
@@ -1121,6 +1142,10 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
   PhaseClock pc;
   pc.start(P);
   unsigned long long target = 0;  // barrier arrivals so far (thread 0)
+  if (tid == 0) {
+    f_n = 0;
+    next_post = 0;
+  }
   __syncthreads();
   pc.mark(5);
   for (uint32_t s = 0; s < P.nsteps; s++) {
@@ -1183,17 +1208,12 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
           X[j] = xv;
           Sv[j] = sv;
         }
-        // one warp per listed spike walks its synapses onto this block
-        for (uint32_t k = wid; k < f_n; k += kT1 / 32) {
-          const uint32_t j = f_j[k];
-          for (uint32_t e = lrow[j] + lane; e < lrow[j + 1]; e += 32) {
-            const uint32_t code = __ldg(P.t1_lin + me.l0 + e);
-            const float w = __ldg(P.t1_linw + me.l0 + e);
-            const uint32_t r = code >> 16, ql = code & 0xffffu;
-            const float cv = f_c[k][r] * P.rg[r];
-            const long long fx = __double2ll_rn((double)(w * cv) * kFix);
-            atomicAdd((unsigned long long *)&acc[(size_t)P.lin_of_rec[r] * kT1 + ql], (unsigned long long)fx);
-          }
+        // the deliveries of all but the last pass (the last pass's are made
+        // by the first warps while the others start the NMDA sums)
+        if (c0 + kT1F < cnt) {
+          deliver_listed(P, me, f_n, f_j, f_c, lrow, acc, wid, lane, kT1 / 32);
+          __syncthreads();
+          if (tid == 0) f_n = 0;
         }
         __syncthreads();
       }
@@ -1201,10 +1221,18 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
       pc.mark(1);
     }
     // ---- NMDA sums of the block's posts (order of nmda_pull1_f32) ----
-    // a warp takes two posts at once, each summed lane-strided with four
-    // edges loaded ahead, then both butterflies
-    for (uint32_t qa = wid; qa < np; qa += kT1 / 16) {
-      const uint32_t qb = qa + kT1 / 32;
+    // the first kDelW warps deliver the last pass's listed spikes (their
+    // synapse rows come from L2) and then join; every warp takes posts two
+    // at a time from a shared counter, sums each lane-strided with four
+    // edges loaded ahead, then both butterflies (any warp gives the same
+    // sums)
+    if (wid < kDelW) deliver_listed(P, me, f_n, f_j, f_c, lrow, acc, wid, lane, kDelW);
+    for (;;) {
+      uint32_t qa = 0;
+      if (lane == 0) qa = atomicAdd(&next_post, 2u);
+      qa = __shfl_sync(fsd::kFull, qa, 0);
+      if (qa >= np) break;
+      const uint32_t qb = qa + 1;
       const uint32_t ea0 = erow[qa], ea1 = erow[qa + 1];
       const uint32_t eb0 = qb < np ? erow[qb] : 0u, eb1 = qb < np ? erow[qb + 1] : 0u;
       const uint32_t len = max(ea1 - ea0, eb1 - eb0);
@@ -1237,6 +1265,11 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
     }
     __syncthreads();
     pc.mark(2);
+    // (the pass counters are reset behind the barrier above, for the next step)
+    if (tid == 0) {
+      f_n = 0;
+      next_post = 0;
+    }
     // ---- the neurons' step ----
     if (active) {
       long long rv[4];
