@@ -416,9 +416,10 @@ def main():
         line = {"profile_steps": args.profile_steps, "stats": eng.stats(), "layout": eng.layout()}
         if args.phase_clock:
             ph = eng.phase_times().astype(np.float64) / args.profile_steps
-            names = (["lists+deliveries", "nmda copies", "nmda sums", "neuron steps", "barrier", "set-up"]
+            names = (["list lookups", "nmda copies", "deliveries+nmda sums", "neuron steps", "barrier rest",
+                      "set-up", "barrier wait (thread 0)"]
                      if eng.layout()["kernel"] == "single_step" else
-                     ["nmda pull", "drive draws", "neuron steps", "pushes", "barrier", "-"])
+                     ["nmda pull", "drive draws", "neuron steps", "pushes", "barrier", "-", "-"])
             line["cycles_per_timestep"] = {nm: {"mean": round(float(ph[:, k].mean()), 1),
                                                 "max": round(float(ph[:, k].max()), 1)}
                                            for k, nm in enumerate(names) if nm != "-"}

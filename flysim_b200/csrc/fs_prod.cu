@@ -1072,11 +1072,12 @@ __device__ __forceinline__ void deliver_listed(const Params &P, const Blk1 &me, 
 // work() while thread 0 waits.
 template <class F>
 __device__ __forceinline__ bool grid_sync_work(unsigned int *bar, int *err, uint32_t count,
-                                               unsigned long long &target, F &&work,
+                                               unsigned long long &target, PhaseClock &pc, F &&work,
                                                unsigned int limit = 1u << 24) {
   __syncthreads();
   if (threadIdx.x == 0) {
     if (count > 1) arrive_and_wait(bar, err, count, target, limit);
+    pc.mark(6);  // thread 0's wait for the other blocks
   } else if (threadIdx.x >= 32) {
     work();
   }
@@ -1330,19 +1331,31 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
       // spiked (the listed spikes are redone after the barrier)
       const uint64_t tn = t + 1;
       float *Xn = (s & 1u) ? cx0 : cx1, *Sn = (s & 1u) ? cs0 : cs1;
-      const bool ok = grid_sync_work(P.bar, P.err, gridDim.x, target, [&]() {
+      const bool ok = grid_sync_work(P.bar, P.err, gridDim.x, target, pc, [&]() {
         for (uint32_t qq = tid - 32; qq < np; qq += kT1 - 32) {
           float gv = 0.0f;
           d_hits[qq] = (uint8_t)draw_one<float>(P, me.post0 + qq, tn, gv);
           d_gauss[qq] = gv;
         }
-        for (uint32_t j = tid - 32; j < NT; j += kT1 - 32) {
-          const uint32_t c = cls[j];
-          if (c != 255) {
-            float xv = X[j], sv = Sv[j];
-            nmda_pre_step<float>(xv, sv, false, 1.0f, ctab[3 * c], ctab[3 * c + 1], ctab[3 * c + 2]);
-            Xn[j] = xv;
-            Sn[j] = sv;
+        if (P.t1_ncls == 1) {  // one class (the usual case): its constants in registers
+          const float k0 = ctab[0], k1 = ctab[1], k2 = ctab[2];
+          for (uint32_t j = tid - 32; j < NT; j += kT1 - 32) {
+            if (cls[j] != 255) {
+              float xv = X[j], sv = Sv[j];
+              nmda_pre_step<float>(xv, sv, false, 1.0f, k0, k1, k2);
+              Xn[j] = xv;
+              Sn[j] = sv;
+            }
+          }
+        } else {
+          for (uint32_t j = tid - 32; j < NT; j += kT1 - 32) {
+            const uint32_t c = cls[j];
+            if (c != 255) {
+              float xv = X[j], sv = Sv[j];
+              nmda_pre_step<float>(xv, sv, false, 1.0f, ctab[3 * c], ctab[3 * c + 1], ctab[3 * c + 2]);
+              Xn[j] = xv;
+              Sn[j] = sv;
+            }
           }
         }
       });
@@ -3030,9 +3043,10 @@ int prod_debug_drive(Prod *p, uint64_t t0, uint32_t nsteps, uint32_t first, uint
 }
 
 // Phase clock: per block, SM cycles spent in each phase of the persistent
-// kernels since it was switched on (k_prod1: 0 spike lists and deliveries,
-// 1 NMDA copies, 2 NMDA sums, 3 neuron steps and spike lists, 4 grid
-// barrier; k_prod: 0 NMDA pull, 1 drive draws, 2 neuron steps, 3 pushes,
+// kernels since it was switched on (k_prod1: 0 spike-list lookups, 1 NMDA
+// copies of listed spikes, 2 last deliveries and NMDA sums, 3 neuron steps
+// and spike lists, 6 thread 0's barrier wait, 4 the rest of the barrier,
+// 5 set-up; k_prod: 0 NMDA pull, 1 drive draws, 2 neuron steps, 3 pushes,
 // 4 grid barrier).
 int prod_phase_clock(Prod *p, int enable, cudaStream_t st, std::string &err) {
   const uint32_t nb = std::max(p->blocks, p->b1_blocks);

@@ -317,8 +317,10 @@ int fs_debug_single_step_plan(const fs_net_desc *desc, uint32_t sm_count, uint64
  * the reference).  fs_debug_phase_clock(h, 1) zeroes and switches on
  * per-block counters of SM cycles per phase, 0 switches them off;
  * fs_debug_phase_times copies up to cap counters, [blocks][8], and the
- * block count.  Phases: single-step kernel 0 spike lists and deliveries,
- * 1 NMDA copies, 2 NMDA sums, 3 neuron steps, 4 grid barrier, 5 set-up;
+ * block count.  Phases: single-step kernel 0 spike-list lookups, 1 NMDA
+ * copies of listed spikes, 2 last deliveries and NMDA sums, 3 neuron steps,
+ * 6 thread 0's wait at the grid barrier, 4 the rest of the barrier (the
+ * other warps' drive draws and NMDA copies), 5 set-up;
  * interval kernel 0 NMDA pull, 1 drive draws, 2 neuron steps, 3 pushes,
  * 4 grid barrier.  The tile kernels have no phase clock. */
 int fs_debug_phase_clock(fs_handle *h, int enable);
