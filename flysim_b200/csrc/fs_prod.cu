@@ -127,8 +127,10 @@ struct Params {
   const uint32_t *gv_row, *gv_ent;
   uint32_t gv_n;
   float *gv_st, *gv_xt;  // [steps][gv_n]
-  uint32_t *t1_cnt;      // [4] spikes listed in step t, slot t mod 4
-  uint4 *t1_list;        // [2][n][2] (id, inc, c0, c1), (c2, c3, 0, 0)
+  uint32_t *t1_cnt;      // [4] overflow entries of step t, slot t mod 4
+  uint32_t t1_slots;     // entries per block region of a step's list
+  uint4 *t1_list;        // [2][blocks][t1_slots][2] (id, inc, c0, c1), (c2, c3, step + 1, 0)
+  uint4 *t1_ovf;         // [2][n][2] the overflow lists
 };
 
 // Block plan of k_prod1: posts [post0, post0 + np), tracked neurons [trk0,
@@ -782,12 +784,13 @@ __device__ __forceinline__ bool neuron_step(const Params &P, const NeuronPar<T> 
 }
 
 // Spike outputs of a warp's step: the per-step bitmap and count, the total.
+// total = false: the caller adds its spikes to the total itself (once).
 __device__ __forceinline__ void spike_outputs(const Params &P, uint32_t m, bool spk, uint32_t p, uint32_t s,
-                                              uint32_t lane) {
+                                              uint32_t lane, bool total = true) {
   if (spk && P.bits) atomicOr(P.bits + (size_t)s * P.words + (p >> 5), 1u << (p & 31));
   if (lane == 0) {
     if (P.counts) atomicAdd(P.counts + s, (unsigned)__popc(m));
-    atomicAdd(P.spike_total, (unsigned long long)__popc(m));
+    if (total) atomicAdd(P.spike_total, (unsigned long long)__popc(m));
   }
 }
 
@@ -1120,7 +1123,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
   extern __shared__ __align__(16) unsigned char sm1[];
   __shared__ float gn[kT1], d_gauss[kT1], f_c[kT1F][4], nf_inc[kT1F];
   __shared__ uint8_t d_hits[kT1];
-  __shared__ uint32_t f_j[kT1F], f_n, nf_j[kT1F], nf_n, next_post;
+  __shared__ uint32_t f_j[kT1F], f_n, nf_j[kT1F], nf_n, next_post, blk_n;
   const Blk1 me = P.b1[blockIdx.x];
   const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const uint32_t n = P.n, mask = P.mask, NT = me.ntrk, np = me.np;
@@ -1187,6 +1190,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
     // read in step t - 1, so it can be emptied now (every append to it comes
     // after two more barriers)
     if (blockIdx.x == 0 && tid == 0) __stcg(P.t1_cnt + ((uint32_t)(t + 2u) & 3u), 0u);
+    if (tid == 0) blk_n = 0;  // this step's spikes of the block (read after the NMDA sums' barrier)
     if (s > 0) {
       // ---- spikes of step t - 1 ----
       // the buffer of this step already holds every copy advanced as if its
@@ -1195,16 +1199,18 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
       // synapses onto this block are delivered
       const float *Xo = (s & 1u) ? cx0 : cx1, *So = (s & 1u) ? cs0 : cs1;
       const uint32_t par = (uint32_t)(t - 1u) & 1u;
-      const uint4 *lst = P.t1_list + (size_t)par * n * 2;
-      const uint32_t cslot = (uint32_t)(t - 1u) & 3u;
-      // the first pass's entries are loaded with the count (one round trip;
-      // entries past the count are ignored)
+      const uint32_t tag = (uint32_t)(t - 1u) + 1u;  // entries of step t - 1 carry it
+      const uint32_t nreg = gridDim.x * P.t1_slots;   // block-region entries (<= kT1F)
+      const uint4 *reg = P.t1_list + (size_t)par * nreg * 2;
+      const uint4 *ovf = P.t1_ovf + (size_t)par * n * 2;
+      // the regions' entries are loaded with the overflow count (one round
+      // trip); stale entries carry another step's tag
       uint4 a0 = make_uint4(0u, 0u, 0u, 0u), b0 = a0;
-      if (tid < n) {
-        a0 = __ldcg(lst + 2 * (size_t)tid);
-        b0 = __ldcg(lst + 2 * (size_t)tid + 1);
+      if (tid < nreg) {
+        a0 = __ldcg(reg + 2 * (size_t)tid);
+        b0 = __ldcg(reg + 2 * (size_t)tid + 1);
       }
-      const uint32_t cnt = __ldcg(P.t1_cnt + cslot);
+      const uint32_t cnt = nreg + __ldcg(P.t1_cnt + ((uint32_t)(t - 1u) & 3u));
       for (uint32_t c0 = 0; c0 < cnt; c0 += kT1F) {
         if (tid == 0) {
           f_n = 0;
@@ -1213,8 +1219,13 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
         __syncthreads();
         const uint32_t i = c0 + tid;
         if (tid < kT1F && i < cnt) {
-          const uint4 a = c0 == 0 ? a0 : __ldcg(lst + 2 * (size_t)i), b = c0 == 0 ? b0 : __ldcg(lst + 2 * (size_t)i + 1);
-          const int j = find_sorted(gid, NT, a.x);
+          uint4 a = a0, b = b0;
+          if (i >= nreg) {  // an overflow entry: every one is of step t - 1
+            a = __ldcg(ovf + 2 * (size_t)(i - nreg));
+            b = __ldcg(ovf + 2 * (size_t)(i - nreg) + 1);
+            b.z = tag;
+          }
+          const int j = b.z == tag ? find_sorted(gid, NT, a.x) : -1;
           if (j >= 0) {
             if (cls[j] != 255) {
               const uint32_t k = atomicAdd(&nf_n, 1u);
@@ -1327,16 +1338,26 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
       if (own && P.gv_row) gv_write<float>(P, p, s, st);
       const uint32_t m = __ballot_sync(fsd::kFull, spk);
       if (m) {
-        spike_outputs(P, m, spk, p, s, lane);
+        spike_outputs(P, m, spk, p, s, lane, false);
+        // the spike goes to this block's region of the step's list (a
+        // shared-memory counter); past the region's slots, to the overflow
+        // list (a global counter)
         const uint32_t par = (uint32_t)t & 1u;
         const int leader = __ffs(m) - 1;
         uint32_t base = 0;
-        if ((int)lane == leader) base = atomicAdd(P.t1_cnt + ((uint32_t)t & 3u), (uint32_t)__popc(m));
+        if ((int)lane == leader) base = atomicAdd(&blk_n, (uint32_t)__popc(m));
         base = __shfl_sync(fsd::kFull, base, leader);
         if (spk) {
-          uint4 *e = P.t1_list + ((size_t)par * n + base + __popc(m & ((1u << lane) - 1u))) * 2;
+          const uint32_t k = base + __popc(m & ((1u << lane) - 1u));
+          uint4 *e;
+          if (k < P.t1_slots) {
+            e = P.t1_list + (((size_t)par * gridDim.x + blockIdx.x) * P.t1_slots + k) * 2;
+          } else {
+            const uint32_t o = atomicAdd(P.t1_cnt + ((uint32_t)t & 3u), 1u);
+            e = P.t1_ovf + ((size_t)par * n + o) * 2;
+          }
           __stcg(e, make_uint4(p, __float_as_uint(inc), __float_as_uint(cinc[0]), __float_as_uint(cinc[1])));
-          __stcg(e + 1, make_uint4(__float_as_uint(cinc[2]), __float_as_uint(cinc[3]), 0u, 0u));
+          __stcg(e + 1, make_uint4(__float_as_uint(cinc[2]), __float_as_uint(cinc[3]), (uint32_t)t + 1u, 0u));
         }
         if (s + 1 == P.nsteps) {
           // the launch's last step: its spikes go into the delay ring, which
@@ -1397,6 +1418,13 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
   if (own) {
     store_neuron<float>(P, p, st);
     if (P.nspk && nsp) P.nspk[p] += nsp;
+  }
+  // the launch's spikes, added to the total once per warp
+  if (active) {
+    uint32_t w = nsp;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) w += __shfl_xor_sync(fsd::kFull, w, o);
+    if (lane == 0 && w) atomicAdd(P.spike_total, (unsigned long long)w);
   }
 }
 
@@ -1619,7 +1647,11 @@ int launch(Prod *p, uint32_t nsteps, bool want_bits, bool wantV, cudaStream_t st
     }
     p->ev.push_back({a, b});
   }
-  if (p->single && cudaMemsetAsync(P.t1_cnt, 0, 16, st) != cudaSuccess) {
+  // the single-step kernel's lists start empty (region entries are told
+  // apart by their step tag; a reset or a restored checkpoint moves the
+  // step counter back)
+  if (p->single && (cudaMemsetAsync(P.t1_cnt, 0, 16, st) != cudaSuccess ||
+                    cudaMemsetAsync(P.t1_list, 0, (size_t)2 * p->b1_blocks * P.t1_slots * 32, st) != cudaSuccess)) {
     err = "memset";
     return FS_ERR_CUDA;
   }
@@ -2235,7 +2267,10 @@ static int prod_create_from(Prod **out, const fs_net_desc *d, const fs_run_opts 
         UPF(t1_cls_tab, S1.tab.data(), S1.tab.size());
         if ((rc = dup(p, (uint16_t **)&P.t1_eidx, S1.eidx.data(), S1.eidx.size(), st, err))) goto fail;
         if ((rc = dup(p, &P.t1_cnt, (const uint32_t *)nullptr, 4, st, err))) goto fail;
-        if ((rc = dup(p, &P.t1_list, (const uint4 *)nullptr, (size_t)4 * n, st, err))) goto fail;
+        P.t1_slots = std::min<uint32_t>(16, kT1F / (uint32_t)S1.blk.size());
+        if ((rc = dup(p, &P.t1_list, (const uint4 *)nullptr, (size_t)2 * S1.blk.size() * P.t1_slots * 2, st, err)) ||
+            (rc = dup(p, &P.t1_ovf, (const uint4 *)nullptr, (size_t)4 * n, st, err)))
+          goto fail;
         P.t1_ncls = (uint32_t)(S1.tab.size() / 3);
         P.t1_smem = S1.smem;
         p->single = true;
