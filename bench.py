@@ -309,9 +309,12 @@ def run_reference(args, rank):
     One bench step = one repeat (-rp) of a trial of FS_REF_TRIAL_MS (default
     200 ms) simulated, timed by the reference's own Run-phase timer; the
     first W repeats are discarded.  The build is FS_REF_BUILD (stock or ftz,
-    the -mdaz-ftz build of the same sources; default stock) at -t = all host
-    threads (FS_REF_THREADS overrides)."""
-    build = os.environ.get("FS_REF_BUILD", "stock")
+    the -mdaz-ftz build of the same sources) at -t = all host threads
+    (FS_REF_THREADS overrides).  The default is the fastest of the four
+    (build x -t 1 / -t all) measured on the 16-thread GPU hosts: ftz at all
+    threads (stock -t 16 0.0382, ftz -t 16 0.0426, stock -t 1 0.0099, ftz -t 1
+    0.0102 sim-s/wall-s)."""
+    build = os.environ.get("FS_REF_BUILD", "ftz")
     ref = os.path.join(ROOT, "oracle", "_ref", "flysim_ref" + ("_ftz" if build == "ftz" else ""))
     if rank != 0:
         return 0
