@@ -266,107 +266,76 @@ __device__ __forceinline__ float comp4(const float4 &q, int k) {
 template <int U>
 __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint32_t np, uint64_t tb, uint32_t L,
                                               float (*gn)[kTile], uint32_t wid, uint32_t lane) {
-  constexpr uint32_t CH = 8u * U;      // edges of a post per chunk
+  constexpr uint32_t CH = 8u * U;      // edges per warp round
   const float4 *sh = (const float4 *)P.s_hist;
   const uint32_t S4 = P.slots >> 2, qmask = S4 - 1, mask = P.mask;
   const uint32_t nvl = (L + 3u) >> 2;  // vectors needed for L steps
   const uint32_t nw = kThreads / 32;
   const uint32_t k = lane & 3u, g = lane >> 2;
   const bool kv = k < nvl;
-  if (!P.in_row) {
-    for (uint32_t i = wid * 32 + lane; i < np * L; i += nw * 32) gn[i / np][i % np] = 0.0f;
-    return;
+  uint32_t code[U];
+  float w[U];
+  auto fetch = [&](uint32_t base, uint32_t end) {
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const uint32_t eu = base + g + 8u * u;
+      code[u] = eu < end ? __ldg(P.in_code + eu) : 0u;
+      w[u] = eu < end ? __ldg(P.in_w + eu) : 0.0f;
+    }
+  };
+  uint32_t q = wid, b0 = 0, b1 = 0;
+  if (P.in_row && q < np) {
+    b0 = __ldg(P.in_row + p0 + q);
+    b1 = __ldg(P.in_row + p0 + q + 1);
+    fetch(b0, b1);
   }
-  // The warp's work is a stream of (post, chunk) items: posts wid, wid + nw,
-  // ...; chunks 0 .. max(1, ceil(edges / CH)) - 1.  Three items are in flight:
-  // the codes and weights of the item after next are loading, the windows
-  // of the next item are loading, and the current item is summed.
-  struct Cur {
-    uint32_t q, c, b0, b1, nch;
-  };
-  auto first = [&](uint32_t q) {
-    Cur r{q, 0u, 0u, 0u, 1u};
-    if (q < np) {
-      r.b0 = __ldg(P.in_row + p0 + q);
-      r.b1 = __ldg(P.in_row + p0 + q + 1);
-      r.nch = max(1u, (r.b1 - r.b0 + CH - 1) / CH);
+  for (; q < np; q += nw) {
+    const uint32_t qn = q + nw;
+    uint32_t n0 = 0, n1 = 0;
+    if (P.in_row && qn < np) {
+      n0 = __ldg(P.in_row + p0 + qn);
+      n1 = __ldg(P.in_row + p0 + qn + 1);
     }
-    return r;
-  };
-  auto next = [&](Cur r) {
-    if (r.c + 1 < r.nch) {
-      r.c++;
-      return r;
-    }
-    return first(r.q + nw);
-  };
-  auto fetch = [&](const Cur &r, uint32_t (&code)[U], float (&w)[U]) {
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    const uint32_t nch = (b1 - b0 + CH - 1) / CH;
+    for (uint32_t c = 0; c < nch; c++) {
+      const uint32_t e = b0 + c * CH + g;
+      float4 v[U];
 #pragma unroll
-    for (int u = 0; u < U; u++) {
-      const uint32_t eu = r.b0 + r.c * CH + g + 8u * u;
-      const bool ok = r.q < np && eu < r.b1;
-      code[u] = ok ? __ldg(P.in_code + eu) : 0u;
-      w[u] = ok ? __ldg(P.in_w + eu) : 0.0f;
-    }
-  };
-  auto windows = [&](const Cur &r, const uint32_t (&code)[U], float4 (&v)[U]) {
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-      const uint32_t e = r.b0 + r.c * CH + g + 8u * u;
-      const bool ok = r.q < np && kv && e < r.b1;
-      const uint32_t pre = code[u] & 0xffffffu, d = code[u] >> 24;
-      const uint32_t a = (uint32_t)(tb - 1u - d) & mask;
-      const float4 *row = sh + ((size_t)pre * kSH + (a & 3u)) * S4;
-      v[u] = ok ? __ldca(row + (((a >> 2) + k) & qmask)) : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-  };
-  Cur A = first(wid);
-  uint32_t cF[U];
-  float wF[U], wA[U];
-  float4 vA[U], vW[U];
-  fetch(A, cF, wF);
-  windows(A, cF, vA);
-#pragma unroll
-  for (int u = 0; u < U; u++) wA[u] = wF[u];
-  Cur W = next(A);
-  fetch(W, cF, wF);
-  float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-  while (A.q < np) {
-    float wW[U];
-    windows(W, cF, vW);  // the next item's windows go in flight
-#pragma unroll
-    for (int u = 0; u < U; u++) wW[u] = wF[u];
-    const Cur F = next(W);
-    fetch(F, cF, wF);    // and the codes of the one after
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-      acc[0] += wA[u] * vA[u].x;
-      acc[1] += wA[u] * vA[u].y;
-      acc[2] += wA[u] * vA[u].z;
-      acc[3] += wA[u] * vA[u].w;
-    }
-    if (A.c + 1 == A.nch) {  // the post's last chunk: quads combined, stored
-#pragma unroll
-      for (int o = 4; o < 32; o <<= 1)
-#pragma unroll
-        for (int i = 0; i < 4; i++) acc[i] += __shfl_xor_sync(fsd::kFull, acc[i], o);
-      if (lane < 4) {
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-          const uint32_t j = 4u * lane + (uint32_t)i;
-          if (j < L) gn[j][A.q] = acc[i];
-        }
+      for (int u = 0; u < U; u++) {
+        const bool ok = kv && e + 8u * u < b1;
+        const uint32_t pre = code[u] & 0xffffffu, d = code[u] >> 24;
+        const uint32_t a = (uint32_t)(tb - 1u - d) & mask;
+        const float4 *row = sh + ((size_t)pre * kSH + (a & 3u)) * S4;
+        v[u] = ok ? __ldca(row + (((a >> 2) + k) & qmask)) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
+      float wc[U];
 #pragma unroll
-      for (int i = 0; i < 4; i++) acc[i] = 0.0f;
-    }
-    A = W;
-    W = F;
+      for (int u = 0; u < U; u++) wc[u] = w[u];
+      if (c + 1 < nch) fetch(b0 + (c + 1) * CH, b1);
+      else if (qn < np) fetch(n0, n1);
 #pragma unroll
-    for (int u = 0; u < U; u++) {
-      vA[u] = vW[u];
-      wA[u] = wW[u];
+      for (int u = 0; u < U; u++) {
+        acc[0] += wc[u] * v[u].x;
+        acc[1] += wc[u] * v[u].y;
+        acc[2] += wc[u] * v[u].z;
+        acc[3] += wc[u] * v[u].w;
+      }
     }
+    if (nch == 0 && qn < np) fetch(n0, n1);
+#pragma unroll
+    for (int o = 4; o < 32; o <<= 1)
+#pragma unroll
+      for (int i = 0; i < 4; i++) acc[i] += __shfl_xor_sync(fsd::kFull, acc[i], o);
+    if (lane < 4) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const uint32_t j = 4u * lane + (uint32_t)i;
+        if (j < L) gn[j][q] = acc[i];
+      }
+    }
+    b0 = n0;
+    b1 = n1;
   }
 }
 
@@ -1450,7 +1419,7 @@ __device__ __forceinline__ void params_to_smem(Params &Psh, const Params *__rest
 }
 
 template <class T, int U>
-__global__ void __launch_bounds__(kThreads, U == 4 ? 4 : 2) k_tile_pull(const Params *__restrict__ Ps,
+__global__ void __launch_bounds__(kThreads, U == 4 ? 4 : 3) k_tile_pull(const Params *__restrict__ Ps,
                                                           const IvTile *__restrict__ tiles, uint32_t bs,
                                                           uint32_t L) {
   __shared__ __align__(16) Params Psh;
@@ -2974,7 +2943,7 @@ int tiles_solo_create(Prod *p, std::string &err) {
   p->tiles = new Tiles();
   p->tiles->fp64 = p->fp64;
   std::vector<Prod *> one{p};
-  return tiles_plan(*p->tiles, one, p->fp64 ? TileW<double>::W : kTile, 4, err);
+  return tiles_plan(*p->tiles, one, p->fp64 ? TileW<double>::W : kTile, 8, err);
 }
 
 void tiles_delete(Tiles *T) {
