@@ -420,9 +420,11 @@ def main():
         if args.phase_clock:
             ph = eng.phase_times().astype(np.float64) / args.profile_steps
             names = (["list lookups", "nmda copies", "deliveries+nmda sums", "neuron steps", "barrier rest",
-                      "set-up", "barrier wait (thread 0)"]
+                      "set-up", "barrier wait (thread 0)", "-", "lookups: entry count in (lap)",
+                      "lookups: search done (lap)", "sums: warp 0 deliveries issued (lap)",
+                      "sums: warp 0 out of posts (lap)"]
                      if eng.layout()["kernel"] == "single_step" else
-                     ["nmda pull", "drive draws", "neuron steps", "pushes", "barrier", "-", "-"])
+                     ["nmda pull", "drive draws", "neuron steps", "pushes", "barrier"])
             line["cycles_per_timestep"] = {nm: {"mean": round(float(ph[:, k].mean()), 1),
                                                 "max": round(float(ph[:, k].max()), 1)}
                                            for k, nm in enumerate(names) if nm != "-"}

@@ -521,13 +521,13 @@ class Engine:
 
     def phase_times(self) -> np.ndarray:
         """SM cycles per block and phase since the clock was switched on,
-        [blocks, 8]."""
+        [blocks, 16]."""
         nb = C.c_uint32()
         _check(lib().fs_debug_phase_times(self._h, None, 0, C.byref(nb)), self._h)
-        out = np.zeros(nb.value * 8, np.uint64)
+        out = np.zeros(nb.value * 16, np.uint64)
         _check(lib().fs_debug_phase_times(self._h, out.ctypes.data_as(C.POINTER(C.c_uint64)), out.size,
                                           C.byref(nb)), self._h)
-        return out.reshape(nb.value, 8)
+        return out.reshape(nb.value, 16)
 
     def inject_wait_failure(self):
         """Sets the device error word as a bounded wait that gave up would."""

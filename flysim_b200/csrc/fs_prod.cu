@@ -115,15 +115,18 @@ struct Params {
   // in-edges of its posts as (tracked index, weight) in CSR order, and the
   // spike lists of the last two steps
   const struct Blk1 *b1;
-  const uint32_t *t1_gid, *t1_lrow, *t1_lin, *t1_erow;
+  const uint32_t *t1_gid, *t1_lin, *t1_grow;
+  const uint16_t *t1_lrow, *t1_perm;
   const uint8_t *t1_cls;
   const float *t1_linw, *t1_ew, *t1_cls_tab;
   const uint16_t *t1_eidx;
+  const uint32_t *t1_bits;   // per block: bitmap of its tracked neurons' ids
+  const uint16_t *t1_rank;   // per block: tracked neurons in the bitmap's earlier words
   uint32_t t1_ncls, t1_smem;
   // GatingVariable output (or null): selections of neuron p are entries
   // [gv_row[p], gv_row[p+1]) of gv_ent (output column | receptor << 28)
   void *gn_buf;          // tile kernels: NMDA sums of a batch of steps, [L][n]
-  unsigned long long *phase;  // phase clock: [blocks][8] SM cycles per phase, or null
+  unsigned long long *phase;  // phase clock: [blocks][16] SM cycles per phase, or null
   const uint32_t *gv_row, *gv_ent;
   uint32_t gv_n;
   float *gv_st, *gv_xt;  // [steps][gv_n]
@@ -133,12 +136,15 @@ struct Params {
   uint4 *t1_ovf;         // [2][n][2] the overflow lists
 };
 
-// Block plan of k_prod1: posts [post0, post0 + np), tracked neurons [trk0,
-// trk0 + ntrk) of the t1 arrays (their linear rows at lrow0, ntrk + 1
-// offsets), NMDA edges [e0, e0 + ne), edge rows at erow0 (np + 1 offsets),
-// linear delivery entries from l0.
+// Block plan of k_prod1: posts [post0, post0 + np); tracked neurons [trk0,
+// trk0 + ntrk) of the per-tracked t1 arrays (their slots in t1_perm, their
+// linear rows at lrow0, ntrk + 1 offsets); NMDA edge entries [e0, e0 + ne)
+// (groups of four posts in rows of 32, the groups' first rows at grow0,
+// (np + 3) / 4 + 1 of them); linear delivery entries from l0.
 struct Blk1 {
-  uint32_t post0, np, trk0, ntrk, lrow0, e0, ne, erow0, l0, pad;
+  uint32_t post0, np, trk0, ntrk, lrow0, e0, ne, grow0, l0;
+  uint32_t bm0, w0, nwd;  // bitmap: words [w0, w0 + nwd) of the id space, at t1_bits + bm0
+  uint32_t s0, nslot;     // slot tables (t1_gid, t1_cls) at s0, nslot of them (a multiple of 32)
 };
 
 // ---- Philox-4x32-10 -------------------------------------------------------
@@ -189,23 +195,35 @@ __device__ __forceinline__ bool arrive_and_wait(unsigned int *bar, int *err, uin
   unsigned long long *ctr = (unsigned long long *)bar;
   target += count;
   red_release_gpu(ctr, 1ull);
+  // the error word is looked at every 64 polls only: a load after an acquire
+  // load waits for it, so checking it on every poll would double the time
+  // between polls
   unsigned int spins = 0;
   while (ld_acquire_gpu(ctr) < target) {
-    if (*(volatile int *)err) return false;
-    if (++spins > limit) {
-      atomicExch(err, 2);
-      return false;
+    if ((++spins & 63u) == 0u) {
+      if (*(volatile int *)err) return false;
+      if (spins > limit) {
+        atomicExch(err, 2);
+        return false;
+      }
     }
   }
   return true;
 }
 
+// A block leaves when thread 0's wait failed (its own limit, or the error
+// word set by another block); thread 0 hands the outcome to the block
+// through shared memory, so no thread reads global memory after the
+// barrier.  A block that passed a barrier which another block gave up on
+// finds the error word set while it waits at the next one (that block never
+// arrives there), so every block leaves within 64 polls of the failure.
 __device__ __forceinline__ bool grid_sync(unsigned int *bar, int *err, uint32_t count, unsigned long long &target,
                                           unsigned int limit = 1u << 24) {
+  __shared__ int ok;
   __syncthreads();
-  if (count > 1 && threadIdx.x == 0) arrive_and_wait(bar, err, count, target, limit);
+  if (threadIdx.x == 0) ok = count > 1 ? arrive_and_wait(bar, err, count, target, limit) : 1;
   __syncthreads();
-  return *(volatile int *)err == 0;
+  return ok != 0;
 }
 
 // Loads of the NMDA s history may be served by L1 (ld.global.ca): a block
@@ -340,11 +358,12 @@ __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint
 }
 
 // Single-step pull of networks whose delays are all 0 (every network in the
-// reference's own format): one warp per post, lane l summing the post's
-// edges l, l + 32, l + 64, ... in order (fused multiply-adds), then an xor
-// butterfly over 16, 8, 4, 2, 1.  The single-step persistent kernel
-// (k_prod1) sums its shared-memory copy of the same edges in the same
-// order, so a batch instance equals its solo run bit for bit.
+// reference's own format): the eight lanes of a quarter warp sum one post,
+// lane l of the quarter its edges l, l + 8, l + 16, ... in order (fused
+// multiply-adds), then an xor butterfly over 4, 2, 1.  The single-step
+// persistent kernel (k_prod1) sums its shared-memory copy of the same edges
+// in the same order, so the two kernels, and a batch instance and its solo
+// run, give the same sums bit for bit.
 __device__ __forceinline__ void nmda_pull1_f32(const Params &P, uint32_t p0, uint32_t np, uint64_t tb,
                                                float (*gn)[kTile], uint32_t wid, uint32_t lane) {
   const float *sh = (const float *)P.s_hist;
@@ -355,17 +374,20 @@ __device__ __forceinline__ void nmda_pull1_f32(const Params &P, uint32_t p0, uin
     return;
   }
   const uint32_t slot = (uint32_t)(tb - 1u) & mask;
-  for (uint32_t q = wid; q < np; q += nw) {
-    const uint32_t b0 = __ldg(P.in_row + p0 + q), b1 = __ldg(P.in_row + p0 + q + 1);
+  const uint32_t h = lane >> 3, l8 = lane & 7u;
+  for (uint32_t q0 = wid * 4u; q0 < np; q0 += nw * 4u) {
+    const uint32_t q = q0 + h;
+    const bool has = q < np;
+    const uint32_t b0 = has ? __ldg(P.in_row + p0 + q) : 0u, b1 = has ? __ldg(P.in_row + p0 + q + 1) : 0u;
     float acc = 0.0f;
-    for (uint32_t e = b0 + lane; e < b1; e += 32) {
+    for (uint32_t e = b0 + l8; e < b1; e += 8) {
       const uint32_t pre = __ldg(P.in_code + e) & 0xffffffu;
       // row 0 of the shifted copies holds slot i at element i
       acc = __fmaf_rn(__ldg(P.in_w + e), __ldca(sh + (size_t)pre * kSH * S + slot), acc);
     }
 #pragma unroll
-    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(fsd::kFull, acc, o);
-    if (lane == 0) gn[0][q] = acc;
+    for (int o = 4; o; o >>= 1) acc += __shfl_xor_sync(fsd::kFull, acc, o);
+    if (l8 == 0 && has) gn[0][q] = acc;
   }
 }
 
@@ -491,19 +513,27 @@ __device__ __forceinline__ void draw_inputs(const Params &P, uint32_t p0, uint32
 // ---- phase clock (debug aid) -------------------------------------------------
 // When P.phase is set, thread 0 of each block adds the SM cycles between
 // consecutive marks to its block's counter k (a relaxed add per mark).
+constexpr uint32_t kPhaseSlots = 16;  // counters per block
 struct PhaseClock {
   unsigned long long *out;
   long long t;
   __device__ __forceinline__ void start(const Params &P) {
-    out = (P.phase && threadIdx.x == 0) ? P.phase + (size_t)blockIdx.x * 8 : nullptr;
+    out = (P.phase && threadIdx.x == 0) ? P.phase + (size_t)blockIdx.x * kPhaseSlots : nullptr;
     if (out) t = clock64();
   }
+  // adds the cycles since the last mark to counter k and restarts the count
   __device__ __forceinline__ void mark(int k) {
     if (out) {
       const long long now = clock64();
       atomicAdd(out + k, (unsigned long long)(now - t));
       t = now;
     }
+  }
+  // adds the cycles since the last mark to counter k once `dep` is known
+  // (a branch on it comes first), without restarting the count; `dep` is
+  // never 0xffffffff at a call
+  __device__ __forceinline__ void lap(int k, uint32_t dep = 0u) {
+    if (out && dep != 0xffffffffu) atomicAdd(out + k, (unsigned long long)(clock64() - t));
   }
 };
 
@@ -512,10 +542,12 @@ struct PhaseClock {
 // advances it; the per-step arithmetic below is the single definition used
 // by the interval kernel (k_prod / k_prod_batch) and the single-step kernel
 // (k_prod1), so the two give bit-identical neurons.
+constexpr uint8_t kPjTM = 0x80;  // NeuronPar::pj: Tsodyks-Markram plasticity on (next to the receptor bits)
+
 template <class T>
 struct NeuronPar {
   uint32_t a;
-  uint8_t pj;
+  uint8_t pj;  // bit r: the neuron projects onto receptor r; kPjTM
   int32_t rf, sd;
   T vth, vreset, df, ef, dvm, cm, leak, mg;
   T vrev[5], dfs[5], extg[5];
@@ -531,9 +563,12 @@ struct NeuronState {
   uint32_t ns;
   T G[4], est[4], sp[4];
   T ex, es, xp, spre;
+  float tmu, tmx;  // Tsodyks-Markram u, x (float between steps)
 };
 
-template <class T>
+// kTM = false: the caller never runs a Tsodyks-Markram network (no
+// registers are spent on its state).
+template <class T, bool kTM = true>
 __device__ __forceinline__ void load_neuron(const Params &P, uint32_t p, NeuronPar<T> &q, NeuronState<T> &st) {
   const uint32_t n = P.n;
   q.a = P.act[p];
@@ -561,6 +596,15 @@ __device__ __forceinline__ void load_neuron(const Params &P, uint32_t p, NeuronP
   q.pdfxt = (T)__ldg(P.p_dfxt + p);
   q.pdfst = (T)__ldg(P.p_dfst + p);
   q.pefas = (T)__ldg(P.p_efas + p);
+  // the Tsodyks-Markram state lives in registers for the launch (or batch;
+  // its parameters are read-only loads of each step); a neuron without
+  // projections has no presynaptic state
+  st.tmu = st.tmx = 0.0f;
+  if (kTM && P.plast == PL_TM && q.pj && P.tm_on[p]) {
+    q.pj |= kPjTM;
+    st.tmu = P.tm_u[p];
+    st.tmx = P.tm_x[p];
+  }
   st.V = ((T *)P.V)[p];
   st.cnt = P.Count[p];
   st.ns = P.NS[p];
@@ -576,9 +620,14 @@ __device__ __forceinline__ void load_neuron(const Params &P, uint32_t p, NeuronP
   st.spre = ((T *)P.s_pre)[p];
 }
 
-template <class T>
-__device__ __forceinline__ void store_neuron(const Params &P, uint32_t p, const NeuronState<T> &st) {
+template <class T, bool kTM = true>
+__device__ __forceinline__ void store_neuron(const Params &P, uint32_t p, const NeuronPar<T> &q,
+                                             const NeuronState<T> &st) {
   const uint32_t n = P.n;
+  if (kTM && (q.pj & kPjTM)) {
+    P.tm_u[p] = st.tmu;
+    P.tm_x[p] = st.tmx;
+  }
   ((T *)P.V)[p] = st.V;
   P.Count[p] = st.cnt;
   P.NS[p] = st.ns;
@@ -610,7 +659,7 @@ __device__ __forceinline__ void nmda_pre_step(T &xp, T &spre, bool spk, T inc, T
 // per-step outputs of step s, then the presynaptic state: the increment inc of
 // a spike and, per linear receptor, c = inc + st(t-1)(1 - df) for the push.
 // Returns whether the neuron spiked.
-template <class T>
+template <class T, bool kTM = true>
 __device__ __forceinline__ bool neuron_step(const Params &P, const NeuronPar<T> &q, NeuronState<T> &st,
                                             const long long (&rv)[4], T gnmda, uint32_t hit, T gauss, T gapI,
                                             uint32_t p, bool own, uint32_t s, T (&cinc)[4], T &inc_out) {
@@ -703,20 +752,20 @@ __device__ __forceinline__ bool neuron_step(const Params &P, const NeuronPar<T> 
   if (q.pj && own) {
     if (P.plast == PL_STD) inc = (T)P.D[p];
     else if (P.plast == PL_STP) inc = (T)P.D[p] * (T)P.F[p];
-    else if (P.plast == PL_TM && P.tm_on[p]) {
-      T u = (T)P.tm_u[p], x = (T)P.tm_x[p];
-      const T U = (T)P.tm_U[p];
+    else if (kTM && (q.pj & kPjTM)) {
+      T u = (T)st.tmu, x = (T)st.tmx;
+      const T U = (T)__ldg(P.tm_U + p);
       if (spk) {
         u = u + U * ((T)1 - u);
         const T rel = u * x;
         inc = rel;
         x = x - rel;
       } else {
-        u = U + (u - U) * (T)P.tm_dff[p];
-        x = (T)1 + (x - (T)1) * (T)P.tm_dfr[p];
+        u = U + (u - U) * (T)__ldg(P.tm_dff + p);
+        x = (T)1 + (x - (T)1) * (T)__ldg(P.tm_dfr + p);
       }
-      P.tm_u[p] = (float)u;
-      P.tm_x[p] = (float)x;
+      st.tmu = (float)u;
+      st.tmx = (float)x;
     }
 #pragma unroll
     for (int r = 0; r < 4; r++) {
@@ -879,7 +928,7 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
     }
   }
   if (own) {
-    store_neuron<T>(P, p, st);
+    store_neuron<T>(P, p, q, st);
     if (P.gap_row) ((T *)P.Vg)[(size_t)((P.t0 + sb) & 1u) * n + p] = st.V;
     if (P.nspk && nsp) P.nspk[p] += nsp;
   }
@@ -1023,8 +1072,10 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) k_prod(const
 //    same function and operands as the neuron's owner, so every copy equals
 //    the owner's value bit for bit);
 //  * the NMDA in-edges of its posts live in shared memory as (tracked index,
-//    weight), summed per post by one warp (lane-strided, then an xor
+//    weight), summed per post by eight lanes (lane-strided, then an xor
 //    butterfly: the order of nmda_pull1_f32);
+//  * a listed spike is matched to the block's tracked neurons through a
+//    bitmap of their ids with per-word ranks (two shared-memory loads);
 //  * a spike's linear synapses are delivered by the blocks of its targets:
 //    each block walks the rows of its tracked neurons that spiked and adds
 //    w*c (2^-40 fixed point, integer atomics: any order gives the same sum)
@@ -1040,14 +1091,17 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) k_prod(const
 constexpr uint32_t kT1 = 512;   // threads of k_prod1 (= max posts per block)
 constexpr uint32_t kT1F = 512;  // listed spikes looked up per pass
 
-__device__ __forceinline__ int find_sorted(const uint32_t *a, uint32_t n, uint32_t x) {
-  uint32_t lo = 0, hi = n;
-  while (lo < hi) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (a[mid] < x) lo = mid + 1;
-    else hi = mid;
-  }
-  return (lo < n && a[lo] == x) ? (int)lo : -1;
+// Tracked index of neuron id in a block (or -1): bit id of the block's
+// bitmap (words [w0, w0 + nwd) of the id space) says whether it is
+// tracked, and its index is the number of tracked neurons below it: the
+// count of the earlier words (rank) plus the set bits below it in its word.
+__device__ __forceinline__ int find_tracked(const uint32_t *bits, const uint16_t *rank, uint32_t w0, uint32_t nwd,
+                                            uint32_t id) {
+  const uint32_t w = (id >> 5) - w0;  // ids below the first word wrap to >= nwd
+  if (w >= nwd) return -1;
+  const uint32_t word = bits[w], b = id & 31u;
+  if (!((word >> b) & 1u)) return -1;
+  return (int)rank[w] + __popc(word & ((1u << b) - 1u));
 }
 
 // Deliveries of a pass of listed spikes onto a block (k_prod1): warp w of
@@ -1056,7 +1110,7 @@ __device__ __forceinline__ int find_sorted(const uint32_t *a, uint32_t n, uint32
 // fixed point into the per-post accumulators.
 constexpr uint32_t kDelW = 4;  // warps that deliver the last pass
 __device__ __forceinline__ void deliver_listed(const Params &P, const Blk1 &me, uint32_t nf, const uint32_t *f_j,
-                                               const float (*f_c)[4], const uint32_t *lrow, long long *acc,
+                                               const float (*f_c)[4], const uint16_t *lrow, long long *acc,
                                                uint32_t w, uint32_t lane, uint32_t nw) {
   for (uint32_t k = w; k < nf; k += nw) {
     const uint32_t j = f_j[k];
@@ -1077,55 +1131,68 @@ template <class F>
 __device__ __forceinline__ bool grid_sync_work(unsigned int *bar, int *err, uint32_t count,
                                                unsigned long long &target, PhaseClock &pc, F &&work,
                                                unsigned int limit = 1u << 24) {
+  __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    if (count > 1) arrive_and_wait(bar, err, count, target, limit);
+    ok = count > 1 ? arrive_and_wait(bar, err, count, target, limit) : 1;
     pc.mark(6);  // thread 0's wait for the other blocks
   } else if (threadIdx.x >= 32) {
     work();
   }
   __syncthreads();
-  return *(volatile int *)err == 0;
+  return ok != 0;
 }
 
+// kTM: the network has Tsodyks-Markram plasticity (an instance without it
+// spends no registers on its state).
+template <bool kTM>
 __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params P) {
   extern __shared__ __align__(16) unsigned char sm1[];
   __shared__ float gn[kT1], d_gauss[kT1], f_c[kT1F][4], nf_inc[kT1F];
   __shared__ uint8_t d_hits[kT1];
-  __shared__ uint32_t f_j[kT1F], f_n, nf_j[kT1F], nf_n, next_post, blk_n;
+  __shared__ uint32_t f_j[kT1F], f_n, nf_j[kT1F], nf_n, next_grp, blk_n;
   const Blk1 me = P.b1[blockIdx.x];
   const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  const uint32_t n = P.n, mask = P.mask, NT = me.ntrk, np = me.np;
+  const uint32_t n = P.n, mask = P.mask, NT = me.ntrk, NS = me.nslot, np = me.np, ng = (np + 3) / 4;
   // shared-memory layout (16-byte aligned pieces first); the NMDA copies are
-  // double-buffered by step parity: buffer s & 1 holds the values after
-  // step t0 + s - 1
+  // per slot (a tracked neuron's slot is perm[j]) and double-buffered by
+  // step parity: buffer s & 1 holds the values after step t0 + s - 1
   long long *acc = (long long *)sm1;                           // [nlin][kT1]
-  float *const cx0 = (float *)(acc + (size_t)max(1u, P.nlin) * kT1);  // [NT] NMDA x copies
-  float *const cs0 = cx0 + NT;                                 // [NT] NMDA s copies
-  float *const cx1 = cs0 + NT;
-  float *const cs1 = cx1 + NT;
-  float *ctab = cs1 + NT;                                      // [ncls][3]
-  float *ew = ctab + 3 * P.t1_ncls;                            // [ne]
-  uint32_t *gid = (uint32_t *)(ew + me.ne);                    // [NT]
-  uint32_t *lrow = gid + NT;                                   // [NT + 1]
-  uint32_t *erow = lrow + NT + 1;                              // [np + 1]
-  uint16_t *eidx = (uint16_t *)(erow + np + 1);                // [ne]
-  uint8_t *cls = (uint8_t *)(eidx + me.ne);                    // [NT]
+  float *const cx0 = (float *)(acc + (size_t)max(1u, P.nlin) * kT1);  // [NS] NMDA x copies
+  float *const cs0 = cx0 + NS;                                 // [NS] NMDA s copies
+  float *const cx1 = cs0 + NS;
+  float *const cs1 = cx1 + NS;
+  float *ctab = cs1 + NS;                                      // [ncls][3]
+  float *ew = ctab + 3 * P.t1_ncls;                            // [ne] edge weights, group rows
+  uint32_t *bits = (uint32_t *)(ew + me.ne);                   // [nwd] tracked-neuron bitmap
+  uint32_t *grow = bits + me.nwd;                              // [ng + 1] first row of each group
+  uint16_t *eidx = (uint16_t *)(grow + ng + 1);                // [ne] edge sources' slots
+  uint16_t *rank = eidx + me.ne;                               // [nwd]
+  uint16_t *lrow = rank + me.nwd;                              // [NT + 1] linear rows
+  uint16_t *perm = lrow + NT + 1;                              // [NT] slots
+  uint8_t *cls = (uint8_t *)(perm + NT);                       // [NS] kinetics class, 255: none
   // ---- tables ----
   for (uint32_t i = tid; i < max(1u, P.nlin) * kT1; i += kT1) acc[i] = 0ll;
   for (uint32_t i = tid; i < 3 * P.t1_ncls; i += kT1) ctab[i] = __ldg(P.t1_cls_tab + i);
-  for (uint32_t j = tid; j < NT; j += kT1) {
-    const uint32_t g = __ldg(P.t1_gid + me.trk0 + j);
-    const uint8_t c = __ldg(P.t1_cls + me.trk0 + j);
-    gid[j] = g;
-    cls[j] = c;
+  for (uint32_t i = tid; i < NS; i += kT1) {
+    const uint32_t g = __ldg(P.t1_gid + me.s0 + i);
+    const uint8_t c = __ldg(P.t1_cls + me.s0 + i);
+    cls[i] = c;
     // the copies start from the owners' values after the last step before
-    // this launch (written back by the previous launch)
-    cx0[j] = c != 255 ? __ldcg((const float *)P.x_pre + g) : 0.0f;
-    cs0[j] = c != 255 ? __ldcg((const float *)P.s_pre + g) : 0.0f;
+    // this launch (written back by the previous launch); every other slot
+    // holds 0 in both buffers (the zero-weight fillers read them)
+    cx0[i] = c != 255 ? __ldcg((const float *)P.x_pre + g) : 0.0f;
+    cs0[i] = c != 255 ? __ldcg((const float *)P.s_pre + g) : 0.0f;
+    cx1[i] = 0.0f;
+    cs1[i] = 0.0f;
+  }
+  for (uint32_t w = tid; w < me.nwd; w += kT1) {
+    bits[w] = __ldg(P.t1_bits + me.bm0 + w);
+    rank[w] = __ldg(P.t1_rank + me.bm0 + w);
   }
   for (uint32_t j = tid; j <= NT; j += kT1) lrow[j] = __ldg(P.t1_lrow + me.lrow0 + j);
-  for (uint32_t q = tid; q <= np; q += kT1) erow[q] = __ldg(P.t1_erow + me.erow0 + q);
+  for (uint32_t j = tid; j < NT; j += kT1) perm[j] = __ldg(P.t1_perm + me.trk0 + j);
+  for (uint32_t g = tid; g <= ng; g += kT1) grow[g] = __ldg(P.t1_grow + me.grow0 + g);
   for (uint32_t e = tid; e < me.ne; e += kT1) {
     ew[e] = __ldg(P.t1_ew + me.e0 + e);
     eidx[e] = __ldg(P.t1_eidx + me.e0 + e);
@@ -1136,7 +1203,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
   const uint32_t p = own ? me.post0 + tid : me.post0;
   NeuronPar<float> q;
   NeuronState<float> st;
-  if (active) load_neuron<float>(P, p, q, st);
+  if (active) load_neuron<float, kTM>(P, p, q, st);
   uint32_t nsp = 0;
   if (own) {
     float gv = 0.0f;
@@ -1148,7 +1215,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
   unsigned long long target = 0;  // barrier arrivals so far (thread 0)
   if (tid == 0) {
     f_n = 0;
-    next_post = 0;
+    next_grp = 0;
   }
   __syncthreads();
   pc.mark(5);
@@ -1180,6 +1247,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
         b0 = __ldcg(reg + 2 * (size_t)tid + 1);
       }
       const uint32_t cnt = nreg + __ldcg(P.t1_cnt + ((uint32_t)(t - 1u) & 3u));
+      pc.lap(8, cnt);  // the list's entry count is in
       for (uint32_t c0 = 0; c0 < cnt; c0 += kT1F) {
         if (tid == 0) {
           f_n = 0;
@@ -1194,11 +1262,12 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
             b = __ldcg(ovf + 2 * (size_t)(i - nreg) + 1);
             b.z = tag;
           }
-          const int j = b.z == tag ? find_sorted(gid, NT, a.x) : -1;
+          const int j = b.z == tag ? find_tracked(bits, rank, me.w0, me.nwd, a.x) : -1;
           if (j >= 0) {
-            if (cls[j] != 255) {
+            const uint32_t sl = perm[j];
+            if (cls[sl] != 255) {
               const uint32_t k = atomicAdd(&nf_n, 1u);
-              nf_j[k] = (uint32_t)j;
+              nf_j[k] = sl;
               nf_inc[k] = __uint_as_float(a.y);
             }
             if (lrow[j + 1] > lrow[j]) {
@@ -1212,13 +1281,15 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
           }
         }
         __syncthreads();
-        // the NMDA copies of the listed neurons, from their previous values
+        pc.lap(9);  // the look-ups are done
+        // the NMDA copies of the listed neurons (by slot), from their
+        // previous values
         for (uint32_t k = tid; k < nf_n; k += kT1) {
-          const uint32_t j = nf_j[k], c = cls[j];
-          float xv = Xo[j], sv = So[j];
+          const uint32_t sl = nf_j[k], c = cls[sl];
+          float xv = Xo[sl], sv = So[sl];
           nmda_pre_step<float>(xv, sv, true, nf_inc[k], ctab[3 * c], ctab[3 * c + 1], ctab[3 * c + 2]);
-          X[j] = xv;
-          Sv[j] = sv;
+          X[sl] = xv;
+          Sv[sl] = sv;
         }
         // the deliveries of all but the last pass (the last pass's are made
         // by the first warps while the others start the NMDA sums)
@@ -1234,53 +1305,44 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
     }
     // ---- NMDA sums of the block's posts (order of nmda_pull1_f32) ----
     // the first kDelW warps deliver the last pass's listed spikes (their
-    // synapse rows come from L2) and then join; every warp takes posts two
-    // at a time from a shared counter, sums each lane-strided with four
-    // edges loaded ahead, then both butterflies (any warp gives the same
-    // sums)
-    if (wid < kDelW) deliver_listed(P, me, f_n, f_j, f_c, lrow, acc, wid, lane, kDelW);
-    for (;;) {
-      uint32_t qa = 0;
-      if (lane == 0) qa = atomicAdd(&next_post, 2u);
-      qa = __shfl_sync(fsd::kFull, qa, 0);
-      if (qa >= np) break;
-      const uint32_t qb = qa + 1;
-      const uint32_t ea0 = erow[qa], ea1 = erow[qa + 1];
-      const uint32_t eb0 = qb < np ? erow[qb] : 0u, eb1 = qb < np ? erow[qb + 1] : 0u;
-      const uint32_t len = max(ea1 - ea0, eb1 - eb0);
-      float aa = 0.0f, ab = 0.0f;
-      for (uint32_t o = lane; o < len; o += 128) {
-        float wa[4], va[4], wb[4], vb[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          const uint32_t xa = ea0 + o + 32u * u, xb = eb0 + o + 32u * u;
-          wa[u] = xa < ea1 ? ew[xa] : 0.0f;
-          va[u] = xa < ea1 ? Sv[eidx[xa]] : 0.0f;
-          wb[u] = xb < eb1 ? ew[xb] : 0.0f;
-          vb[u] = xb < eb1 ? Sv[eidx[xb]] : 0.0f;
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          if (ea0 + o + 32u * u < ea1) aa = __fmaf_rn(wa[u], va[u], aa);
-          if (eb0 + o + 32u * u < eb1) ab = __fmaf_rn(wb[u], vb[u], ab);
-        }
-      }
-#pragma unroll
-      for (int o = 16; o; o >>= 1) {
-        aa += __shfl_xor_sync(fsd::kFull, aa, o);
-        ab += __shfl_xor_sync(fsd::kFull, ab, o);
-      }
-      if (lane == 0) {
-        gn[qa] = aa;
-        if (qb < np) gn[qb] = ab;
-      }
+    // synapse rows come from L2) and then join; every warp takes groups of
+    // four posts from a shared counter and walks the group's rows of 32
+    // entries: lane l of quarter h sums post 4g + h's edges l, l + 8, ... in
+    // order (then zero-weight fillers, which leave the sum unchanged), four
+    // rows loaded ahead, then the butterfly over 4, 2, 1
+    if (wid < kDelW) {
+      deliver_listed(P, me, f_n, f_j, f_c, lrow, acc, wid, lane, kDelW);
+      pc.lap(10);  // warp 0's deliveries are issued
     }
+    for (;;) {
+      uint32_t g = 0;
+      if (lane == 0) g = atomicAdd(&next_grp, 1u);
+      g = __shfl_sync(fsd::kFull, g, 0);
+      if (g >= ng) break;
+      const uint32_t iend = grow[g + 1] * 32u;
+      uint32_t i = grow[g] * 32u + lane;
+      float sum = 0.0f;
+      for (; i + 96u < iend; i += 128u) {
+        const float w0 = ew[i], w1 = ew[i + 32], w2 = ew[i + 64], w3 = ew[i + 96];
+        const float v0 = Sv[eidx[i]], v1 = Sv[eidx[i + 32]], v2 = Sv[eidx[i + 64]], v3 = Sv[eidx[i + 96]];
+        sum = __fmaf_rn(w0, v0, sum);
+        sum = __fmaf_rn(w1, v1, sum);
+        sum = __fmaf_rn(w2, v2, sum);
+        sum = __fmaf_rn(w3, v3, sum);
+      }
+      for (; i < iend; i += 32u) sum = __fmaf_rn(ew[i], Sv[eidx[i]], sum);
+#pragma unroll
+      for (int o = 4; o; o >>= 1) sum += __shfl_xor_sync(fsd::kFull, sum, o);
+      const uint32_t qq = 4 * g + (lane >> 3);
+      if ((lane & 7u) == 0 && qq < np) gn[qq] = sum;
+    }
+    pc.lap(11);  // warp 0 found no more posts to sum
     __syncthreads();
     pc.mark(2);
     // (the pass counters are reset behind the barrier above, for the next step)
     if (tid == 0) {
       f_n = 0;
-      next_post = 0;
+      next_grp = 0;
     }
     // ---- the neurons' step ----
     if (active) {
@@ -1302,7 +1364,8 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
       }
       const uint32_t qs = own ? tid : 0;
       float cinc[4], inc;
-      const bool spk = neuron_step<float>(P, q, st, rv, gn[qs], d_hits[qs], d_gauss[qs], 0.0f, p, own, s, cinc, inc);
+      const bool spk =
+          neuron_step<float, kTM>(P, q, st, rv, gn[qs], d_hits[qs], d_gauss[qs], 0.0f, p, own, s, cinc, inc);
       nsp += spk ? 1u : 0u;
       if (own && P.gv_row) gv_write<float>(P, p, s, st);
       const uint32_t m = __ballot_sync(fsd::kFull, spk);
@@ -1360,7 +1423,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
         }
         if (P.t1_ncls == 1) {  // one class (the usual case): its constants in registers
           const float k0 = ctab[0], k1 = ctab[1], k2 = ctab[2];
-          for (uint32_t j = tid - 32; j < NT; j += kT1 - 32) {
+          for (uint32_t j = tid - 32; j < NS; j += kT1 - 32) {
             if (cls[j] != 255) {
               float xv = X[j], sv = Sv[j];
               nmda_pre_step<float>(xv, sv, false, 1.0f, k0, k1, k2);
@@ -1369,7 +1432,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
             }
           }
         } else {
-          for (uint32_t j = tid - 32; j < NT; j += kT1 - 32) {
+          for (uint32_t j = tid - 32; j < NS; j += kT1 - 32) {
             const uint32_t c = cls[j];
             if (c != 255) {
               float xv = X[j], sv = Sv[j];
@@ -1385,7 +1448,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
     }
   }
   if (own) {
-    store_neuron<float>(P, p, st);
+    store_neuron<float, kTM>(P, p, q, st);
     if (P.nspk && nsp) P.nspk[p] += nsp;
   }
   // the launch's spikes, added to the total once per warp
@@ -1637,7 +1700,8 @@ int launch(Prod *p, uint32_t nsteps, bool want_bits, bool wantV, cudaStream_t st
     return FS_OK;
   }
   if (p->single) {
-    e = cudaLaunchCooperativeKernel((const void *)k_prod1, p->b1_blocks, kT1, args, P.t1_smem, st);
+    const void *k1 = P.plast == PL_TM ? (const void *)k_prod1<true> : (const void *)k_prod1<false>;
+    e = cudaLaunchCooperativeKernel(k1, p->b1_blocks, kT1, args, P.t1_smem, st);
   } else {
     // (the FP64 pull does not take the edges-in-flight parameter)
     const void *k = p->fp64 ? (const void *)k_prod<double, 4>
@@ -1797,12 +1861,74 @@ static int host_net(const fs_net_desc *d, HostNet &H, std::string &err) {
 // fit in shared memory or there are more than 255 NMDA kinetics classes.
 struct Single {
   std::vector<Blk1> blk;
-  std::vector<uint32_t> gid, lrow, lin, erow;
+  std::vector<uint32_t> gid, lin, grow, bits;  // gid, cls: per slot
   std::vector<uint8_t> cls;
   std::vector<float> linw, ew, tab;
-  std::vector<uint16_t> eidx;
+  std::vector<uint16_t> eidx, rank, lrow, perm;  // lrow, perm: per tracked neuron
   uint32_t smem = 0;
 };
+
+// Shared memory of k_prod1's tables for one block (the kernel's layout):
+// accumulators | x, s copies x2 (per slot) | class table | edge weights |
+// bitmap | group rows | edge slots | ranks | linear rows | slots of the
+// tracked neurons | classes (per slot).
+static size_t single_smem(uint32_t nlin, uint32_t ncls, const Blk1 &k) {
+  const size_t ng = ((size_t)k.np + 3) / 4;
+  return (size_t)std::max(1u, nlin) * kT1 * 8 + (size_t)k.nslot * 16 + 3 * (size_t)ncls * 4 + (size_t)k.ne * 4 +
+         (size_t)k.nwd * 4 + (ng + 1) * 4 + (size_t)k.ne * 2 + (size_t)k.nwd * 2 + ((size_t)k.ntrk + 1) * 2 +
+         (size_t)k.ntrk * 2 + (size_t)k.nslot;
+}
+
+// Slots of a block's tracked neurons in its shared-memory copies, so that
+// the gathers of one row of NMDA edges (32 tracked indices, `rows` lists
+// them) fall in as few lanes of the same bank as a greedy pass finds: the
+// neurons in the most rows first, each into the bank (slot mod 32) that
+// least raises the rows' largest bank counts, at most cap per bank.  The
+// slots change where values live, not which values a sum adds or in which
+// order.  Returns the slot count (a multiple of 32).
+static uint32_t color_slots(uint32_t nt, const std::vector<std::vector<uint32_t>> &rows, std::vector<uint16_t> &slot) {
+  slot.assign(nt, 0);
+  if (nt == 0) return 0;
+  std::vector<std::vector<uint32_t>> in_rows(nt);
+  for (uint32_t i = 0; i < rows.size(); i++)
+    for (uint32_t j : rows[i])
+      if (in_rows[j].empty() || in_rows[j].back() != i) in_rows[j].push_back(i);
+  std::vector<uint32_t> order(nt);
+  for (uint32_t j = 0; j < nt; j++) order[j] = j;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](uint32_t a, uint32_t b) { return in_rows[a].size() > in_rows[b].size(); });
+  const uint32_t cap = (nt + 31) / 32 + 2;
+  std::vector<std::array<uint16_t, 32>> cnt(rows.size());
+  std::vector<uint16_t> mx(rows.size(), 0);
+  for (auto &c : cnt) c.fill(0);
+  std::vector<uint32_t> fill(32, 0), bank(nt, 0);
+  for (uint32_t j : order) {
+    uint64_t best = ~0ull;
+    uint32_t bb = 0;
+    for (uint32_t b = 0; b < 32; b++) {
+      if (fill[b] >= cap) continue;
+      uint64_t score = 0;
+      for (uint32_t i : in_rows[j]) score += (cnt[i][b] + 1u > mx[i] ? 1024u : 0u) + cnt[i][b];
+      if (score < best) {
+        best = score;
+        bb = b;
+      }
+    }
+    bank[j] = bb;
+    fill[bb]++;
+    for (uint32_t i : in_rows[j]) {
+      cnt[i][bb]++;
+      mx[i] = std::max<uint16_t>(mx[i], cnt[i][bb]);
+    }
+  }
+  std::vector<uint32_t> next(32, 0);
+  uint32_t maxfill = 0;
+  for (uint32_t j = 0; j < nt; j++) {
+    slot[j] = (uint16_t)(next[bank[j]]++ * 32 + bank[j]);
+    maxfill = std::max(maxfill, next[bank[j]]);
+  }
+  return 32 * maxfill;
+}
 
 static bool plan_single(uint32_t n, uint32_t nlin, uint32_t sm_count, const std::vector<uint32_t> &in_row,
                         const std::vector<uint32_t> &in_code, const std::vector<float> &in_w,
@@ -1880,11 +2006,11 @@ static bool plan_single(uint32_t n, uint32_t nlin, uint32_t sm_count, const std:
       lin_b[blk_of_unit[post >> 5]].push_back(((uint64_t)a << 32) | e);
     }
   std::vector<int32_t> loc(n, -1);
-  const size_t fixed = (size_t)std::max(1u, nlin) * kT1 * 8 + S1.tab.size() * 4 + 64;
   S1.blk.clear();
-  S1.gid.clear(); S1.lrow.clear(); S1.lin.clear(); S1.erow.clear(); S1.cls.clear();
-  S1.linw.clear(); S1.ew.clear(); S1.eidx.clear();
+  S1.gid.clear(); S1.lrow.clear(); S1.lin.clear(); S1.grow.clear(); S1.cls.clear(); S1.perm.clear();
+  S1.linw.clear(); S1.ew.clear(); S1.eidx.clear(); S1.bits.clear(); S1.rank.clear();
   size_t smax = 0;
+  bool big_lin = false;
   for (uint32_t b = 0; b < B; b++) {
     const uint32_t P0 = cut[b] * 32, P1 = std::min(n, cut[b + 1] * 32);
     std::vector<uint64_t> &L = lin_b[b];
@@ -1895,37 +2021,92 @@ static bool plan_single(uint32_t n, uint32_t nlin, uint32_t sm_count, const std:
     for (uint64_t x : L) trk.push_back((uint32_t)(x >> 32));
     std::sort(trk.begin(), trk.end());
     trk.erase(std::unique(trk.begin(), trk.end()), trk.end());
-    if (trk.size() > 65535) {
-      why = "a block tracks more than 65535 presynaptic neurons";
+    if (trk.size() > 65535 - 95) {
+      why = "a block tracks more than 65440 presynaptic neurons";
       return false;
     }
+    big_lin |= L.size() > 65535;  // (reported after the shared-memory check)
     Blk1 bk{};
     bk.post0 = P0;
     bk.np = P1 - P0;
-    bk.trk0 = (uint32_t)S1.gid.size();
+    bk.trk0 = (uint32_t)S1.perm.size();
     bk.ntrk = (uint32_t)trk.size();
     bk.lrow0 = (uint32_t)S1.lrow.size();
     bk.e0 = (uint32_t)S1.ew.size();
-    bk.erow0 = (uint32_t)S1.erow.size();
+    bk.grow0 = (uint32_t)S1.grow.size();
     bk.l0 = (uint32_t)S1.lin.size();
+    for (uint32_t j = 0; j < trk.size(); j++) loc[trk[j]] = (int32_t)j;
+    // bitmap of the tracked ids over the words they span, and per word the
+    // tracked neurons in the words before it
+    bk.bm0 = (uint32_t)S1.bits.size();
+    bk.w0 = trk.empty() ? 0u : trk.front() >> 5;
+    bk.nwd = trk.empty() ? 0u : (trk.back() >> 5) - bk.w0 + 1;
+    S1.bits.resize((size_t)bk.bm0 + bk.nwd, 0u);
+    S1.rank.resize((size_t)bk.bm0 + bk.nwd, 0u);
+    for (uint32_t a : trk) S1.bits[bk.bm0 + (a >> 5) - bk.w0] |= 1u << (a & 31u);
+    for (uint32_t w = 0, c = 0; w < bk.nwd; w++) {
+      S1.rank[bk.bm0 + w] = (uint16_t)c;
+      c += (uint32_t)__builtin_popcount(S1.bits[bk.bm0 + w]);
+    }
+    // NMDA in-edges: posts in groups of four, a group's edges in rows of 32
+    // (row r, quarter h, lane l: edge 8r + l of post 4g + h in CSR order, or
+    // a zero-weight filler), as many rows as its longest post needs
+    const uint32_t npb = P1 - P0, ng = (npb + 3) / 4;
+    std::vector<uint32_t> grow(ng + 1, 0);
+    for (uint32_t g = 0; g < ng; g++) {
+      uint32_t R = 0;
+      for (uint32_t h = 0; h < 4 && 4 * g + h < npb; h++) {
+        const uint32_t q = P0 + 4 * g + h;
+        R = std::max(R, (in_row[q + 1] - in_row[q] + 7) / 8);
+      }
+      grow[g + 1] = grow[g] + R;
+    }
+    const uint32_t nrow = grow[ng];
+    std::vector<int32_t> ent((size_t)nrow * 32, -1);  // tracked index per entry, -1: filler
+    std::vector<std::vector<uint32_t>> rows(nrow);
+    for (uint32_t g = 0; g < ng; g++)
+      for (uint32_t h = 0; h < 4 && 4 * g + h < npb; h++) {
+        const uint32_t q = P0 + 4 * g + h;
+        for (uint32_t e = 0; e < in_row[q + 1] - in_row[q]; e++) {
+          const uint32_t r = grow[g] + e / 8, x = r * 32 + 8 * h + (e & 7u);
+          ent[x] = loc[in_code[in_row[q] + e] & 0xffffffu];
+          rows[r].push_back((uint32_t)ent[x]);
+        }
+      }
+    for (auto &rw : rows) std::sort(rw.begin(), rw.end());
+    std::vector<uint16_t> slot;
+    bk.nslot = color_slots(bk.ntrk, rows, slot);
+    if (bk.nslot > 65535) {
+      why = "a block needs more than 65535 slots";
+      return false;
+    }
+    bk.s0 = (uint32_t)S1.gid.size();
+    S1.gid.resize((size_t)bk.s0 + bk.nslot, 0xffffffffu);
+    S1.cls.resize((size_t)bk.s0 + bk.nslot, 255);
     for (uint32_t j = 0; j < trk.size(); j++) {
-      loc[trk[j]] = (int32_t)j;
-      S1.gid.push_back(trk[j]);
-      S1.cls.push_back(255);
+      S1.perm.push_back(slot[j]);
+      S1.gid[bk.s0 + slot[j]] = trk[j];
     }
-    // NMDA in-edges in CSR order; the classes of the neurons they come from
-    for (uint32_t q = P0; q <= P1; q++) S1.erow.push_back(in_row[q] - in_row[P0]);
-    for (uint32_t e = in_row[P0]; e < in_row[P1]; e++) {
-      const uint32_t a = in_code[e] & 0xffffffu;
-      S1.eidx.push_back((uint16_t)loc[a]);
+    for (uint32_t g = 0; g <= ng; g++) S1.grow.push_back(grow[g]);
+    for (uint32_t x = 0; x < nrow * 32; x++) {
+      if (ent[x] < 0) {
+        S1.eidx.push_back(0);
+        S1.ew.push_back(0.0f);
+        continue;
+      }
+      const uint32_t r = x / 32, h = (x & 31u) / 8, g = (uint32_t)(std::upper_bound(grow.begin(), grow.end(), r) -
+                                                                     grow.begin()) - 1;
+      const uint32_t q = P0 + 4 * g + h, e = in_row[q] + 8 * (r - grow[g]) + (x & 7u);
+      const uint32_t a = in_code[e] & 0xffffffu, sl = slot[(uint32_t)ent[x]];
+      S1.eidx.push_back((uint16_t)sl);
       S1.ew.push_back(in_w[e]);
-      S1.cls[bk.trk0 + loc[a]] = (uint8_t)cls_of[a];
+      S1.cls[bk.s0 + sl] = (uint8_t)cls_of[a];
     }
-    bk.ne = in_row[P1] - in_row[P0];
+    bk.ne = nrow * 32;
     // linear rows per tracked neuron (L is sorted by neuron)
     size_t k = 0;
     for (uint32_t j = 0; j < trk.size(); j++) {
-      S1.lrow.push_back((uint32_t)(S1.lin.size() - bk.l0));
+      S1.lrow.push_back((uint16_t)(S1.lin.size() - bk.l0));
       while (k < L.size() && (uint32_t)(L[k] >> 32) == trk[j]) {
         const uint32_t e = (uint32_t)L[k];
         const uint32_t post = out_code[e] & 0x3fffffu, r = (out_code[e] >> 22) & 3u;
@@ -1934,15 +2115,18 @@ static bool plan_single(uint32_t n, uint32_t nlin, uint32_t sm_count, const std:
         k++;
       }
     }
-    S1.lrow.push_back((uint32_t)(S1.lin.size() - bk.l0));
+    S1.lrow.push_back((uint16_t)(S1.lin.size() - bk.l0));
     for (uint32_t a : trk) loc[a] = -1;
     S1.blk.push_back(bk);
-    const size_t need = fixed + (size_t)bk.ntrk * (4 * 4 + 4 + 4 + 1) + 4 + (size_t)bk.ne * 6 + (size_t)(bk.np + 1) * 4;
-    smax = std::max(smax, need);
+    smax = std::max(smax, single_smem(nlin, (uint32_t)tabs.size(), bk));
   }
   // dynamic shared memory next to the kernel's ~15 KB of static arrays
   if (smax > (size_t)200 * 1024) {
     why = "a block's tables need " + std::to_string(smax) + " bytes of shared memory";
+    return false;
+  }
+  if (big_lin) {
+    why = "a block receives more than 65535 linear synapses";
     return false;
   }
   S1.smem = (uint32_t)((smax + 15) & ~(size_t)15);
@@ -1961,23 +2145,49 @@ static bool validate_single(const HostNet &H, const Single &S1, std::string &err
   const uint32_t ncls = (uint32_t)(S1.tab.size() / 3);
   uint32_t next_post = 0;
   uint64_t lin_total = 0, nmda_total = 0;
-  std::vector<uint8_t> seen;
   for (uint32_t b = 0; b < S1.blk.size(); b++) {
     const Blk1 &k = S1.blk[b];
     if (k.post0 != next_post || k.post0 % 32 || k.np == 0 || k.np > kT1 || k.post0 + k.np > n)
       return fail(b, "post range");
     next_post = k.post0 + k.np;
-    if (k.ntrk > 65535 || (size_t)k.trk0 + k.ntrk > S1.gid.size() || (size_t)k.lrow0 + k.ntrk + 1 > S1.lrow.size() ||
-        (size_t)k.erow0 + k.np + 1 > S1.erow.size() || (size_t)k.e0 + k.ne > S1.ew.size() ||
-        (size_t)k.e0 + k.ne > S1.eidx.size())
+    const uint32_t ng = (k.np + 3) / 4;
+    if (k.ntrk > k.nslot || k.nslot % 32 || k.nslot > 65535 || (size_t)k.trk0 + k.ntrk > S1.perm.size() ||
+        (size_t)k.s0 + k.nslot > S1.gid.size() || (size_t)k.s0 + k.nslot > S1.cls.size() ||
+        (size_t)k.lrow0 + k.ntrk + 1 > S1.lrow.size() || (size_t)k.grow0 + ng + 1 > S1.grow.size() ||
+        (size_t)k.e0 + k.ne > S1.ew.size() || (size_t)k.e0 + k.ne > S1.eidx.size() ||
+        (size_t)k.bm0 + k.nwd > S1.bits.size() || (size_t)k.bm0 + k.nwd > S1.rank.size() ||
+        ((uint64_t)k.w0 + k.nwd) * 32 > (uint64_t)n + 31)
       return fail(b, "table range");
+    // slots: a one-to-one map of the tracked neurons into [0, nslot), the
+    // other slots empty; tracked ids ascending (the bitmap's rank order)
+    std::vector<int32_t> trk_of(k.nslot, -1);
+    std::vector<uint32_t> trk(k.ntrk);
     for (uint32_t j = 0; j < k.ntrk; j++) {
-      const uint32_t g = S1.gid[k.trk0 + j];
-      if (g >= n || (j && g <= S1.gid[k.trk0 + j - 1])) return fail(b, "tracked ids not sorted");
-      const uint8_t c = S1.cls[k.trk0 + j];
+      const uint32_t sl = S1.perm[k.trk0 + j];
+      if (sl >= k.nslot || trk_of[sl] >= 0) return fail(b, "slots");
+      trk_of[sl] = (int32_t)j;
+      trk[j] = S1.gid[k.s0 + sl];
+      if (trk[j] >= n || (j && trk[j] <= trk[j - 1])) return fail(b, "tracked ids not sorted");
+    }
+    for (uint32_t sl = 0; sl < k.nslot; sl++) {
+      const uint8_t c = S1.cls[k.s0 + sl];
+      if (trk_of[sl] < 0 && (c != 255 || S1.gid[k.s0 + sl] != 0xffffffffu)) return fail(b, "empty slot");
       if (c != 255 && c >= ncls) return fail(b, "kinetics class");
     }
-    const uint32_t *lr = &S1.lrow[k.lrow0];
+    // the bitmap look-up the kernel makes gives every tracked neuron its
+    // index, and the bitmap holds no other neuron
+    uint32_t set = 0;
+    for (uint32_t w = 0; w < k.nwd; w++) set += (uint32_t)__builtin_popcount(S1.bits[k.bm0 + w]);
+    if (set != k.ntrk) return fail(b, "bitmap");
+    for (uint32_t j = 0; j < k.ntrk; j++) {
+      const uint32_t g = trk[j], w = (g >> 5) - k.w0;
+      if (w >= k.nwd) return fail(b, "bitmap");
+      const uint32_t word = S1.bits[k.bm0 + w];
+      if (!((word >> (g & 31u)) & 1u) ||
+          S1.rank[k.bm0 + w] + (uint32_t)__builtin_popcount(word & ((1u << (g & 31u)) - 1u)) != j)
+        return fail(b, "bitmap");
+    }
+    const uint16_t *lr = &S1.lrow[k.lrow0];
     if (lr[0] != 0) return fail(b, "linear rows");
     for (uint32_t j = 0; j < k.ntrk; j++)
       if (lr[j + 1] < lr[j]) return fail(b, "linear rows");
@@ -1988,23 +2198,35 @@ static bool validate_single(const HostNet &H, const Single &S1, std::string &err
       if (q >= k.np || r > 3 || H.lin_of_rec[r] < 0) return fail(b, "linear entry");
     }
     lin_total += lr[k.ntrk];
-    const uint32_t *er = &S1.erow[k.erow0];
-    if (er[0] != 0 || er[k.np] != k.ne) return fail(b, "edge rows");
-    for (uint32_t q = 0; q < k.np; q++)
-      if (er[q + 1] < er[q] || er[q + 1] - er[q] != H.in_row[k.post0 + q + 1] - H.in_row[k.post0 + q])
-        return fail(b, "edge rows");
-    for (uint32_t e = 0; e < k.ne; e++) {
-      const uint16_t j = S1.eidx[k.e0 + e];
-      if (j >= k.ntrk || S1.cls[k.trk0 + j] == 255) return fail(b, "edge index");
-      if (S1.gid[k.trk0 + j] != (H.in_code[H.in_row[k.post0] + e] & 0xffffffu)) return fail(b, "edge source");
+    // NMDA edges: every edge of every post at its entry (row grow[g] + e / 8,
+    // quarter h, lane e mod 8) with its weight and its source's slot, every
+    // other entry of the group's rows a zero-weight filler on a valid slot
+    const uint32_t *gr = &S1.grow[k.grow0];
+    if (gr[0] != 0 || (uint64_t)gr[ng] * 32 != k.ne) return fail(b, "group rows");
+    std::vector<uint8_t> used(k.ne, 0);
+    for (uint32_t g = 0; g < ng; g++) {
+      if (gr[g + 1] < gr[g]) return fail(b, "group rows");
+      for (uint32_t h = 0; h < 4 && 4 * g + h < k.np; h++) {
+        const uint32_t q = k.post0 + 4 * g + h, b0 = H.in_row[q], len = H.in_row[q + 1] - b0;
+        if ((len + 7) / 8 > gr[g + 1] - gr[g]) return fail(b, "group rows");
+        for (uint32_t e = 0; e < len; e++) {
+          const uint32_t x = (gr[g] + e / 8) * 32 + 8 * h + (e & 7u);
+          const uint16_t sl = S1.eidx[k.e0 + x];
+          if (sl >= k.nslot || trk_of[sl] < 0 || S1.cls[k.s0 + sl] == 255) return fail(b, "edge slot");
+          if (trk[trk_of[sl]] != (H.in_code[b0 + e] & 0xffffffu)) return fail(b, "edge source");
+          if (std::memcmp(&S1.ew[k.e0 + x], &H.in_w[b0 + e], 4) != 0) return fail(b, "edge weight");
+          used[x] = 1;
+        }
+      }
     }
-    nmda_total += k.ne;
-    // the kernel's layout: acc | x, s copies x2 | class table | edge weights |
-    // ids | linear rows | edge rows | edge indices | classes
-    const size_t need = (size_t)std::max(1u, H.nlin) * kT1 * 8 + (size_t)k.ntrk * 16 + 3 * (size_t)ncls * 4 +
-                        (size_t)k.ne * 4 + (size_t)k.ntrk * 4 + ((size_t)k.ntrk + 1) * 4 + ((size_t)k.np + 1) * 4 +
-                        (size_t)k.ne * 2 + (size_t)k.ntrk;
-    if (need > S1.smem) return fail(b, "shared memory");
+    for (uint32_t x = 0; x < k.ne; x++) {
+      if (used[x]) {
+        nmda_total++;
+      } else if (S1.ew[k.e0 + x] != 0.0f || std::signbit(S1.ew[k.e0 + x]) || S1.eidx[k.e0 + x] >= k.nslot) {
+        return fail(b, "filler");
+      }
+    }
+    if (single_smem(H.nlin, ncls, k) > S1.smem) return fail(b, "shared memory");
   }
   if (next_post != n) return fail((uint32_t)S1.blk.size(), "posts not covered");
   if (lin_total != H.nlin_e || nmda_total != H.nnm_e) return fail(0, "synapse count");
@@ -2027,11 +2249,11 @@ int prod_check_single_plan(const fs_net_desc *d, uint32_t sm_count, uint64_t *st
   for (const Blk1 &k : S1.blk) {
     stats[2] = std::max<uint64_t>(stats[2], k.np);
     stats[3] = std::max<uint64_t>(stats[3], k.ntrk);
-    stats[4] = std::max<uint64_t>(stats[4], k.ne);
+    stats[4] = std::max<uint64_t>(stats[4], H.in_row[k.post0 + k.np] - H.in_row[k.post0]);
   }
   stats[5] = S1.smem;
   stats[6] = S1.lin.size();
-  stats[7] = S1.eidx.size();
+  stats[7] = H.nnm_e;
   return FS_OK;
 }
 
@@ -2220,21 +2442,26 @@ static int prod_create_from(Prod **out, const fs_net_desc *d, const fs_run_opts 
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
       cudaFuncAttributes fa{};
-      cudaFuncGetAttributes(&fa, (const void *)k_prod1);
+      cudaFuncGetAttributes(&fa, (const void *)k_prod1<true>);
       const int dyn_max = std::min<int>(200 * 1024, maxsm - (int)fa.sharedSizeBytes);
       if ((int)S1.smem <= dyn_max &&
-          cudaFuncSetAttribute((const void *)k_prod1, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max) ==
+          cudaFuncSetAttribute((const void *)k_prod1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max) ==
+              cudaSuccess &&
+          cudaFuncSetAttribute((const void *)k_prod1<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max) ==
               cudaSuccess) {
         if ((rc = dup(p, (Blk1 **)&P.b1, S1.blk.data(), S1.blk.size(), st, err))) goto fail;
         UPU(t1_gid, S1.gid.data(), S1.gid.size());
-        UPU(t1_lrow, S1.lrow.data(), S1.lrow.size());
+        if ((rc = dup(p, (uint16_t **)&P.t1_lrow, S1.lrow.data(), S1.lrow.size(), st, err))) goto fail;
+        if ((rc = dup(p, (uint16_t **)&P.t1_perm, S1.perm.data(), S1.perm.size(), st, err))) goto fail;
         UPU(t1_lin, S1.lin.data(), S1.lin.size());
-        UPU(t1_erow, S1.erow.data(), S1.erow.size());
+        UPU(t1_grow, S1.grow.data(), S1.grow.size());
         if ((rc = dup(p, (uint8_t **)&P.t1_cls, S1.cls.data(), S1.cls.size(), st, err))) goto fail;
         UPF(t1_linw, S1.linw.data(), S1.linw.size());
         UPF(t1_ew, S1.ew.data(), S1.ew.size());
         UPF(t1_cls_tab, S1.tab.data(), S1.tab.size());
         if ((rc = dup(p, (uint16_t **)&P.t1_eidx, S1.eidx.data(), S1.eidx.size(), st, err))) goto fail;
+        UPU(t1_bits, S1.bits.data(), S1.bits.size());
+        if ((rc = dup(p, (uint16_t **)&P.t1_rank, S1.rank.data(), S1.rank.size(), st, err))) goto fail;
         if ((rc = dup(p, &P.t1_cnt, (const uint32_t *)nullptr, 4, st, err))) goto fail;
         P.t1_slots = std::min<uint32_t>(16, kT1F / (uint32_t)S1.blk.size());
         if ((rc = dup(p, &P.t1_list, (const uint4 *)nullptr, (size_t)2 * S1.blk.size() * P.t1_slots * 2, st, err)) ||
@@ -3090,10 +3317,10 @@ int prod_phase_clock(Prod *p, int enable, cudaStream_t st, std::string &err) {
     return FS_OK;
   }
   if (!p->phase_buf) {
-    int rc = dal(p, &p->phase_buf, (size_t)nb * 8, err);
+    int rc = dal(p, &p->phase_buf, (size_t)nb * kPhaseSlots, err);
     if (rc) return rc;
   }
-  cudaError_t e = cudaMemsetAsync(p->phase_buf, 0, (size_t)nb * 8 * 8, st);
+  cudaError_t e = cudaMemsetAsync(p->phase_buf, 0, (size_t)nb * kPhaseSlots * 8, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     err = std::string("phase clock: ") + cudaGetErrorString(e);
@@ -3110,7 +3337,7 @@ int prod_phase_times(Prod *p, uint64_t *out, uint32_t cap, uint32_t *blocks, cud
     err = "phase clock was never switched on";
     return FS_ERR_ARG;
   }
-  const size_t k = std::min<size_t>(cap, (size_t)nb * 8);
+  const size_t k = std::min<size_t>(cap, (size_t)nb * kPhaseSlots);
   cudaError_t e = cudaStreamSynchronize(st);
   if (e == cudaSuccess && k) e = cudaMemcpy(out, p->phase_buf, k * 8, cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) {

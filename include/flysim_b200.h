@@ -316,13 +316,15 @@ int fs_debug_single_step_plan(const fs_net_desc *desc, uint32_t sm_count, uint64
 /* Phase clock of the persistent kernels (a profiling aid; no counterpart in
  * the reference).  fs_debug_phase_clock(h, 1) zeroes and switches on
  * per-block counters of SM cycles per phase, 0 switches them off;
- * fs_debug_phase_times copies up to cap counters, [blocks][8], and the
+ * fs_debug_phase_times copies up to cap counters, [blocks][16], and the
  * block count.  Phases: single-step kernel 0 spike-list lookups, 1 NMDA
  * copies of listed spikes, 2 last deliveries and NMDA sums, 3 neuron steps,
  * 6 thread 0's wait at the grid barrier, 4 the rest of the barrier (the
- * other warps' drive draws and NMDA copies), 5 set-up;
- * interval kernel 0 NMDA pull, 1 drive draws, 2 neuron steps, 3 pushes,
- * 4 grid barrier.  The tile kernels have no phase clock. */
+ * other warps' drive draws and NMDA copies), 5 set-up, and laps inside a
+ * phase (cycles from its start): 8 the list's entry count loaded, 9 the
+ * look-ups done, 10 warp 0's deliveries issued, 11 warp 0 out of posts to
+ * sum; interval kernel 0 NMDA pull, 1 drive draws, 2 neuron steps,
+ * 3 pushes, 4 grid barrier.  The tile kernels have no phase clock. */
 int fs_debug_phase_clock(fs_handle *h, int enable);
 int fs_debug_phase_times(fs_handle *h, uint64_t *out, uint32_t cap, uint32_t *blocks);
 /* Failure detection on the host side: stores into the handle's device error
