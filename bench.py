@@ -422,7 +422,8 @@ def main():
             names = (["list lookups", "nmda copies", "deliveries+nmda sums", "neuron steps", "barrier rest",
                       "set-up", "barrier wait (thread 0)", "-", "lookups: entry count in (lap)",
                       "lookups: search done (lap)", "sums: warp 0 deliveries issued (lap)",
-                      "sums: warp 0 out of posts (lap)"]
+                      "sums: warp 0 out of posts (lap)", "lookups: thread 0's entries in (lap)",
+                      "neuron steps: warp 0 stepped (lap)"]
                      if eng.layout()["kernel"] == "single_step" else
                      ["nmda pull", "drive draws", "neuron steps", "pushes", "barrier"])
             line["cycles_per_timestep"] = {nm: {"mean": round(float(ph[:, k].mean()), 1),

@@ -1247,7 +1247,8 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
         b0 = __ldcg(reg + 2 * (size_t)tid + 1);
       }
       const uint32_t cnt = nreg + __ldcg(P.t1_cnt + ((uint32_t)(t - 1u) & 3u));
-      pc.lap(8, cnt);  // the list's entry count is in
+      pc.lap(8, cnt);    // the list's entry count is in
+      pc.lap(12, b0.w);  // thread 0's entries are in
       for (uint32_t c0 = 0; c0 < cnt; c0 += kT1F) {
         if (tid == 0) {
           f_n = 0;
@@ -1366,6 +1367,7 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
       float cinc[4], inc;
       const bool spk =
           neuron_step<float, kTM>(P, q, st, rv, gn[qs], d_hits[qs], d_gauss[qs], 0.0f, p, own, s, cinc, inc);
+      pc.lap(13, spk ? 1u : 0u);  // warp 0's neurons have stepped
       nsp += spk ? 1u : 0u;
       if (own && P.gv_row) gv_write<float>(P, p, s, st);
       const uint32_t m = __ballot_sync(fsd::kFull, spk);

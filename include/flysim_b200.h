@@ -323,7 +323,7 @@ int fs_debug_single_step_plan(const fs_net_desc *desc, uint32_t sm_count, uint64
  * other warps' drive draws and NMDA copies), 5 set-up, and laps inside a
  * phase (cycles from its start): 8 the list's entry count loaded, 9 the
  * look-ups done, 10 warp 0's deliveries issued, 11 warp 0 out of posts to
- * sum; interval kernel 0 NMDA pull, 1 drive draws, 2 neuron steps,
+ * sum, 12 thread 0's list entries loaded, 13 warp 0's neuron steps done; interval kernel 0 NMDA pull, 1 drive draws, 2 neuron steps,
  * 3 pushes, 4 grid barrier.  The tile kernels have no phase clock. */
 int fs_debug_phase_clock(fs_handle *h, int enable);
 int fs_debug_phase_times(fs_handle *h, uint64_t *out, uint32_t cap, uint32_t *blocks);
