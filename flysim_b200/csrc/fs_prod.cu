@@ -272,33 +272,41 @@ __device__ __forceinline__ float comp4(const float4 &q, int k) {
   return k == 0 ? q.x : k == 1 ? q.y : k == 2 ? q.z : q.w;
 }
 
-// Lanes work in quads: the four lanes of a quad take the same edge and each
-// loads one of its window's 16-byte vectors (lane k: steps 4k..4k+3), so one
-// warp load instruction covers eight edges whose vectors share a cache line
-// per edge (about 1.25 L1 wavefronts per edge instead of 3 for a lane per
-// edge); each lane keeps U edges in flight.  The next round's edge codes
-// and weights are fetched while the current windows are in flight.  Quad g
-// sums the post's edges g, g + 8, g + 16, ... in that order whatever U is
-// (U only sets how many are in flight), then the eight quads are combined
-// by a butterfly, so the sums depend on neither U nor the block plan.
+// Lanes work in groups that each take one edge, lane k of a group loading
+// vector k of the edge's window (steps 4k..4k+3), so one warp load covers a
+// group's worth of edges whose vectors share a cache line per edge (about
+// 1.25 L1 wavefronts per edge instead of 3 for a lane per edge); each lane
+// keeps U edges in flight, and the next round's edge codes and weights are
+// fetched while the current windows are in flight.  Networks whose interval
+// is at most 12 steps (batches of at most 12 steps: three vectors) use
+// triads, lanes 3g + k for g < 10 (lanes 30 and 31 idle), so a warp load
+// covers ten edges; the others use quads, lanes 4g + k for g < 8.  Group g
+// sums the post's edges g, g + G, g + 2G, ... (G = 10 or 8) in that order
+// whatever U is (U only sets how many are in flight); then triads are
+// combined in a fixed tree (g + 5 onto g, then g + 3, g + 2 and g + 1) and
+// quads by an xor butterfly over the eight groups.  The group size depends
+// on the network's interval alone, so the sums depend on neither U, the
+// block plan, the kernel nor the length of a batch.
 template <int U>
 __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint32_t np, uint64_t tb, uint32_t L,
                                               float (*gn)[kTile], uint32_t wid, uint32_t lane) {
-  constexpr uint32_t CH = 8u * U;      // edges per warp round
   const float4 *sh = (const float4 *)P.s_hist;
   const uint32_t S4 = P.slots >> 2, qmask = S4 - 1, mask = P.mask;
   const uint32_t nvl = (L + 3u) >> 2;  // vectors needed for L steps
   const uint32_t nw = kThreads / 32;
-  const uint32_t k = lane & 3u, g = lane >> 2;
-  const bool kv = k < nvl;
+  const bool tri = P.interval <= 12u;
+  const uint32_t G = tri ? 10u : 8u;   // groups (edges per warp load)
+  const uint32_t CH = G * U;           // edges per warp round
+  const uint32_t g = tri ? lane / 3u : lane >> 2, k = tri ? lane - 3u * g : lane & 3u;
+  const bool gv = g < G, kv = gv && k < nvl;
   uint32_t code[U];
   float w[U];
   auto fetch = [&](uint32_t base, uint32_t end) {
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      const uint32_t eu = base + g + 8u * u;
-      code[u] = eu < end ? __ldg(P.in_code + eu) : 0u;
-      w[u] = eu < end ? __ldg(P.in_w + eu) : 0.0f;
+      const uint32_t eu = base + g + G * u;
+      code[u] = gv && eu < end ? __ldg(P.in_code + eu) : 0u;
+      w[u] = gv && eu < end ? __ldg(P.in_w + eu) : 0.0f;
     }
   };
   uint32_t q = wid, b0 = 0, b1 = 0;
@@ -321,7 +329,7 @@ __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint
       float4 v[U];
 #pragma unroll
       for (int u = 0; u < U; u++) {
-        const bool ok = kv && e + 8u * u < b1;
+        const bool ok = kv && e + G * u < b1;
         const uint32_t pre = code[u] & 0xffffffu, d = code[u] >> 24;
         const uint32_t a = (uint32_t)(tb - 1u - d) & mask;
         const float4 *row = sh + ((size_t)pre * kSH + (a & 3u)) * S4;
@@ -341,11 +349,27 @@ __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint
       }
     }
     if (nch == 0 && qn < np) fetch(n0, n1);
+    if (tri) {
+      // g + 5 onto g (g < 5), g + 3 onto g (g < 2), then g + 2 and g + 1
+      // onto g = 0: lane k ends with its four steps' sums
 #pragma unroll
-    for (int o = 4; o < 32; o <<= 1)
+      for (int i = 0; i < 4; i++) {
+        float t = __shfl_down_sync(fsd::kFull, acc[i], 15);
+        if (g < 5u) acc[i] += t;
+        t = __shfl_down_sync(fsd::kFull, acc[i], 9);
+        if (g < 2u) acc[i] += t;
+        t = __shfl_down_sync(fsd::kFull, acc[i], 6);
+        if (g == 0u) acc[i] += t;
+        t = __shfl_down_sync(fsd::kFull, acc[i], 3);
+        if (g == 0u) acc[i] += t;
+      }
+    } else {
 #pragma unroll
-      for (int i = 0; i < 4; i++) acc[i] += __shfl_xor_sync(fsd::kFull, acc[i], o);
-    if (lane < 4) {
+      for (int o = 4; o < 32; o <<= 1)
+#pragma unroll
+        for (int i = 0; i < 4; i++) acc[i] += __shfl_xor_sync(fsd::kFull, acc[i], o);
+    }
+    if (lane < (tri ? 3u : 4u)) {
 #pragma unroll
       for (int i = 0; i < 4; i++) {
         const uint32_t j = 4u * lane + (uint32_t)i;
@@ -1484,7 +1508,7 @@ __device__ __forceinline__ void params_to_smem(Params &Psh, const Params *__rest
 }
 
 template <class T, int U>
-__global__ void __launch_bounds__(kThreads, U == 4 ? 4 : 3) k_tile_pull(const Params *__restrict__ Ps,
+__global__ void __launch_bounds__(kThreads, U == 4 ? 4 : 2) k_tile_pull(const Params *__restrict__ Ps,
                                                           const IvTile *__restrict__ tiles, uint32_t bs,
                                                           uint32_t L) {
   __shared__ __align__(16) Params Psh;
@@ -3172,7 +3196,7 @@ int tiles_solo_create(Prod *p, std::string &err) {
   p->tiles = new Tiles();
   p->tiles->fp64 = p->fp64;
   std::vector<Prod *> one{p};
-  return tiles_plan(*p->tiles, one, p->fp64 ? TileW<double>::W : kTile, 8, err);
+  return tiles_plan(*p->tiles, one, p->fp64 ? TileW<double>::W : kTile, 4, err);
 }
 
 void tiles_delete(Tiles *T) {
