@@ -132,8 +132,11 @@ struct Params {
   float *gv_st, *gv_xt;  // [steps][gv_n]
   uint32_t *t1_cnt;      // [4] overflow entries of step t, slot t mod 4
   uint32_t t1_slots;     // entries per block region of a step's list
-  uint4 *t1_list;        // [2][blocks][t1_slots][2] (id, inc, c0, c1), (c2, c3, step + 1, 0)
-  uint4 *t1_ovf;         // [2][n][2] the overflow lists
+  uint32_t t1_w;         // 16-byte words per list entry: 1 or 2
+  uint4 *t1_list;        // [2][blocks][t1_slots][t1_w]: (id, inc, c, step + 1) when every neuron
+                         // projects onto at most one linear receptor (c: that receptor's),
+                         // else (id, inc, c0, c1), (c2, c3, step + 1, 0)
+  uint4 *t1_ovf;         // [2][n][t1_w] the overflow lists
 };
 
 // Block plan of k_prod1: posts [post0, post0 + np); tracked neurons [trk0,
@@ -686,7 +689,8 @@ __device__ __forceinline__ void nmda_pre_step(T &xp, T &spre, bool spk, T inc, T
 template <class T, bool kTM = true>
 __device__ __forceinline__ bool neuron_step(const Params &P, const NeuronPar<T> &q, NeuronState<T> &st,
                                             const long long (&rv)[4], T gnmda, uint32_t hit, T gauss, T gapI,
-                                            uint32_t p, bool own, uint32_t s, T (&cinc)[4], T &inc_out) {
+                                            uint32_t p, bool own, uint32_t s, T (&cinc)[4], T &inc_out,
+                                            const float *tm = nullptr) {
   const uint32_t n = P.n;
   T g[5];
 #pragma unroll
@@ -778,15 +782,17 @@ __device__ __forceinline__ bool neuron_step(const Params &P, const NeuronPar<T> 
     else if (P.plast == PL_STP) inc = (T)P.D[p] * (T)P.F[p];
     else if (kTM && (q.pj & kPjTM)) {
       T u = (T)st.tmu, x = (T)st.tmx;
-      const T U = (T)__ldg(P.tm_U + p);
+      // parameters from the caller's per-thread copy (tm: U, dff, dfr) or
+      // from global memory
+      const T U = (T)(tm ? tm[0] : __ldg(P.tm_U + p));
       if (spk) {
         u = u + U * ((T)1 - u);
         const T rel = u * x;
         inc = rel;
         x = x - rel;
       } else {
-        u = U + (u - U) * (T)__ldg(P.tm_dff + p);
-        x = (T)1 + (x - (T)1) * (T)__ldg(P.tm_dfr + p);
+        u = U + (u - U) * (T)(tm ? tm[1] : __ldg(P.tm_dff + p));
+        x = (T)1 + (x - (T)1) * (T)(tm ? tm[2] : __ldg(P.tm_dfr + p));
       }
       st.tmu = (float)u;
       st.tmx = (float)x;
@@ -860,32 +866,55 @@ __device__ __forceinline__ void gv_write(const Params &P, uint32_t p, uint32_t s
 // ring slots of the next PD steps are in flight while the current step
 // computes (they are final: every push into them happened before the
 // interval began); a warp pushes the spikes of its own lanes, so a step
-// needs no block barrier.
+// needs no block barrier.  neuron_load issues a thread's loads (parameters,
+// state, Tsodyks-Markram parameters into its shared-memory copy, the first
+// ring slots).  (Issuing them before the batch's drive draws, to overlap
+// the draws, measured the same on the 1 M network: 0.7538 -> 0.7541.)
+template <class T>
+struct StepRegs {
+  NeuronPar<T> q;
+  NeuronState<T> st;
+  long long rv[4], rv2[4];  // ring slots of the first steps (step 0, step 1)
+};
+
+template <class T, int PD>
+__device__ __forceinline__ void neuron_load(const Params &P, uint32_t p0, uint32_t np, uint32_t sb, uint32_t L,
+                                            StepRegs<T> &R, float *tm3) {
+  static_assert(PD == 1 || PD == 2, "ring prefetch distance 1 or 2");
+  const uint32_t tid = threadIdx.x, mask = P.mask;
+  const bool own = tid < np;
+  const uint32_t p = own ? p0 + tid : p0;  // non-owners read a valid neuron, write nothing
+  load_neuron<T>(P, p, R.q, R.st);
+  if (R.q.pj & kPjTM) {
+    tm3[3 * tid] = P.tm_U[p];
+    tm3[3 * tid + 1] = P.tm_dff[p];
+    tm3[3 * tid + 2] = P.tm_dfr[p];
+  }
+  const uint32_t tprev = (uint32_t)(P.t0 + sb - 1u) & mask, tn = (uint32_t)(P.t0 + sb) & mask;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int ri = P.lin_of_rec[r];
+    R.rv[r] = (ri >= 0 && own) ? (long long)__ldcg(ring_at(P, ri, p, tprev)) : 0ll;
+    R.rv2[r] = (PD == 2 && ri >= 0 && own && L > 1) ? (long long)__ldcg(ring_at(P, ri, p, tn)) : 0ll;
+  }
+}
+
+// The L steps of neuron_load's neuron; tm3: the thread's Tsodyks-Markram
+// parameters (read every step from shared memory rather than from global
+// memory on the step's dependency chain).
 template <class T, int PD>
 __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint32_t np, uint32_t sb, uint32_t L,
                                              T (*gn)[TileW<T>::W], const uint8_t (*hits)[TileW<T>::W],
                                              const T (*gauss)[TileW<T>::W], const SpikeList<T> &lst,
-                                             const T *gapI) {
+                                             const T *gapI, StepRegs<T> &R, const float *tm3) {
   const uint32_t tid = threadIdx.x, lane = tid & 31;
   const uint32_t n = P.n, S = P.slots, mask = P.mask;
   const bool own = tid < np;
-  const uint32_t p = own ? p0 + tid : p0;  // non-owners read a valid neuron, write nothing
-  NeuronPar<T> q;
-  NeuronState<T> st;
-  load_neuron<T>(P, p, q, st);
+  const uint32_t p = own ? p0 + tid : p0;
+  NeuronPar<T> &q = R.q;
+  NeuronState<T> &st = R.st;
+  long long(&rv)[4] = R.rv, (&rv2)[4] = R.rv2;
   uint32_t nsp = 0;
-  // ring slots of the first steps: rv for step 0, rv2 for step 1 (PD == 2)
-  static_assert(PD == 1 || PD == 2, "ring prefetch distance 1 or 2");
-  long long rv[4], rv2[4];
-  {
-    const uint32_t tprev = (uint32_t)(P.t0 + sb - 1u) & mask, tn = (uint32_t)(P.t0 + sb) & mask;
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-      const int ri = P.lin_of_rec[r];
-      rv[r] = (ri >= 0 && own) ? (long long)__ldcg(ring_at(P, ri, p, tprev)) : 0ll;
-      rv2[r] = (PD == 2 && ri >= 0 && own && L > 1) ? (long long)__ldcg(ring_at(P, ri, p, tn)) : 0ll;
-    }
-  }
   for (uint32_t j = 0; j < L; j++) {
     const uint32_t s = sb + j;
     const uint64_t t = P.t0 + s;
@@ -909,7 +938,7 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
     const uint32_t qs = tid < np ? tid : 0;
     T cinc[4], inc;
     const bool spk = neuron_step<T>(P, q, st, cur, gn[j][qs], hits[j][qs], gauss[j][qs],
-                                    P.gap_row ? gapI[qs] : (T)0, p, own, s, cinc, inc);
+                                    P.gap_row ? gapI[qs] : (T)0, p, own, s, cinc, inc, tm3 + 3 * tid);
     nsp += spk ? 1u : 0u;
     if (own && P.gv_row) gv_write<T>(P, p, s, st);
     if (own && (q.pj & (1u << FS_NMDA))) {
@@ -962,7 +991,7 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
 template <class T>
 struct TileBufs {
   static constexpr uint32_t kT = TileW<T>::W;
-  static constexpr uint32_t kCap = sizeof(T) == 4 ? 448 : 192;
+  static constexpr uint32_t kCap = sizeof(T) == 4 ? 320 : 192;
   T gn[kLB][kT];
   T gauss[kLB][kT];
   T gapI[kT];
@@ -993,6 +1022,10 @@ __device__ __forceinline__ void tile_steps(const Params &P, uint32_t tp0, uint32
   constexpr uint32_t kCap = TileBufs<T>::kCap;
   const SpikeList<T> lst{&B.l_n, B.l_p, B.l_tm, B.l_c, kCap};
   const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  // warps without neurons in this tile skip the steps
+  const bool act = (tid & ~31u) < np;
+  __shared__ float tm3[kThreads * 3];
+  StepRegs<T> R;
   draw_inputs<T>(P, tp0, np, P.t0 + bs, L, B.hits, B.gauss);
   if (P.gap_row) {
     // gap currents of this step (interval 1): g (V_other - V_self) over
@@ -1012,8 +1045,8 @@ __device__ __forceinline__ void tile_steps(const Params &P, uint32_t tp0, uint32
   }
   __syncthreads();
   pc.mark(1);
-  // warps without neurons in this tile skip the steps
-  if ((tid & ~31u) < np) neuron_steps<T, PD>(P, tp0, np, bs, L, B.gn, B.hits, B.gauss, lst, B.gapI);
+  if (act) neuron_load<T, PD>(P, tp0, np, bs, L, R, tm3);
+  if (act) neuron_steps<T, PD>(P, tp0, np, bs, L, B.gn, B.hits, B.gauss, lst, B.gapI, R, tm3);
   __syncthreads();
   pc.mark(2);
   // the batch's spikes: with fewer spikes than warps the whole block
@@ -1261,18 +1294,19 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
       const uint32_t par = (uint32_t)(t - 1u) & 1u;
       const uint32_t tag = (uint32_t)(t - 1u) + 1u;  // entries of step t - 1 carry it
       const uint32_t nreg = gridDim.x * P.t1_slots;   // block-region entries (<= kT1F)
-      const uint4 *reg = P.t1_list + (size_t)par * nreg * 2;
-      const uint4 *ovf = P.t1_ovf + (size_t)par * n * 2;
+      const uint32_t W = P.t1_w;
+      const uint4 *reg = P.t1_list + (size_t)par * nreg * W;
+      const uint4 *ovf = P.t1_ovf + (size_t)par * n * W;
       // the regions' entries are loaded with the overflow count (one round
       // trip); stale entries carry another step's tag
       uint4 a0 = make_uint4(0u, 0u, 0u, 0u), b0 = a0;
       if (tid < nreg) {
-        a0 = __ldcg(reg + 2 * (size_t)tid);
-        b0 = __ldcg(reg + 2 * (size_t)tid + 1);
+        a0 = __ldcg(reg + W * (size_t)tid);
+        if (W == 2) b0 = __ldcg(reg + 2 * (size_t)tid + 1);
       }
       const uint32_t cnt = nreg + __ldcg(P.t1_cnt + ((uint32_t)(t - 1u) & 3u));
       pc.lap(8, cnt);    // the list's entry count is in
-      pc.lap(12, b0.w);  // thread 0's entries are in
+      pc.lap(12, a0.x);  // thread 0's entries are in
       for (uint32_t c0 = 0; c0 < cnt; c0 += kT1F) {
         if (tid == 0) {
           f_n = 0;
@@ -1282,12 +1316,13 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
         const uint32_t i = c0 + tid;
         if (tid < kT1F && i < cnt) {
           uint4 a = a0, b = b0;
-          if (i >= nreg) {  // an overflow entry: every one is of step t - 1
-            a = __ldcg(ovf + 2 * (size_t)(i - nreg));
-            b = __ldcg(ovf + 2 * (size_t)(i - nreg) + 1);
-            b.z = tag;
+          const bool over = i >= nreg;  // an overflow entry: every one is of step t - 1
+          if (over) {
+            a = __ldcg(ovf + W * (size_t)(i - nreg));
+            if (W == 2) b = __ldcg(ovf + 2 * (size_t)(i - nreg) + 1);
           }
-          const int j = b.z == tag ? find_tracked(bits, rank, me.w0, me.nwd, a.x) : -1;
+          const bool cur = over || (W == 2 ? b.z : a.w) == tag;
+          const int j = cur ? find_tracked(bits, rank, me.w0, me.nwd, a.x) : -1;
           if (j >= 0) {
             const uint32_t sl = perm[j];
             if (cls[sl] != 255) {
@@ -1299,9 +1334,9 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
               const uint32_t k = atomicAdd(&f_n, 1u);
               f_j[k] = (uint32_t)j;
               f_c[k][0] = __uint_as_float(a.z);
-              f_c[k][1] = __uint_as_float(a.w);
-              f_c[k][2] = __uint_as_float(b.x);
-              f_c[k][3] = __uint_as_float(b.y);
+              f_c[k][1] = __uint_as_float(W == 2 ? a.w : a.z);
+              f_c[k][2] = __uint_as_float(W == 2 ? b.x : a.z);
+              f_c[k][3] = __uint_as_float(W == 2 ? b.y : a.z);
             }
           }
         }
@@ -1407,15 +1442,22 @@ __global__ void __launch_bounds__(kT1, 1) k_prod1(const __grid_constant__ Params
         base = __shfl_sync(fsd::kFull, base, leader);
         if (spk) {
           const uint32_t k = base + __popc(m & ((1u << lane) - 1u));
+          const uint32_t W = P.t1_w;
           uint4 *e;
           if (k < P.t1_slots) {
-            e = P.t1_list + (((size_t)par * gridDim.x + blockIdx.x) * P.t1_slots + k) * 2;
+            e = P.t1_list + (((size_t)par * gridDim.x + blockIdx.x) * P.t1_slots + k) * W;
           } else {
             const uint32_t o = atomicAdd(P.t1_cnt + ((uint32_t)t & 3u), 1u);
-            e = P.t1_ovf + ((size_t)par * n + o) * 2;
+            e = P.t1_ovf + ((size_t)par * n + o) * W;
           }
-          __stcg(e, make_uint4(p, __float_as_uint(inc), __float_as_uint(cinc[0]), __float_as_uint(cinc[1])));
-          __stcg(e + 1, make_uint4(__float_as_uint(cinc[2]), __float_as_uint(cinc[3]), (uint32_t)t + 1u, 0u));
+          if (W == 2) {
+            __stcg(e, make_uint4(p, __float_as_uint(inc), __float_as_uint(cinc[0]), __float_as_uint(cinc[1])));
+            __stcg(e + 1, make_uint4(__float_as_uint(cinc[2]), __float_as_uint(cinc[3]), (uint32_t)t + 1u, 0u));
+          } else {
+            // at most one receptor's c is not 0: the sum is that c exactly
+            const float cl = ((cinc[0] + cinc[1]) + cinc[2]) + cinc[3];
+            __stcg(e, make_uint4(p, __float_as_uint(inc), __float_as_uint(cl), (uint32_t)t + 1u));
+          }
         }
         if (s + 1 == P.nsteps) {
           // the launch's last step: its spikes go into the delay ring, which
@@ -1709,7 +1751,7 @@ int launch(Prod *p, uint32_t nsteps, bool want_bits, bool wantV, cudaStream_t st
   // apart by their step tag; a reset or a restored checkpoint moves the
   // step counter back)
   if (p->single && (cudaMemsetAsync(P.t1_cnt, 0, 16, st) != cudaSuccess ||
-                    cudaMemsetAsync(P.t1_list, 0, (size_t)2 * p->b1_blocks * P.t1_slots * 32, st) != cudaSuccess)) {
+                    cudaMemsetAsync(P.t1_list, 0, (size_t)2 * p->b1_blocks * P.t1_slots * 16 * P.t1_w, st) != cudaSuccess)) {
     err = "memset";
     return FS_ERR_CUDA;
   }
@@ -1962,21 +2004,21 @@ static bool plan_single(uint32_t n, uint32_t nlin, uint32_t sm_count, const std:
                         const std::vector<float> &out_w, const std::vector<float> &p_dfxt,
                         const std::vector<float> &p_dfst, const std::vector<float> &p_efas, const uint8_t *proj,
                         Single &S1, std::string &why) {
-  const uint32_t units = (n + 31) / 32, per = kT1 / 32;
+  // the posts are cut into blocks at groups of four (the NMDA sums' unit),
+  // balancing the rows of 32 edge entries the groups take (each group's
+  // longest post) plus one row's worth per group for its other work: the
+  // sums phase, proportional to the rows, is the longest of a step
+  const uint32_t units = (n + 3) / 4, per = kT1 / 4;
   uint32_t B = std::min<uint32_t>(sm_count, units);
   if (B == 0 || (uint64_t)B * per < units) {
     why = "more than 512 posts per block would be needed";
     return false;
   }
-  // linear in-degree per post
-  std::vector<uint32_t> lin_in(n, 0);
-  for (uint32_t e = 0; e < out_code.size(); e++) lin_in[out_code[e] & 0x3fffffu]++;
   std::vector<double> pre(units + 1, 0.0);
   for (uint32_t u = 0; u < units; u++) {
-    double c = 0;
-    for (uint32_t q = u * 32; q < std::min(n, u * 32 + 32); q++)
-      c += 24.0 + (double)(in_row[q + 1] - in_row[q]) + 0.25 * lin_in[q];
-    pre[u + 1] = pre[u] + c;
+    uint32_t R = 0;
+    for (uint32_t q = u * 4; q < std::min(n, u * 4 + 4); q++) R = std::max(R, (in_row[q + 1] - in_row[q] + 7) / 8);
+    pre[u + 1] = pre[u] + 1.0 + (double)R;
   }
   std::vector<uint32_t> cut(B + 1, units);
   cut[0] = 0;
@@ -2029,7 +2071,7 @@ static bool plan_single(uint32_t n, uint32_t nlin, uint32_t sm_count, const std:
   for (uint32_t a = 0; a < n; a++)
     for (uint32_t e = out_row[a]; e < out_row[a + 1]; e++) {
       const uint32_t post = out_code[e] & 0x3fffffu;
-      lin_b[blk_of_unit[post >> 5]].push_back(((uint64_t)a << 32) | e);
+      lin_b[blk_of_unit[post >> 2]].push_back(((uint64_t)a << 32) | e);
     }
   std::vector<int32_t> loc(n, -1);
   S1.blk.clear();
@@ -2038,7 +2080,7 @@ static bool plan_single(uint32_t n, uint32_t nlin, uint32_t sm_count, const std:
   size_t smax = 0;
   bool big_lin = false;
   for (uint32_t b = 0; b < B; b++) {
-    const uint32_t P0 = cut[b] * 32, P1 = std::min(n, cut[b + 1] * 32);
+    const uint32_t P0 = cut[b] * 4, P1 = std::min(n, cut[b + 1] * 4);
     std::vector<uint64_t> &L = lin_b[b];
     std::sort(L.begin(), L.end());
     std::vector<uint32_t> trk;
@@ -2173,7 +2215,7 @@ static bool validate_single(const HostNet &H, const Single &S1, std::string &err
   uint64_t lin_total = 0, nmda_total = 0;
   for (uint32_t b = 0; b < S1.blk.size(); b++) {
     const Blk1 &k = S1.blk[b];
-    if (k.post0 != next_post || k.post0 % 32 || k.np == 0 || k.np > kT1 || k.post0 + k.np > n)
+    if (k.post0 != next_post || k.post0 % 4 || k.np == 0 || k.np > kT1 || k.post0 + k.np > n)
       return fail(b, "post range");
     next_post = k.post0 + k.np;
     const uint32_t ng = (k.np + 3) / 4;
@@ -2490,6 +2532,11 @@ static int prod_create_from(Prod **out, const fs_net_desc *d, const fs_run_opts 
         if ((rc = dup(p, (uint16_t **)&P.t1_rank, S1.rank.data(), S1.rank.size(), st, err))) goto fail;
         if ((rc = dup(p, &P.t1_cnt, (const uint32_t *)nullptr, 4, st, err))) goto fail;
         P.t1_slots = std::min<uint32_t>(16, kT1F / (uint32_t)S1.blk.size());
+        // one 16-byte word per listed spike when no neuron projects onto two
+        // linear receptors (its one c travels alone), else two
+        P.t1_w = 1;
+        for (uint32_t i = 0; i < n; i++)
+          if (__builtin_popcount(proj[i] & 15u) > 1) P.t1_w = 2;
         if ((rc = dup(p, &P.t1_list, (const uint4 *)nullptr, (size_t)2 * S1.blk.size() * P.t1_slots * 2, st, err)) ||
             (rc = dup(p, &P.t1_ovf, (const uint4 *)nullptr, (size_t)4 * n, st, err)))
           goto fail;

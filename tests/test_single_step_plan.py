@@ -44,13 +44,14 @@ def test_plan_of_reference_networks(built, case):
 
 @pytest.mark.parametrize("n", [33, 700, 4735, 12345])
 def test_plan_of_small_and_ragged_networks(built, n):
-    # one warp per block up to the 512-post maximum per block
+    # blocks cut at groups of four posts, up to one block per SM and the
+    # 512-post maximum per block
     from flysim_b200 import netgen, network
     c = netgen.connectome_fast(n=n, regions=max(2, n // 345), delays=False, seed=13)
     na = network.connectome_net(c, with_delays=False)
     st = built.single_step_plan(na.desc, 148)
     assert st["qualifies"] == 1, built.lib().fs_last_error(None)
-    assert st["blocks"] == min(148, (n + 31) // 32) and st["max_posts"] <= 512
+    assert st["blocks"] == min(148, (n + 3) // 4) and st["max_posts"] <= 512
 
 
 def test_oversized_blocks_fall_back(built):
