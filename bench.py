@@ -268,7 +268,9 @@ def run_compat(args, rank):
     """--mode compat: the reference-order engine (the mode whose files equal
     the reference's byte for byte) on the 20k network with delays 0, read
     from its .conf like the reference reads it; --ltp adds long-term
-    plasticity, which only this mode runs.  One step = 1 s simulated."""
+    plasticity (-LTP, the keywords' default parameters), in any mode (the
+    production modes run it on their LTP kernel).  One step = 1 s
+    simulated."""
     import flysim_b200 as fb
     from flysim_b200 import netgen
     if rank != 0:
@@ -280,8 +282,28 @@ def run_compat(args, rank):
         netgen.write_connectome(c, conf, with_delays=False)
         netgen.write_pro(pro, 1000.0, seeds=(SEED,), outputs=())
         m = fb.Model(conf, pro, ltp=args.ltp)
-        eng = fb.Engine(m.desc(), "compat", chunk_steps=1000)
+        eng = fb.Engine(m.desc(), args.mode, chunk_steps=1000)
         eng.reset(m.seed())
+        if args.profile_steps:
+            # one run (for ncu), with --phase-clock the LTP kernel's phases
+            eng.run(args.profile_steps // 4)
+            eng.sync()
+            if args.phase_clock:
+                eng.phase_clock(True)
+            eng.run(args.profile_steps)
+            eng.sync()
+            line = {"profile_steps": args.profile_steps, "stats": eng.stats(), "layout": eng.layout()}
+            if args.phase_clock and eng.layout()["kernel"] == "ltp":
+                ph = eng.phase_times().astype(np.float64) / args.profile_steps
+                names = {0: "nmda pull", 1: "drive draws", 2: "neuron steps", 4: "barrier after steps",
+                         5: "pushes", 6: "barrier after pushes", 7: "ltp rules"}
+                line["cycles_per_timestep"] = {nm: {"mean": round(float(ph[:, k].mean()), 1),
+                                                    "max": round(float(ph[:, k].max()), 1)}
+                                               for k, nm in names.items()}
+            print(json.dumps(line))
+            eng.close()
+            m.close()
+            return 0
         for _ in range(args.warmup):
             eng.run_timed(STEPS_PER_BENCH_STEP // 10)
         ms = [eng.run_timed(STEPS_PER_BENCH_STEP) for _ in range(args.steps)]
@@ -293,12 +315,14 @@ def run_compat(args, rank):
     tot = float(np.sum(ms))
     sim_s = args.steps * STEPS_PER_BENCH_STEP * DT * 1e-3
     print(json.dumps({
-        "metric": METRIC + ", compat mode" + (" with LTP" if args.ltp else ""), "value": sim_s / (tot * 1e-3),
+        "metric": METRIC + ", %s mode" % args.mode + (" with LTP" if args.ltp else ""), "value": sim_s / (tot * 1e-3),
         "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": tot / args.steps, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "connectome-shaped network, 20000 neurons, delays 0, read from its .conf; "
-                               "compat mode (reference operation order and random streams)%s; one step = 1 s "
-                               "simulated" % (", -LTP" if args.ltp else "")},
+                               "%s%s; one step = 1 s simulated" % (
+                                   "compat mode (reference operation order and random streams)"
+                                   if args.mode == "compat" else args.mode + " mode",
+                                   ", -LTP" if args.ltp else "")},
         "gpu_launches": st["launches"], "spikes": st["spikes"]}))
     return 0
 
@@ -380,7 +404,8 @@ def main():
     ap.add_argument("--mode", default="fp32", choices=["fp32", "fp64", "compat"],
                     help="compat: the reference-order engine on the delays-0 network read from its .conf "
                          "(a measurement line of its own, not the headline)")
-    ap.add_argument("--ltp", action="store_true", help="with --mode compat: run the network with -LTP")
+    ap.add_argument("--ltp", action="store_true",
+                    help="run the delays-0 network read from its .conf with -LTP (any mode; its own line)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-same-network", action="store_true",
                     help="skip the delays-0 measurement of the network the reference arm runs")
@@ -396,7 +421,7 @@ def main():
     if args.impl == "reference":
         return run_reference(args, rank)
 
-    if args.mode == "compat":
+    if args.mode == "compat" or args.ltp:
         return run_compat(args, rank)
     import torch
     import torch.distributed as dist

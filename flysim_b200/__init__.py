@@ -66,7 +66,8 @@ class CompatLayout(C.Structure):
 
 
 class SynList(C.Structure):
-    _fields_ = [("n", C.c_uint64), ("pre", _u32), ("post", _u32), ("rec", _u8), ("g", _f), ("delay", _u16)]
+    _fields_ = [("n", C.c_uint64), ("pre", _u32), ("post", _u32), ("rec", _u8), ("g", _f), ("delay", _u16),
+                ("ltp", _u8)]
 
 
 class TmParams(C.Structure):
@@ -136,6 +137,7 @@ def lib() -> C.CDLL:
         "fs_debug_expf": (C.c_int, [_f, _f, C.c_uint64]),
         "fs_debug_expf_noalloc": (C.c_int, [_f, _f, C.c_uint64]),
         "fs_get_state": (C.c_int, [vp, _f, _i32, _u32]),
+        "fs_get_weights": (C.c_int, [vp, _f, C.c_uint64]),
         "fs_debug_barrier_timeout": (C.c_int, [C.c_uint32]),
         "fs_debug_philox": (C.c_int, [_u32, _u32, C.c_uint64, _u32]),
         "fs_engine_layout": (C.c_int, [vp, _u32, _u32, _u32, C.POINTER(C.c_int)]),
@@ -202,7 +204,7 @@ def exported_symbols() -> Sequence[str]:
                         "fs_reset", "fs_set_drive", "fs_set_act", "fs_set_injection", "fs_step", "fs_run",
                         "fs_run_timed",
                         "fs_sync", "fs_stats", "fs_kernel_time", "fs_debug_expf", "fs_debug_expf_noalloc",
-                        "fs_get_state", "fs_debug_barrier_timeout", "fs_engine_layout",
+                        "fs_get_state", "fs_get_weights", "fs_debug_barrier_timeout", "fs_engine_layout",
                         "fs_debug_single_step_plan", "fs_debug_philox",
                         "fs_debug_drive",
                         "fs_debug_inject_wait_failure", "fs_debug_phase_clock", "fs_debug_phase_times",
@@ -458,11 +460,11 @@ class Engine:
 
     def layout(self):
         """Launch layout (production modes): blocks, threads, interval and
-        the kernels that run the network ("interval", "single_step" or
-        "tiles")."""
+        the kernels that run the network ("interval", "single_step",
+        "tiles" or "ltp")."""
         b, t, i, k = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_int()
         _check(lib().fs_engine_layout(self._h, C.byref(b), C.byref(t), C.byref(i), C.byref(k)), self._h)
-        kind = {0: "interval", 1: "single_step", 2: "tiles"}[k.value]
+        kind = {0: "interval", 1: "single_step", 2: "tiles", 3: "ltp"}[k.value]
         return dict(blocks=b.value, threads=t.value, interval=i.value, kernel=kind,
                     single_step=kind == "single_step")
 
@@ -490,6 +492,13 @@ class Engine:
         _check(lib().fs_get_state(self._h, V.ctypes.data_as(_f), cnt.ctypes.data_as(_i32),
                                   ns.ctypes.data_as(_u32)), self._h)
         return V, cnt, ns
+
+    def weights(self, n_syn: int) -> np.ndarray:
+        """Synaptic weights in synapse-list order as long-term plasticity has
+        made them (production modes, networks with LTP)."""
+        g = np.zeros(n_syn, np.float32)
+        _check(lib().fs_get_weights(self._h, g.ctypes.data_as(_f), C.c_uint64(n_syn)), self._h)
+        return g
 
     def checkpoint(self) -> bytes:
         """The handle's state after its last step (production modes), for

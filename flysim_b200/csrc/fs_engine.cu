@@ -649,6 +649,15 @@ int fs_get_state(fs_handle *h, float *V, int32_t *Count, uint32_t *NState) {
   return FS_OK;
 }
 
+int fs_get_weights(fs_handle *h, float *g, uint64_t n) {
+  if (!h) return set_err(nullptr, FS_ERR_ARG, "null handle");
+  if (h->mode == FS_MODE_COMPAT || !h->prod)
+    return set_err(h, FS_ERR_UNSUPPORTED, "fs_get_weights: production modes only");
+  if (n && !g) return set_err(h, FS_ERR_ARG, "fs_get_weights: null output");
+  int rc = fsp::prod_get_weights(h->prod, g, n, h->st, h->err);
+  return rc ? set_err(h, rc, h->err) : FS_OK;
+}
+
 int fs_debug_barrier_timeout(uint32_t poll_limit) {
   if (poll_limit == 0 || poll_limit > (1u << 24))
     return set_err(nullptr, FS_ERR_ARG, "fs_debug_barrier_timeout: poll limit must be 1 .. 2^24");
@@ -669,7 +678,7 @@ int fs_engine_layout(fs_handle *h, uint32_t *blocks, uint32_t *threads, uint32_t
   if (blocks) *blocks = pi.blocks;
   if (threads) *threads = pi.threads;
   if (interval) *interval = pi.interval;
-  if (kernel) *kernel = pi.single_step ? 1 : pi.tiles ? 2 : 0;
+  if (kernel) *kernel = pi.single_step ? 1 : pi.tiles ? 2 : pi.ltp ? 3 : 0;
   return FS_OK;
 }
 

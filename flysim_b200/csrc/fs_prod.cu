@@ -109,6 +109,26 @@ struct Params {
   const uint32_t *gap_row, *gap_other;
   const float *gap_w;
   void *Vg;
+  // long-term plasticity (k_prod_ltp; null unless the network has LTP):
+  // per neuron the trace LP and its delay counter with their parameters;
+  // copies of the last two steps' LP, spike flag and presynaptic gates by
+  // step parity (the LTP phase of step t - 1 reads them while the owners
+  // advance step t); the LTP records of each neuron as presynaptic
+  // (ltp_orow: entry = post | receptor << 24, index of its weight in out_w
+  // or, for NMDA, in_w) and as postsynaptic (ltp_irow: pre | receptor <<
+  // 24, index); the NMDA sums of a step ([n]) and the spike lists of the
+  // last two steps (id, step slot, c per linear receptor; counts [2])
+  void *ltp_lp;
+  int32_t *ltp_clp;
+  const float *ltp_dflp, *ltp_pos, *ltp_neg;
+  const int32_t *ltp_spd;
+  void *ltp_lp2, *ltp_sp2;
+  uint8_t *ltp_spk2;
+  const uint32_t *ltp_orow, *ltp_oent, *ltp_oidx, *ltp_irow, *ltp_ient, *ltp_iidx;
+  void *ltp_gn;
+  uint32_t *ltp_cnt, *ltp_id;
+  uint16_t *ltp_tm;
+  void *ltp_c;
   // single-step kernel k_prod1 (null unless the network takes it): per
   // block, the presynaptic neurons it tracks (sorted ids, NMDA kinetics
   // class, rows of their linear synapses onto the block's posts), the NMDA
@@ -391,6 +411,7 @@ __device__ __forceinline__ void nmda_pull_f32(const Params &P, uint32_t p0, uint
 // persistent kernel (k_prod1) sums its shared-memory copy of the same edges
 // in the same order, so the two kernels, and a batch instance and its solo
 // run, give the same sums bit for bit.
+template <bool kMW = false>
 __device__ __forceinline__ void nmda_pull1_f32(const Params &P, uint32_t p0, uint32_t np, uint64_t tb,
                                                float (*gn)[kTile], uint32_t wid, uint32_t lane) {
   const float *sh = (const float *)P.s_hist;
@@ -410,7 +431,8 @@ __device__ __forceinline__ void nmda_pull1_f32(const Params &P, uint32_t p0, uin
     for (uint32_t e = b0 + l8; e < b1; e += 8) {
       const uint32_t pre = __ldg(P.in_code + e) & 0xffffffu;
       // row 0 of the shifted copies holds slot i at element i
-      acc = __fmaf_rn(__ldg(P.in_w + e), __ldca(sh + (size_t)pre * kSH * S + slot), acc);
+      const float w = kMW ? __ldcg(P.in_w + e) : __ldg(P.in_w + e);
+      acc = __fmaf_rn(w, __ldca(sh + (size_t)pre * kSH * S + slot), acc);
     }
 #pragma unroll
     for (int o = 4; o; o >>= 1) acc += __shfl_xor_sync(fsd::kFull, acc, o);
@@ -418,7 +440,7 @@ __device__ __forceinline__ void nmda_pull1_f32(const Params &P, uint32_t p0, uin
   }
 }
 
-template <class T>
+template <class T, bool kMW = false>
 __device__ __forceinline__ void nmda_pull(const Params &P, uint32_t p0, uint32_t np, uint64_t tb, uint32_t L,
                                           T (*gn)[TileW<T>::W], uint32_t wid, uint32_t lane) {
   const T *sh = (const T *)P.s_hist;
@@ -433,7 +455,7 @@ __device__ __forceinline__ void nmda_pull(const Params &P, uint32_t p0, uint32_t
       const uint32_t e0 = __ldg(P.in_row + p), e1 = __ldg(P.in_row + p + 1);
       for (uint32_t e = e0 + lane; e < e1; e += 32) {
         const uint32_t code = __ldg(P.in_code + e);
-        const T w = (T)__ldg(P.in_w + e);
+        const T w = (T)(kMW ? __ldcg(P.in_w + e) : __ldg(P.in_w + e));
         const uint32_t pre = code & 0xffffffu, d = code >> 24;
         const T *row = sh + (size_t)pre * S;
         const uint32_t a = (uint32_t)(tb - 1u - d) & mask;
@@ -456,7 +478,9 @@ __device__ __forceinline__ void nmda_pull(const Params &P, uint32_t p0, uint32_t
 // Threads start, start+stride, ... of a group walk the out-edges of neuron q
 // (four edges per thread per round, loads issued before the atomics) and add
 // w*c[receptor] as 2^-40 fixed point to ring[receptor][post][(tm+delay) mod S].
-template <class T>
+// kMW: the weights change during the launch (LTP), so they are read
+// through L2 rather than the read-only path.
+template <class T, bool kMW = false>
 __device__ __forceinline__ void push_spike(const Params &P, uint32_t q, uint32_t tm, const T (&cj)[4],
                                            uint32_t start, uint32_t stride) {
   const uint32_t mask = P.mask;
@@ -468,7 +492,7 @@ __device__ __forceinline__ void push_spike(const Params &P, uint32_t q, uint32_t
     for (int u = 0; u < 4; u++) {
       const uint32_t eu = e + u * stride;
       code[u] = eu < oe ? __ldg(P.out_code + eu) : 0u;
-      w[u] = eu < oe ? __ldg(P.out_w + eu) : 0.0f;
+      w[u] = eu < oe ? (kMW ? __ldcg(P.out_w + eu) : __ldg(P.out_w + eu)) : 0.0f;
     }
 #pragma unroll
     for (int u = 0; u < 4; u++) {
@@ -683,17 +707,28 @@ __device__ __forceinline__ void nmda_pre_step(T &xp, T &spre, bool spk, T inc, T
   spre = fma_t<T>(pdfst, spre, (pefas * xp) * ((T)1 - spre));
 }
 
+// Long-term plasticity trace of one neuron (k_prod_ltp): LP and its
+// back-propagation delay counter, with their parameters.  LP is float in
+// both modes, as the reference keeps it, so the weights LTP writes depend
+// only on the spike times (FP32 and FP64 runs rewrite them alike).
+template <class T>
+struct LtpTrace {
+  float lp, dflp;
+  int32_t clp, spd;
+};
+
 // One step of neuron p: fold the linear conductances' delivered sums
 // (rv: 2^-40 fixed point) into G, add the external drive (hit bits, injection
 // current) and the NMDA sum gnmda, VmEul + firing (code/EqsGnl2.cpp:152-251),
 // per-step outputs of step s, then the presynaptic state: the increment inc of
 // a spike and, per linear receptor, c = inc + st(t-1)(1 - df) for the push.
-// Returns whether the neuron spiked.
-template <class T, bool kTM = true>
+// kLTP: also the LP trace of a neuron with LTP on (lt; firLP and ltpEul,
+// code/EqsGnl2.cpp:207-216, :254-280).  Returns whether the neuron spiked.
+template <class T, bool kTM = true, bool kLTP = false>
 __device__ __forceinline__ bool neuron_step(const Params &P, const NeuronPar<T> &q, NeuronState<T> &st,
                                             const long long (&rv)[4], T gnmda, uint32_t hit, T gauss, T gapI,
                                             uint32_t p, bool own, uint32_t s, T (&cinc)[4], T &inc_out,
-                                            const float *tm = nullptr) {
+                                            const float *tm = nullptr, LtpTrace<T> *lt = nullptr) {
   const uint32_t n = P.n;
   T g[5];
 #pragma unroll
@@ -761,6 +796,9 @@ __device__ __forceinline__ bool neuron_step(const Params &P, const NeuronPar<T> 
     if (st.V > q.vth) {
       ns |= FS_NS_FIRE;
       fire_now = true;
+      if constexpr (kLTP) {
+        if (q.a & FS_ACT_LTP) ns |= FS_NS_LP_FIRE;
+      }
     }
   }
   if (fire_now) {
@@ -772,6 +810,22 @@ __device__ __forceinline__ bool neuron_step(const Params &P, const NeuronPar<T> 
     } else {
       st.cnt = 0;
       ns &= ~FS_NS_FIRE;
+    }
+  }
+  if constexpr (kLTP) {
+    if (q.a & FS_ACT_LTP) {  // firLP + ltpEul
+      if (ns & FS_NS_LP_FIRE) {
+        if (lt->clp == lt->spd) {
+          ns = (ns | FS_NS_LP_SPIKE) & ~FS_NS_LP_FIRE;
+          lt->clp = 0;
+        } else {
+          ns &= ~FS_NS_LP_SPIKE;
+          lt->clp++;
+        }
+      } else {
+        ns &= ~FS_NS_LP_SPIKE;
+      }
+      lt->lp = (ns & FS_NS_LP_SPIKE) ? __fadd_rn(lt->lp, 1.0f) : __fmul_rn(lt->dflp, lt->lp);
     }
   }
   st.ns = ns;
@@ -910,7 +964,7 @@ __device__ __forceinline__ void neuron_load(const Params &P, uint32_t p0, uint32
 // The L steps of neuron_load's neuron; tm3: the thread's Tsodyks-Markram
 // parameters (read every step from shared memory rather than from global
 // memory on the step's dependency chain).
-template <class T, int PD>
+template <class T, int PD, bool kLTP = false>
 __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint32_t np, uint32_t sb, uint32_t L,
                                              T (*gn)[TileW<T>::W], const uint8_t (*hits)[TileW<T>::W],
                                              const T (*gauss)[TileW<T>::W], const SpikeList<T> &lst,
@@ -923,6 +977,13 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
   NeuronState<T> &st = R.st;
   long long(&rv)[4] = R.rv, (&rv2)[4] = R.rv2;
   uint32_t nsp = 0;
+  LtpTrace<T> lt;
+  if constexpr (kLTP) {
+    lt.lp = ((float *)P.ltp_lp)[p];
+    lt.clp = P.ltp_clp[p];
+    lt.dflp = __ldg(P.ltp_dflp + p);
+    lt.spd = __ldg(P.ltp_spd + p);
+  }
   for (uint32_t j = 0; j < L; j++) {
     const uint32_t s = sb + j;
     const uint64_t t = P.t0 + s;
@@ -945,9 +1006,20 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
     }
     const uint32_t qs = tid < np ? tid : 0;
     T cinc[4], inc;
-    const bool spk = neuron_step<T>(P, q, st, cur, gn[j][qs], hits[j][qs], gauss[j][qs],
-                                    P.gap_row ? gapI[qs] : (T)0, p, own, s, cinc, inc, tm3 + 3 * tid);
+    const bool spk = neuron_step<T, true, kLTP>(P, q, st, cur, gn[j][qs], hits[j][qs], gauss[j][qs],
+                                                P.gap_row ? gapI[qs] : (T)0, p, own, s, cinc, inc, tm3 + 3 * tid,
+                                                &lt);
     nsp += spk ? 1u : 0u;
+    if constexpr (kLTP) {
+      // what the LTP phase of this step reads while the owners run the next
+      if (own) {
+        const uint32_t par = (uint32_t)t & 1u;
+        ((float *)P.ltp_lp2)[(size_t)par * n + p] = lt.lp;
+        P.ltp_spk2[(size_t)par * n + p] = spk ? 1 : 0;
+#pragma unroll
+        for (int r = 0; r < 4; r++) ((T *)P.ltp_sp2)[((size_t)par * 4 + r) * n + p] = st.sp[r];
+      }
+    }
     if (own && P.gv_row) gv_write<T>(P, p, s, st);
     if (own && (q.pj & (1u << FS_NMDA))) {
       if constexpr (sizeof(T) == 4) {
@@ -992,6 +1064,10 @@ __device__ __forceinline__ void neuron_steps(const Params &P, uint32_t p0, uint3
     store_neuron<T>(P, p, q, st);
     if (P.gap_row) ((T *)P.Vg)[(size_t)((P.t0 + sb) & 1u) * n + p] = st.V;
     if (P.nspk && nsp) P.nspk[p] += nsp;
+    if constexpr (kLTP) {
+      ((float *)P.ltp_lp)[p] = lt.lp;
+      P.ltp_clp[p] = lt.clp;
+    }
   }
 }
 
@@ -1022,6 +1098,24 @@ __device__ __forceinline__ void tile_pull(const Params &P, uint32_t tp0, uint32_
   }
 }
 
+// Gap currents of step bs of a tile's posts (interval 1): g (V_other -
+// V_self) over V at the end of the previous step (none before the first).
+template <class T>
+__device__ __forceinline__ void tile_gap(const Params &P, uint32_t tp0, uint32_t np, uint32_t bs, T *gapI) {
+  const uint64_t t = P.t0 + bs;
+  for (uint32_t q = threadIdx.x; q < np; q += kThreads) {
+    T acc = (T)0;
+    if (t > 0) {
+      const T *vp = (const T *)P.Vg + (size_t)((t - 1u) & 1u) * P.n;
+      const uint32_t pq = tp0 + q;
+      const T vs = __ldcg(vp + pq);
+      for (uint32_t e = __ldg(P.gap_row + pq), e1 = __ldg(P.gap_row + pq + 1); e < e1; e++)
+        acc = acc + (T)__ldg(P.gap_w + e) * (__ldcg(vp + __ldg(P.gap_other + e)) - vs);
+    }
+    gapI[q] = acc;
+  }
+}
+
 // The rest of a tile's batch of L steps once its NMDA sums are in B.gn: the
 // drive draws, gap currents, the neurons' steps and the spikes' pushes.
 template <class T, int PD>
@@ -1035,22 +1129,7 @@ __device__ __forceinline__ void tile_steps(const Params &P, uint32_t tp0, uint32
   __shared__ float tm3[kThreads * 3];
   StepRegs<T> R;
   draw_inputs<T>(P, tp0, np, P.t0 + bs, L, B.hits, B.gauss);
-  if (P.gap_row) {
-    // gap currents of this step (interval 1): g (V_other - V_self) over
-    // V at the end of the previous step (none before the first step)
-    const uint64_t t = P.t0 + bs;
-    for (uint32_t q = tid; q < np; q += kThreads) {
-      T acc = (T)0;
-      if (t > 0) {
-        const T *vp = (const T *)P.Vg + (size_t)((t - 1u) & 1u) * P.n;
-        const uint32_t pq = tp0 + q;
-        const T vs = __ldcg(vp + pq);
-        for (uint32_t e = __ldg(P.gap_row + pq), e1 = __ldg(P.gap_row + pq + 1); e < e1; e++)
-          acc = acc + (T)__ldg(P.gap_w + e) * (__ldcg(vp + __ldg(P.gap_other + e)) - vs);
-      }
-      B.gapI[q] = acc;
-    }
-  }
+  if (P.gap_row) tile_gap<T>(P, tp0, np, bs, B.gapI);
   __syncthreads();
   pc.mark(1);
   if (act) neuron_load<T, PD>(P, tp0, np, bs, L, R, tm3);
@@ -1123,6 +1202,196 @@ __device__ __forceinline__ void prod_blocks(const Params &P, uint32_t B0, uint32
 template <class T, int PU>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) k_prod(const __grid_constant__ Params P) {
   prod_blocks<T, PU, 2>(P, P.block_post[blockIdx.x], P.block_post[blockIdx.x + 1], gridDim.x);
+}
+
+// ---- long-term plasticity (networks with LTP, delays 0) ---------------------
+// The reference's LTP (code/EqsGnl2.cpp:1005-1044) rewrites the weight g of
+// a single-target record after the step's gather: on a presynaptic spike
+// g += LP(post)·NegISI(pre) (NegISI > 0) or g *= 1 + LP(post)·NegISI(pre),
+// then on a postsynaptic spike the same with LP(pre) and PosISI(pre).  The
+// record's contribution to its post is g·st, with st its gate.  The
+// production engine keeps one conductance per (post, receptor), G(t) =
+// df·G(t-1) + pushes, which holds sum(g·st) only while g is fixed; a weight
+// change dg after step t makes the next conductance df·(G + dg·st(t)) +
+// pushes, so the LTP phase adds df·dg·st(t) (st(t): the presynaptic
+// neuron's gate after step t, the production gate of every record of that
+// neuron and receptor) to the slot the post folds at step t + 2, as the
+// pushes of step t + 1's spikes do.  NMDA records need no correction: the
+// pull sums g·s_pre over the current weights every step.  Only the records
+// of neurons that spiked are touched (~(out + in degree) per spike).
+// float arithmetic, one rounding per operation (no fused multiply-add), as
+// the reference computes it
+__device__ __forceinline__ float ltp_rule(float g, float lp, float x) {
+  return x > 0.0f ? __fadd_rn(g, __fmul_rn(lp, x)) : __fmul_rn(g, __fadd_rn(1.0f, __fmul_rn(lp, x)));
+}
+
+template <class T>
+__device__ __forceinline__ void ltp_correct(const Params &P, uint32_t post, uint32_t r, T dg, T stv, uint32_t slot) {
+  const T v = (T)__ldg(P.dfst + (size_t)r * P.n + post) * dg * stv * (T)P.rg[r];
+  const long long fx = __double2ll_rn((double)v * kFix);
+  if (fx) atomicAdd(ring_at(P, P.lin_of_rec[r], post, slot), (unsigned long long)fx);
+}
+
+// LTP of record k of neuron a's out-records (a spiked at the step of parity
+// par) and of record k of its in-records; the corrections go to ring slot
+// `slot` (that step + 1).  Each record is rewritten once: by its presynaptic
+// neuron's item when only that neuron spiked, by its postsynaptic neuron's
+// item otherwise (both rules, the presynaptic one first, as the reference
+// applies them).
+template <class T>
+__device__ __forceinline__ void ltp_out_record(const Params &P, uint32_t a, uint32_t k, uint32_t par, uint32_t slot) {
+  const uint32_t n = P.n;
+  const uint32_t ent = __ldg(P.ltp_oent + k), idx = __ldg(P.ltp_oidx + k);
+  const uint32_t b = ent & 0xffffffu, r = ent >> 24;
+  if (__ldcg(P.ltp_spk2 + (size_t)par * n + b)) return;
+  float *wp = (r == FS_NMDA ? (float *)P.in_w : (float *)P.out_w) + idx;
+  const float g0 = __ldcg(wp);
+  const float g1 = ltp_rule(g0, __ldcg((const float *)P.ltp_lp2 + (size_t)par * n + b), __ldg(P.ltp_neg + a));
+  __stcg(wp, g1);
+  if (r != FS_NMDA)
+    ltp_correct<T>(P, b, r, (T)g1 - (T)g0, __ldcg((const T *)P.ltp_sp2 + ((size_t)par * 4 + r) * n + a), slot);
+}
+
+template <class T>
+__device__ __forceinline__ void ltp_in_record(const Params &P, uint32_t a, uint32_t k, uint32_t par, uint32_t slot) {
+  const uint32_t n = P.n;
+  const float *lp = (const float *)P.ltp_lp2 + (size_t)par * n;
+  const uint32_t ent = __ldg(P.ltp_ient + k), idx = __ldg(P.ltp_iidx + k);
+  const uint32_t c = ent & 0xffffffu, r = ent >> 24;
+  float *wp = (r == FS_NMDA ? (float *)P.in_w : (float *)P.out_w) + idx;
+  const float g0 = __ldcg(wp);
+  float g = g0;
+  if (__ldcg(P.ltp_spk2 + (size_t)par * n + c)) g = ltp_rule(g, __ldcg(lp + a), __ldg(P.ltp_neg + c));
+  g = ltp_rule(g, __ldcg(lp + c), __ldg(P.ltp_pos + c));
+  __stcg(wp, g);
+  if (r != FS_NMDA)
+    ltp_correct<T>(P, a, r, (T)g - (T)g0, __ldcg((const T *)P.ltp_sp2 + ((size_t)par * 4 + r) * n + c), slot);
+}
+
+// The LTP of a step's nl listed spikes (ids; parity par), over all warps of
+// the grid: spike j contributes ceil(out_j / 32) + ceil(in_j / 32) items of
+// 32 records, and warp gw takes items gw, gw + nwarps, ...  Every warp
+// forms the same prefix over the spikes, 32 at a time (one spike per lane).
+template <class T>
+__device__ __forceinline__ void ltp_phase(const Params &P, const uint32_t *ids, uint32_t nl, uint32_t par,
+                                          uint32_t slot, uint32_t gw, uint32_t nwarps, uint32_t lane) {
+  uint32_t acc = 0;  // items of the earlier rounds
+  for (uint32_t base = 0; base < nl; base += 32) {
+    const uint32_t j = base + lane;
+    uint32_t a = 0, o0 = 0, co = 0, i0 = 0, ci = 0;
+    if (j < nl) {
+      a = __ldcg(ids + j);
+      o0 = __ldg(P.ltp_orow + a);
+      i0 = __ldg(P.ltp_irow + a);
+      co = (__ldg(P.ltp_orow + a + 1) - o0 + 31u) >> 5;
+      ci = (__ldg(P.ltp_irow + a + 1) - i0 + 31u) >> 5;
+    }
+    uint32_t incl = co + ci;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(fsd::kFull, incl, o);
+      if (lane >= (uint32_t)o) incl += v;
+    }
+    const uint32_t total = __shfl_sync(fsd::kFull, incl, 31);
+    // first item of this round that is this warp's
+    uint32_t it = gw >= acc ? gw - acc : (nwarps - (acc - gw) % nwarps) % nwarps;
+    for (; it < total; it += nwarps) {
+      const uint32_t jl = __ffs(__ballot_sync(fsd::kFull, incl > it)) - 1;  // the spike of item it
+      const uint32_t aj = __shfl_sync(fsd::kFull, a, jl), coj = __shfl_sync(fsd::kFull, co, jl);
+      const uint32_t first = __shfl_sync(fsd::kFull, incl - co - ci, jl);
+      const uint32_t c = it - first;
+      if (c < coj) {
+        const uint32_t b0 = __shfl_sync(fsd::kFull, o0, jl), k = b0 + 32u * c + lane;
+        if (k < __ldg(P.ltp_orow + aj + 1)) ltp_out_record<T>(P, aj, k, par, slot);
+      } else {
+        const uint32_t b0 = __shfl_sync(fsd::kFull, i0, jl), k = b0 + 32u * (c - coj) + lane;
+        if (k < __ldg(P.ltp_irow + aj + 1)) ltp_in_record<T>(P, aj, k, par, slot);
+      }
+    }
+    acc += total;
+  }
+}
+
+// Persistent kernel of networks with LTP (every delay 0, so every step ends
+// at a grid barrier).  Step t of a block: (1) the NMDA sums of its posts
+// over the weights as they were after step t - 1's gather; (2) the pushes of
+// step t - 1's spikes (the network's list, any warp takes any spike) over
+// the linear weights of step t - 1; a grid barrier; (3) the LTP of step t -
+// 1's spikes (no block reads a weight it rewrites until the next barrier);
+// (4) the neurons' steps, which list step t's spikes; a grid barrier.  A
+// launch of steps [t0, t1) ends with (1)-(3) of step t1: the NMDA sums of
+// step t1 (kept in ltp_gn for the next launch, whose first step pulls
+// nothing), the pushes and the LTP of step t1 - 1.  So between launches the
+// weights are those after the last step's LTP, as the reference's are, and
+// nothing else is pending.
+template <class T>
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 2 : 1) k_prod_ltp(const __grid_constant__ Params P) {
+  constexpr uint32_t kT = TileW<T>::W;
+  __shared__ TileBufs<T> B;
+  __shared__ float tm3[kThreads * 3];
+  const uint32_t B0 = P.block_post[blockIdx.x], B1 = P.block_post[blockIdx.x + 1];
+  const uint32_t nblk = gridDim.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const uint32_t gw = blockIdx.x * (kThreads / 32) + wid, nwarps = nblk * (kThreads / 32);
+  const uint32_t n = P.n, mask = P.mask;
+  PhaseClock pc;
+  pc.start(P);
+  unsigned long long target = 0;
+  for (uint32_t s = 0; s <= P.nsteps; s++) {
+    const uint64_t t = P.t0 + s;
+    const bool last = s == P.nsteps;
+    if (s > 0) {
+      for (uint32_t tp0 = B0; tp0 < B1; tp0 += kT) {
+        const uint32_t np = min(kT, B1 - tp0);
+        T(*gn)[kT] = (T(*)[kT])((T *)P.ltp_gn + tp0);
+        if constexpr (sizeof(T) == 4) nmda_pull1_f32<true>(P, tp0, np, t, (float(*)[kTile])gn, wid, lane);
+        else nmda_pull<T, true>(P, tp0, np, t, 1, gn, wid, lane);
+      }
+      pc.mark(0);
+    }
+    if (s > 0) {
+      const uint32_t par = (uint32_t)(t - 1u) & 1u;
+      const uint32_t nl = __ldcg(P.ltp_cnt + par);
+      const uint32_t *ids = P.ltp_id + (size_t)par * n;
+      const uint16_t *tms = P.ltp_tm + (size_t)par * n;
+      const T *cs = (const T *)P.ltp_c + (size_t)par * n * 4;
+      for (uint32_t k = gw; k < nl; k += nwarps) {
+        T cj[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) cj[r] = __ldcg(cs + (size_t)k * 4 + r);
+        push_spike<T, true>(P, __ldcg(ids + k), __ldcg(tms + k), cj, lane, 32);
+      }
+      // step t's list starts empty: its last readers (step t - 2's pushes
+      // and LTP) passed the barrier of step t - 1, its writers come after
+      // the next one (or in the next launch)
+      if (blockIdx.x == 0 && tid == 0) P.ltp_cnt[(uint32_t)t & 1u] = 0u;
+      pc.mark(5);
+      if (!grid_sync(P.bar, P.err, nblk, target)) return;
+      pc.mark(6);
+      ltp_phase<T>(P, ids, nl, par, (uint32_t)t & mask, gw, nwarps, lane);
+      pc.mark(7);
+    }
+    if (last) break;
+    const uint32_t par = (uint32_t)t & 1u;
+    const SpikeList<T> lst{P.ltp_cnt + par, P.ltp_id + (size_t)par * n, P.ltp_tm + (size_t)par * n,
+                           (T(*)[4])((T *)P.ltp_c + (size_t)par * n * 4), n};
+    for (uint32_t tp0 = B0; tp0 < B1; tp0 += kT) {
+      const uint32_t np = min(kT, B1 - tp0);
+      draw_inputs<T>(P, tp0, np, t, 1, B.hits, B.gauss);
+      if (P.gap_row) tile_gap<T>(P, tp0, np, s, B.gapI);
+      __syncthreads();
+      pc.mark(1);
+      if ((tid & ~31u) < np) {
+        StepRegs<T> R;
+        neuron_load<T, 1>(P, tp0, np, s, 1, R, tm3);
+        neuron_steps<T, 1, true>(P, tp0, np, s, 1, (T(*)[kT])((T *)P.ltp_gn + tp0), B.hits, B.gauss, lst, B.gapI, R,
+                                 tm3);
+      }
+      __syncthreads();
+      pc.mark(2);
+    }
+    if (!grid_sync(P.bar, P.err, nblk, target)) return;
+    pc.mark(4);
+  }
 }
 
 // ---- single-step persistent kernel (networks whose delays are all 0) -------
@@ -1613,6 +1882,7 @@ struct Prod {
   uint32_t b1_blocks = 0;  // its blocks (one per SM at most)
   unsigned long long *phase_buf = nullptr;  // phase clock counters (debug aid)
   bool wide = false;  // some block's posts span several tiles: eight NMDA edges in flight
+  bool ltp = false;   // long-term plasticity: runs on k_prod_ltp
   uint32_t n = 0, sm = 148;
   Params P{};
   std::vector<void *> allocs;
@@ -1646,6 +1916,9 @@ struct Prod {
   uint64_t gv_out_cap = 0;
   uint32_t gv_ent_cap = 0;
   std::vector<uint32_t> in_row_h;  // NMDA in-degree prefix (block partitioning)
+  // networks with LTP: where each synapse-list entry's weight lives (index
+  // in out_w, or in in_w with the top bit set)
+  std::vector<uint32_t> wpos;
 };
 
 namespace {
@@ -1775,7 +2048,13 @@ int launch(Prod *p, uint32_t nsteps, bool want_bits, bool wantV, cudaStream_t st
     if (launches) *launches += k;
     return FS_OK;
   }
-  if (p->single) {
+  if (p->ltp) {
+    // both spike lists start empty (a launch leaves none pending)
+    e = cudaMemsetAsync(P.ltp_cnt, 0, 8, st);
+    if (e == cudaSuccess)
+      e = cudaLaunchCooperativeKernel(p->fp64 ? (const void *)k_prod_ltp<double> : (const void *)k_prod_ltp<float>,
+                                      p->blocks, kThreads, args, 0, st);
+  } else if (p->single) {
     const void *k1 = P.plast == PL_TM ? (const void *)k_prod1<true> : (const void *)k_prod1<false>;
     e = cudaLaunchCooperativeKernel(k1, p->b1_blocks, kT1, args, P.t1_smem, st);
   } else {
@@ -2336,6 +2615,76 @@ int prod_check_single_plan(const fs_net_desc *d, uint32_t sm_count, uint64_t *st
 static int prod_create_from(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t sm_count,
                             cudaStream_t st, std::string &err, bool allow_single, HostNet *pre);
 
+// Tables and state of long-term plasticity (k_prod_ltp).  The LTP records
+// are the synapse-list entries with ltp[e] set (all of them when the list
+// has no flags): the reference's single-target records (SynFst1 and
+// SynSlo1, code/EqsGnl2.cpp:1005-1044), whose presynaptic neuron here is
+// the true one.  Each record is located by the index of its weight in
+// out_w or in_w, replaying host_net's fill order.
+static int ltp_create(Prod *p, const fs_net_desc *d, const HostNet &H, size_t T, cudaStream_t st, std::string &err) {
+  const fs_neurons &v = d->neurons;
+  const fs_syn_list &S = *d->syn;
+  const uint32_t n = p->n;
+  Params &P = p->P;
+  std::vector<uint32_t> fo(H.out_row.begin(), H.out_row.end() - 1), fi(H.in_row.begin(), H.in_row.end() - 1);
+  std::vector<uint32_t> orow(n + 1, 0), irow(n + 1, 0), pos(S.n);
+  for (uint64_t e = 0; e < S.n; e++) {
+    pos[e] = S.rec[e] == FS_NMDA ? fi[S.post[e]]++ : fo[S.pre[e]]++;
+    if (!S.ltp || S.ltp[e]) {
+      orow[S.pre[e] + 1]++;
+      irow[S.post[e] + 1]++;
+    }
+  }
+  for (uint32_t i = 0; i < n; i++) {
+    orow[i + 1] += orow[i];
+    irow[i + 1] += irow[i];
+  }
+  const uint32_t nr = orow[n];
+  if (H.nlin_e >= (1ull << 31) || H.nnm_e >= (1ull << 31)) {
+    err = "networks with LTP: at most 2^31 - 1 synapses per receptor class";
+    return FS_ERR_UNSUPPORTED;
+  }
+  p->wpos.resize(S.n);
+  for (uint64_t e = 0; e < S.n; e++) p->wpos[e] = pos[e] | (S.rec[e] == FS_NMDA ? 0x80000000u : 0u);
+  std::vector<uint32_t> oent(nr), oidx(nr), ient(nr), iidx(nr);
+  {
+    std::vector<uint32_t> a(orow.begin(), orow.end() - 1), b(irow.begin(), irow.end() - 1);
+    for (uint64_t e = 0; e < S.n; e++) {
+      if (S.ltp && !S.ltp[e]) continue;
+      const uint32_t r = S.rec[e], x = a[S.pre[e]]++, y = b[S.post[e]]++;
+      oent[x] = S.post[e] | (r << 24);
+      oidx[x] = pos[e];
+      ient[y] = S.pre[e] | (r << 24);
+      iidx[y] = pos[e];
+    }
+  }
+  std::vector<float> zf(n, 0.0f);
+  std::vector<int32_t> zi(n, 0);
+  int rc;
+  if ((rc = dup(p, (uint32_t **)&P.ltp_orow, orow.data(), orow.size(), st, err)) ||
+      (rc = dup(p, (uint32_t **)&P.ltp_irow, irow.data(), irow.size(), st, err)) ||
+      (rc = dup(p, (uint32_t **)&P.ltp_oent, oent.data(), nr, st, err)) ||
+      (rc = dup(p, (uint32_t **)&P.ltp_oidx, oidx.data(), nr, st, err)) ||
+      (rc = dup(p, (uint32_t **)&P.ltp_ient, ient.data(), nr, st, err)) ||
+      (rc = dup(p, (uint32_t **)&P.ltp_iidx, iidx.data(), nr, st, err)) ||
+      (rc = dup(p, (float **)&P.ltp_dflp, v.ltp_dfLP ? v.ltp_dfLP : zf.data(), n, st, err)) ||
+      (rc = dup(p, (float **)&P.ltp_pos, v.ltp_PosISI ? v.ltp_PosISI : zf.data(), n, st, err)) ||
+      (rc = dup(p, (float **)&P.ltp_neg, v.ltp_NegISI ? v.ltp_NegISI : zf.data(), n, st, err)) ||
+      (rc = dup(p, (int32_t **)&P.ltp_spd, v.ltp_SpiLPDy ? v.ltp_SpiLPDy : zi.data(), n, st, err)) ||
+      (rc = dup(p, (uint8_t **)&P.ltp_lp, (const uint8_t *)nullptr, (size_t)n * 4, st, err)) ||
+      (rc = dup(p, &P.ltp_clp, (const int32_t *)nullptr, n, st, err)) ||
+      (rc = dup(p, (uint8_t **)&P.ltp_lp2, (const uint8_t *)nullptr, (size_t)2 * n * 4, st, err)) ||
+      (rc = dup(p, (uint8_t **)&P.ltp_sp2, (const uint8_t *)nullptr, 8 * n * T, st, err)) ||
+      (rc = dup(p, &P.ltp_spk2, (const uint8_t *)nullptr, 2 * (size_t)n, st, err)) ||
+      (rc = dup(p, (uint8_t **)&P.ltp_gn, (const uint8_t *)nullptr, n * T, st, err)) ||
+      (rc = dup(p, &P.ltp_cnt, (const uint32_t *)nullptr, 2, st, err)) ||
+      (rc = dup(p, &P.ltp_id, (const uint32_t *)nullptr, 2 * (size_t)n, st, err)) ||
+      (rc = dup(p, &P.ltp_tm, (const uint16_t *)nullptr, 2 * (size_t)n, st, err)) ||
+      (rc = dup(p, (uint8_t **)&P.ltp_c, (const uint8_t *)nullptr, 8 * n * T, st, err)))
+    return rc;
+  return FS_OK;
+}
+
 int prod_create(Prod **out, const fs_net_desc *d, const fs_run_opts &o, uint32_t sm_count, cudaStream_t st,
                 std::string &err, bool allow_single) {
   return prod_create_from(out, d, o, sm_count, st, err, allow_single, nullptr);
@@ -2351,8 +2700,17 @@ static int prod_create_from(Prod **out, const fs_net_desc *d, const fs_run_opts 
     err = "production modes support up to 4,194,303 neurons per handle";
     return FS_ERR_UNSUPPORTED;
   }
-  if (d->act_ctr & FS_ACT_LTP) {
-    err = "production modes do not implement LTP (use FS_MODE_COMPAT)";
+  // long-term plasticity runs on its own persistent kernel (k_prod_ltp):
+  // not in batches, not on the tile kernels, and only without delays (the
+  // reference has none; a weight change would otherwise have to reach
+  // every delayed copy of the record's gate)
+  const bool ltp = (d->act_ctr & FS_ACT_LTP) != 0;
+  if (ltp && !allow_single) {
+    err = "batches do not run networks with LTP (create them one by one)";
+    return FS_ERR_UNSUPPORTED;
+  }
+  if (ltp && (o.flags & FS_RUN_TILE_KERNELS)) {
+    err = "networks with LTP run on their own persistent kernel, not on the tile kernels";
     return FS_ERR_UNSUPPORTED;
   }
   // gap junctions: the per-neuron term lists of the compat layout (other
@@ -2382,6 +2740,12 @@ static int prod_create_from(Prod **out, const fs_net_desc *d, const fs_run_opts 
   }
   const uint32_t dmin = H.dmin, dmax = H.dmax;
   const uint64_t nlin_e = H.nlin_e, nnm_e = H.nnm_e;
+  if (ltp && dmax != 0) {
+    delete p;
+    err = "networks with LTP need every synaptic delay 0 in the production modes";
+    return FS_ERR_UNSUPPORTED;
+  }
+  p->ltp = ltp;
   std::vector<float> &pdf = H.pdf, &p_dfxt = H.p_dfxt, &p_dfst = H.p_dfst, &p_efas = H.p_efas;
   std::vector<uint8_t> &proj = H.proj;
   std::vector<uint32_t> &out_row = H.out_row, &in_row = H.in_row, &out_code = H.out_code, &in_code = H.in_code;
@@ -2405,8 +2769,11 @@ static int prod_create_from(Prod **out, const fs_net_desc *d, const fs_run_opts 
   P.nlin = p->nlin;
   // ---- grid: all blocks co-resident; posts split by estimated cost ----
   int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p->fp64 ? (const void *)k_prod<double, 4> : (const void *)k_prod<float, 4>,
-                                                kThreads, 0);
+  {
+    const void *kq = ltp ? (p->fp64 ? (const void *)k_prod_ltp<double> : (const void *)k_prod_ltp<float>)
+                         : (p->fp64 ? (const void *)k_prod<double, 4> : (const void *)k_prod<float, 4>);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kq, kThreads, 0);
+  }
   if (occ < 1) occ = 1;
   int per_sm = std::min(occ, 4);
   if (o.blocks_per_sm) per_sm = std::min<int>(occ, (int)o.blocks_per_sm);
@@ -2503,7 +2870,7 @@ static int prod_create_from(Prod **out, const fs_net_desc *d, const fs_run_opts 
       if (L.n_recs && src) p->rec_src[r].assign(src, src + L.n_recs);
     }
   // single-step kernel: FP32, every delay 0, no gap junctions
-  if (allow_single && !p->fp64 && dmax == 0 && !gap && S.n > 0 && !(o.flags & FS_RUN_INTERVAL_KERNEL)) {
+  if (allow_single && !ltp && !p->fp64 && dmax == 0 && !gap && S.n > 0 && !(o.flags & FS_RUN_INTERVAL_KERNEL)) {
     Single S1;
     std::string why;
     if (plan_single(n, p->nlin, sm_count, in_row, in_code, in_w, out_row, out_code, out_w, p_dfxt, p_dfst, p_efas,
@@ -2558,7 +2925,7 @@ static int prod_create_from(Prod **out, const fs_net_desc *d, const fs_run_opts 
   }
   // tile kernels: networks whose blocks would each walk more than two tiles
   // of posts per batch (at 2 blocks per SM: above ~150,000 neurons)
-  if (allow_single && !p->single && !(o.flags & FS_RUN_INTERVAL_KERNEL) &&
+  if (allow_single && !ltp && !p->single && !(o.flags & FS_RUN_INTERVAL_KERNEL) &&
       ((o.flags & FS_RUN_TILE_KERNELS) || (uint64_t)n > (uint64_t)p->blocks * 2 * (p->fp64 ? TileW<double>::W : kTile))) {
     if ((rc = tiles_solo_create(p, err))) goto fail;
   }
@@ -2573,6 +2940,7 @@ static int prod_create_from(Prod **out, const fs_net_desc *d, const fs_run_opts 
     P.gap_w = nullptr;
     P.Vg = nullptr;
   }
+  if (ltp && (rc = ltp_create(p, d, H, T, st, err))) goto fail;
   if ((rc = dal(p, &p->bar, 64, err)) || (rc = dal(p, &p->err, 1, err)) ||
       (rc = dup(p, &p->spike_total, (const unsigned long long *)nullptr, 1, st, err)))
     goto fail;
@@ -2637,6 +3005,12 @@ int prod_reset(Prod *p, uint32_t seed, cudaStream_t st, std::string &err) {
   z(P.Count, n * 4); z(P.NS, n * 4); z(P.Cap, n * 4); z(P.Car, n * 4); z(P.nspk, n * 4); z(P.Irep, (size_t)5 * n * 4);
   z(P.ring, (size_t)std::max<uint32_t>(1, p->nlin) * P.slots * n * 8);
   z(P.Vg, 2 * n * T);
+  // LTP: trace and counter (VarInit, code/EqsGnl2.cpp:363-367); the weights
+  // keep what earlier runs made of them, as the reference's records do
+  z(P.ltp_lp, n * 4);
+  z(P.ltp_clp, n * 4);
+  z(P.ltp_gn, n * T);  // the NMDA sums of step 0 (the history is empty)
+  z(P.ltp_cnt, 8);
   z(p->err, 4);
   z(p->spike_total, 8);
   if (e == cudaSuccess) {
@@ -2821,6 +3195,7 @@ void prod_info(const Prod *p, ProdInfo *info) {
   info->threads = p->single ? kT1 : kThreads;
   info->single_step = p->single ? 1 : 0;
   info->tiles = p->tiles ? 1 : 0;
+  info->ltp = p->ltp ? 1 : 0;
   info->chunks = p->chunks;
   info->lin_edges = p->lin_edges;
   info->nmda_edges = p->nmda_edges;
@@ -3476,6 +3851,13 @@ void state_regions(Prod *p, std::vector<std::pair<void *, size_t>> &r) {
   r.push_back({P.Irep, (size_t)5 * n * 4});
   r.push_back({P.ring, (size_t)std::max<uint32_t>(1, p->nlin) * P.slots * n * 8});
   if (P.Vg) r.push_back({P.Vg, 2 * n * T});
+  if (p->ltp) {  // the weights LTP rewrites, and the traces
+    r.push_back({(void *)P.out_w, p->lin_edges * 4});
+    r.push_back({(void *)P.in_w, p->nmda_edges * 4});
+    r.push_back({P.ltp_lp, n * 4});
+    r.push_back({P.ltp_clp, n * 4});
+    r.push_back({P.ltp_gn, n * T});  // the next step's NMDA sums
+  }
   r.push_back({p->spike_total, 8});
 }
 }  // namespace
@@ -3535,6 +3917,30 @@ int prod_state_load(Prod *p, const uint8_t *buf, cudaStream_t st, std::string &e
   p->ms = 0.0;
   p->kl = 0;
   p->ev_used = 0;
+  return FS_OK;
+}
+
+int prod_get_weights(Prod *p, float *g, uint64_t n, cudaStream_t st, std::string &err) {
+  if (!p->ltp) {
+    err = "fs_get_weights: the network has no LTP (its weights are the description's)";
+    return FS_ERR_UNSUPPORTED;
+  }
+  if (n != p->wpos.size()) {
+    err = "fs_get_weights: n must be the synapse list's length (" + std::to_string(p->wpos.size()) + ")";
+    return FS_ERR_ARG;
+  }
+  std::vector<float> ow(p->lin_edges), iw(p->nmda_edges);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess && !ow.empty()) e = cudaMemcpy(ow.data(), p->P.out_w, ow.size() * 4, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && !iw.empty()) e = cudaMemcpy(iw.data(), p->P.in_w, iw.size() * 4, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    err = std::string("fs_get_weights: ") + cudaGetErrorString(e);
+    return FS_ERR_CUDA;
+  }
+  for (uint64_t i = 0; i < n; i++) {
+    const uint32_t w = p->wpos[i];
+    g[i] = (w & 0x80000000u) ? iw[w & 0x7fffffffu] : ow[w];
+  }
   return FS_OK;
 }
 

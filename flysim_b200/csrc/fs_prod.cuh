@@ -25,6 +25,8 @@ int prod_run(Prod *p, uint32_t nsteps, cudaStream_t st, uint64_t *launches, std:
 int prod_check(Prod *p, cudaStream_t st, uint64_t *spikes_total, std::string &err);
 void prod_kernel_time(Prod *p, double *ms_per_launch, uint64_t *launches);
 int prod_get_state(Prod *p, float *V, int32_t *Count, uint32_t *NState, cudaStream_t st, std::string &err);
+// Current weights in synapse-list order (networks with LTP: n = list size).
+int prod_get_weights(Prod *p, float *g, uint64_t n, cudaStream_t st, std::string &err);
 
 // Builds the single-step plan of a network on the host (no device needed)
 // and checks every index the kernel derives from it; stats[0] = 1 when the
@@ -39,6 +41,7 @@ struct ProdInfo {
   int fp64;
   int single_step;  // the network runs on the single-step kernel
   int tiles;        // the network runs on the tile kernels
+  int ltp;          // the network runs on the LTP kernel (long-term plasticity)
 };
 void prod_info(const Prod *p, ProdInfo *info);
 int prod_spike_counts(Prod *p, uint32_t *counts, cudaStream_t st, std::string &err);

@@ -427,6 +427,7 @@ void build_network(Model &m) {
 
   // ---- flat synapse list for the production modes ----
   net.syn_pre.clear(); net.syn_post.clear(); net.syn_rec.clear(); net.syn_g.clear(); net.syn_delay.clear();
+  net.syn_ltp.clear();
   // group gates carry their link's delay: rebuild the link of each gate
   std::vector<uint16_t> gate_delay[FS_NREC];
   {
@@ -457,6 +458,7 @@ void build_network(Model &m) {
         net.syn_rec.push_back((uint8_t)r);
         net.syn_g.push_back(ra.gate_g[gate]);
         net.syn_delay.push_back(gate_delay[r][gate]);
+        net.syn_ltp.push_back(0);
       }
     for (uint32_t e = 0; e < ra.rec_pre.size(); e++) {
       net.syn_pre.push_back(srec_src[r][e]);
@@ -464,6 +466,7 @@ void build_network(Model &m) {
       net.syn_rec.push_back((uint8_t)r);
       net.syn_g.push_back(ra.rec_g[e]);
       net.syn_delay.push_back(rec_delay[r][e]);
+      net.syn_ltp.push_back(1);
     }
   }
   net.make_views(dt, m.act_ctr);
@@ -502,7 +505,7 @@ void Network::make_views(float dt, uint32_t act_ctr) {
   compat.gap_g = gap_g.data();
   syn.n = syn_pre.size();
   syn.pre = syn_pre.data(); syn.post = syn_post.data(); syn.rec = syn_rec.data();
-  syn.g = syn_g.data(); syn.delay = syn_delay.data();
+  syn.g = syn_g.data(); syn.delay = syn_delay.data(); syn.ltp = syn_ltp.data();
   desc.dt = dt;
   desc.act_ctr = act_ctr;
   desc.compat = &compat;

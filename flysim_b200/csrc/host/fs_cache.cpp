@@ -26,7 +26,7 @@ namespace fsh {
 namespace {
 
 constexpr char kMagic[8] = {'F', 'S', 'B', '2', 'N', 'E', 'T', '\0'};
-constexpr uint32_t kFormat = 4;  // 3: unseeded models are never stored; 4: record sources
+constexpr uint32_t kFormat = 5;  // 3: unseeded models are never stored; 4: record sources; 5: LTP record flags
 constexpr uint32_t kSizes = (uint32_t)(sizeof(Receptor) | sizeof(Link) << 8 | sizeof(Event) << 16);
 
 // 64-bit streaming hash for cache keys and the payload check (not a
@@ -214,7 +214,7 @@ template <class A> void visit_model(A &a, Model &m) {
   }
   a(n.gap_rowptr); a(n.gap_other); a(n.gap_g);
   a(n.gap1_pre); a(n.gap1_post); a(n.gap_ngroup); a(n.gap1_g);
-  a(n.syn_pre); a(n.syn_post); a(n.syn_rec); a(n.syn_g); a(n.syn_delay);
+  a(n.syn_pre); a(n.syn_post); a(n.syn_rec); a(n.syn_g); a(n.syn_delay); a(n.syn_ltp);
   a(n.total_synapses);
 }
 

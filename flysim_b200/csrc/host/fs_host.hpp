@@ -113,6 +113,7 @@ struct Network {
   std::vector<uint8_t> syn_rec;
   std::vector<float> syn_g;
   std::vector<uint16_t> syn_delay;
+  std::vector<uint8_t> syn_ltp;  // 1: a single-target record (LTP rewrites its weight)
 
   uint64_t total_synapses = 0;  // TolSynp of the reference
   // C views

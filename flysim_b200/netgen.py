@@ -218,16 +218,22 @@ EndReceptor
 """
 
 
-def write_connectome(c: Connectome, path: str, with_delays: bool = True) -> None:
+def write_connectome(c: Connectome, path: str, with_delays: bool = True, ltp: Optional[dict] = None) -> None:
     """Writes the network as one population per neuron (the reference's
     connectome format); each connection becomes one target block per
-    receptor."""
+    receptor.  ``ltp`` (keys tLP, SpiLPDy, PosISI, NegISI) adds the
+    long-term plasticity keywords to every population
+    (code/parser.cpp:385-392, :559-575)."""
     order = np.argsort(c.pre, kind="stable")
     pre, post, w, d = c.pre[order], c.post[order], c.weight[order], c.delay_ms[order]
     bounds = np.searchsorted(pre, np.arange(c.n + 1))
+    ltp_lines = "".join("LTP_%s=%s\n" % (k, _fmt(ltp[k])) for k in ("tLP", "SpiLPDy", "PosISI", "NegISI")) if ltp else ""
     with open(path, "w") as f:
         for i in range(c.n):
-            parts = [_POP_HEADER.format(name="n%d" % i, freq=_fmt(c.freq_ext[i]), ext=_fmt(c.ext_eff))]
+            head = _POP_HEADER.format(name="n%d" % i, freq=_fmt(c.freq_ext[i]), ext=_fmt(c.ext_eff))
+            if ltp:
+                head = head.replace("SpikeDly=0\n", "SpikeDly=0\n" + ltp_lines, 1)
+            parts = [head]
             a, b = bounds[i], bounds[i + 1]
             exc = bool(c.excit[i])
             for e in range(a, b):

@@ -98,8 +98,10 @@ def neuron_fields(n: int, dt: float, taum=20.0, cm=0.5, el=-70.0, vth=-50.0, vre
 
 
 def desc_from_arrays(n: int, dt: float, fields: dict, pre, post, rec, g, delay_steps=None,
-                     tm: Optional[dict] = None, act_ctr: int = DEFAULT_ACT) -> NetArrays:
-    """fs_net_desc over numpy arrays (production modes: flat synapse list)."""
+                     tm: Optional[dict] = None, act_ctr: int = DEFAULT_ACT, ltp=None) -> NetArrays:
+    """fs_net_desc over numpy arrays (production modes: flat synapse list).
+    ``ltp``: per entry, whether long-term plasticity rewrites its weight
+    (None: every entry, when act_ctr has the LTP bit)."""
     keep: List[np.ndarray] = []
 
     def p(a, ty, ct):
@@ -125,6 +127,7 @@ def desc_from_arrays(n: int, dt: float, fields: dict, pre, post, rec, g, delay_s
     s.rec = p(rec, np.uint8, _u8)
     s.g = p(g, np.float32, _f)
     s.delay = p(delay_steps if delay_steps is not None else np.zeros(pre.size, np.uint16), np.uint16, _u16)
+    s.ltp = p(ltp, np.uint8, _u8) if ltp is not None else None
     d = NetDesc()
     d.dt = dt
     d.act_ctr = act_ctr
@@ -144,7 +147,8 @@ def desc_from_arrays(n: int, dt: float, fields: dict, pre, post, rec, g, delay_s
         d.tm = None
     na = NetArrays(n=n, dt=dt, fields=fields,
                    syn=dict(pre=pre, post=np.asarray(post), rec=np.asarray(rec), g=np.asarray(g),
-                            delay=np.asarray(delay_steps) if delay_steps is not None else None),
+                            delay=np.asarray(delay_steps) if delay_steps is not None else None,
+                            ltp=np.asarray(ltp, np.uint8) if ltp is not None else None),
                    tm=tm)
     na.desc = d
     na._keep = keep

@@ -146,13 +146,17 @@ typedef struct fs_compat_layout {
 
 /* Flat synapse list for the production modes: one entry per (pre, post,
  * receptor).  delay is in steps (0 = effect on the next step, as the
- * reference). */
+ * reference).  ltp marks the entries whose weight long-term plasticity
+ * rewrites when act_ctr has FS_ACT_LTP: the reference's single-target
+ * records (SynFst1 / SynSlo1, code/EqsGnl2.cpp:1005-1044), not the links
+ * of a population to several targets. */
 typedef struct fs_syn_list {
   uint64_t n;
   const uint32_t *pre, *post;
   const uint8_t *rec;
   const float *g;
   const uint16_t *delay;     /* may be NULL: all zero */
+  const uint8_t *ltp;        /* may be NULL: every entry */
 } fs_syn_list;
 
 /* Tsodyks-Markram short-term plasticity for the production modes, per
@@ -252,8 +256,9 @@ int fs_run_timed(fs_handle *h, uint32_t nsteps, double *device_ms);
  * block of its persistent kernel, the steps between grid barriers, and
  * which kernels run it (kernel): 0 the persistent interval kernel, 1 the
  * single-step kernel (FS_MODE_FP32 networks whose delays are all 0 and that
- * have no gap junctions), 2 the tile kernels (large networks).  No
- * counterpart in the reference. */
+ * have no gap junctions), 2 the tile kernels (large networks), 3 the
+ * long-term plasticity kernel (networks with FS_ACT_LTP).  No counterpart
+ * in the reference. */
 int fs_engine_layout(fs_handle *h, uint32_t *blocks, uint32_t *threads, uint32_t *interval, int *kernel);
 /* Synchronise and report counters. */
 int fs_sync(fs_handle *h);
@@ -353,6 +358,12 @@ int fs_checkpoint_save(fs_handle *h, void *buf, uint64_t cap, uint64_t *bytes);
 int fs_checkpoint_load(fs_handle *h, const void *buf, uint64_t bytes);
 /* Copy state out (V, Count, NState) for checks; arrays of length n. */
 int fs_get_state(fs_handle *h, float *V, int32_t *Count, uint32_t *NState);
+/* The synaptic weights as long-term plasticity has made them, in the order
+ * of the description's fs_syn_list (n = its length): the g of the
+ * reference's records (code/EqsGnl2.cpp:1005-1044), which it never writes
+ * out.  Production modes, networks with FS_ACT_LTP (the weights of other
+ * networks do not change); otherwise FS_ERR_UNSUPPORTED. */
+int fs_get_weights(fs_handle *h, float *g, uint64_t n);
 /* Full conductance view for checks: RVs (FS_NREC*n) after the last step and
  * Isyn (n). */
 int fs_get_syn_state(fs_handle *h, float *g, float *Isyn);
