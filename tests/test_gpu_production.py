@@ -344,6 +344,36 @@ def test_single_step_kernel_equals_interval_kernel(built, variant):
     np.testing.assert_array_equal(ca, cb)
 
 
+@pytest.mark.parametrize("mode", ["fp32", "fp64"])
+def test_tile_kernels_equal_interval_kernel(built, mode):
+    # a 30k connectome with delays of 1-5 ms and Tsodyks-Markram plasticity
+    # on the tile kernels (launch pairs over tiles of posts; FP32 stages each
+    # tile's ring slots in shared memory) against the persistent interval
+    # kernel, with calls that leave batches unaligned and partial: spikes,
+    # membrane potentials and spike counts bit for bit
+    from flysim_b200 import netgen, network
+    c = netgen.connectome(n=30000, regions=58, seed=2)
+    na = network.connectome_net(c, tm=True)
+    runs = []
+    for tiles in (False, True):
+        e = built.Engine(na.desc, mode, chunk_steps=700, tile_kernels=tiles)
+        try:
+            assert e.layout()["kernel"] == ("tiles" if tiles else "interval")
+            e.reset(4)
+            sp = []
+            for k in (1, 999, 7, 1493):
+                sp += e.step(k)[0]
+            runs.append((sp, e.state()[0].copy(), e.spike_counts()))
+        finally:
+            e.close()
+    (a, Va, ca), (b, Vb, cb) = runs
+    assert sum(x.size for x in a) > 1000
+    for t, (x, y) in enumerate(zip(a, b)):
+        np.testing.assert_array_equal(x, y, err_msg="step %d" % t)
+    assert np.array_equal(Va.view(np.uint32), Vb.view(np.uint32))
+    np.testing.assert_array_equal(ca, cb)
+
+
 @pytest.mark.parametrize("case", ["two_pop", "two_pop_std", "two_pop_stp", "conn"])
 def test_single_step_kernel_on_reference_networks(built, case):
     # networks read from the reference's own .conf format (delays 0, the
