@@ -39,13 +39,21 @@ NS_OVF, NS_UDF = 16, 32
 ACT_EXT = (1, 2, 32, 64)  # AMPA, GABA, ACh, GluCl drive bits of ActCtr
 
 
-def simulate(na, steps: int, extra: bool = False, drive=None):
+def simulate(na, steps: int, extra: bool = False, drive=None, ltp: bool = False):
     """Returns (spikes: list of index arrays per step, V: [steps, n] float64)
     and, with `extra`, also the receptor currents Irep [steps, 5, n] (kept
     from the last integrated step while a neuron fires,
     code/EqsGnl2.cpp:196-206) and the LIF state word [steps, n].  drive =
     (hits uint8 [steps, n], injection current [steps, n]) of steps 0 ..
-    steps-1 after a reset."""
+    steps-1 after a reset.
+
+    ltp: long-term plasticity as the production engine applies it to its
+    aggregated conductances (delays 0): step t's NMDA sums use the weights
+    before step t - 1's LTP, then that LTP rewrites the weights and adds
+    df*dg*st(t - 1) of each rewritten linear record to the conductance its
+    post folds at step t + 1, then step t's spikes are pushed with the new
+    weights.  The final weights (after the last step's LTP) are returned
+    last."""
     f, s = na.fields, na.syn
     n = na.n
     if drive is None:
@@ -106,6 +114,17 @@ def simulate(na, steps: int, extra: bool = False, drive=None):
     xp = np.zeros(n)
     spre = np.zeros(n)
     nm = rec == NMDA
+    if ltp:
+        assert not np.any(dl), "LTP runs with delays 0"
+        wf = np.asarray(s["g"], np.float32).copy()
+        elig = np.ones(pre.size, bool) if s.get("ltp") is None else np.asarray(s["ltp"], bool)
+        dflp = np.asarray(f["ltp_dfLP"], np.float32)
+        lpos, lneg = np.asarray(f["ltp_PosISI"], np.float32), np.asarray(f["ltp_NegISI"], np.float32)
+        spd = np.asarray(f["ltp_SpiLPDy"], np.int64)
+        ltp_on = (act & ACT_LTP) != 0
+        lp = np.zeros(n, np.float32)
+        clp = np.zeros(n, np.int64)
+        spk_prev = np.zeros(n, bool)
     spikes, Vout = [], np.zeros((steps, n))
     Irep = np.zeros((5, n))
     Iout = np.zeros((steps, 5, n)) if extra else None
@@ -118,6 +137,14 @@ def simulate(na, steps: int, extra: bool = False, drive=None):
         idx = t - 1 - dl[nm]
         sh = np.where(idx >= 0, s_hist[np.maximum(idx, 0), pre[nm]], 0.0)
         g[NMDA] = np.bincount(post[nm], w[nm] * sh, n)
+        if ltp and spk_prev.any():
+            # LTP of step t - 1 (LP and gates as they were after that step)
+            w_old = wf.copy()
+            wf = ltp_weights(wf, pre, post, elig, spk_prev, lp, lneg, lpos)
+            w = wf.astype(np.float64)
+            dg = w - w_old.astype(np.float64)
+            lin = ~nm & (dg != 0)
+            np.add.at(arrive[t], (rec[lin], post[lin]), dfs[rec[lin], post[lin]] * dg[lin] * sp[rec[lin], pre[lin]])
         isyn = inj
         if drive is not None:
             h = hits_in[t].astype(np.int64)
@@ -152,6 +179,8 @@ def simulate(na, steps: int, extra: bool = False, drive=None):
         done = fire & ~ref
         cnt = np.where(ref, cnt + 1, np.where(done, 0, cnt))
         ns = np.where(done, ns & ~NS_FIRE, ns)
+        if ltp:
+            ns, lp, clp = lp_trace(ns, crossed, ltp_on, lp, clp, spd, dflp)
         Vout[t] = V
         if extra:
             Iout[t] = Irep
@@ -176,9 +205,14 @@ def simulate(na, steps: int, extra: bool = False, drive=None):
         if spk.any():
             for e in np.nonzero(spk[pre] & ~nm)[0]:
                 arrive[t + dl[e], rec[e], post[e]] += w[e] * cinc[rec[e], pre[e]]
-    if extra:
-        return spikes, Vout, Iout, NSout
-    return spikes, Vout
+        if ltp:
+            spk_prev = spk
+    out = (spikes, Vout, Iout, NSout) if extra else (spikes, Vout)
+    if ltp:
+        if spk_prev.any():
+            wf = ltp_weights(wf, pre, post, elig, spk_prev, lp, lneg, lpos)
+        out = out + (wf,)
+    return out
 
 
 NS_LP_FIRE, NS_LP_SPIKE = 4, 8
@@ -193,6 +227,35 @@ def ltp_rule(g, lp, x):
     g, lp, x = (np.asarray(v, np.float32) for v in (g, lp, x))
     one = np.float32(1.0)
     return np.where(x > 0, g + lp * x, g * (one + lp * x)).astype(np.float32)
+
+
+def ltp_weights(w, pre, post, elig, spk, lp, lneg, lpos):
+    """The LTP of one step on float32 weights w (synapse-list order): the
+    flagged records whose pre or post spiked, the presynaptic rule first
+    (post's LP, pre's NegISI), then the postsynaptic one (pre's LP and
+    PosISI)."""
+    w = w.copy()
+    sa, sb = spk[pre], spk[post]
+    m = elig & (sa | sb)
+    wn = w[m]
+    a_, b_ = pre[m], post[m]
+    wn = np.where(sa[m], ltp_rule(wn, lp[b_], lneg[a_]), wn)
+    wn = np.where(sb[m], ltp_rule(wn, lp[a_], lpos[a_]), wn)
+    w[m] = wn
+    return w
+
+
+def lp_trace(ns, crossed, ltp_on, lp, clp, spd, dflp):
+    """LP_FIRE at a threshold crossing, then firLP and ltpEul
+    (code/EqsGnl2.cpp:207-216, :254-280) for the neurons with LTP on; LP is
+    float32 as in the reference."""
+    ns = np.where(crossed & ltp_on, ns | NS_LP_FIRE, ns)
+    lpf = ltp_on & ((ns & NS_LP_FIRE) != 0)
+    hit = lpf & (clp == spd)
+    ns = np.where(hit, (ns | NS_LP_SPIKE) & ~NS_LP_FIRE, np.where(ltp_on, ns & ~NS_LP_SPIKE, ns))
+    clp = np.where(hit, 0, np.where(lpf, clp + 1, clp))
+    lp = np.where(ltp_on, np.where((ns & NS_LP_SPIKE) != 0, lp + np.float32(1.0), dflp * lp), lp)
+    return ns, lp.astype(np.float32), clp
 
 
 def simulate_ltp(na, steps: int, drive=None):
@@ -233,6 +296,7 @@ def simulate_ltp(na, steps: int, drive=None):
     dflp = np.asarray(f["ltp_dfLP"], np.float32)
     lpos, lneg = np.asarray(f["ltp_PosISI"], np.float32), np.asarray(f["ltp_NegISI"], np.float32)
     spd = np.asarray(f["ltp_SpiLPDy"], np.int64)
+    ltp_on = (act & ACT_LTP) != 0
     pre = np.asarray(s["pre"], np.int64)
     post = np.asarray(s["post"], np.int64)
     rec = np.asarray(s["rec"], np.int64)
@@ -293,8 +357,6 @@ def simulate_ltp(na, steps: int, drive=None):
         crossed = ~fire_now & (Vi > vth)
         V = np.where(fire_now, V, Vi)
         ns = np.where(crossed, ns | NS_FIRE, ns)
-        ltp_on = (act & ACT_LTP) != 0
-        ns = np.where(crossed & ltp_on, ns | NS_LP_FIRE, ns)
         fire = fire_now | crossed
         ref = fire & (cnt < rf)
         V = np.where(ref, np.where(cnt == 0, 0.0, vreset), V)
@@ -302,13 +364,7 @@ def simulate_ltp(na, steps: int, drive=None):
         done = fire & ~ref
         cnt = np.where(ref, cnt + 1, np.where(done, 0, cnt))
         ns = np.where(done, ns & ~NS_FIRE, ns)
-        # firLP + ltpEul
-        lpf = ltp_on & ((ns & NS_LP_FIRE) != 0)
-        hit = lpf & (clp == spd)
-        ns = np.where(hit, (ns | NS_LP_SPIKE) & ~NS_LP_FIRE, np.where(ltp_on, ns & ~NS_LP_SPIKE, ns))
-        clp = np.where(hit, 0, np.where(lpf, clp + 1, clp))
-        lp = np.where(ltp_on, np.where((ns & NS_LP_SPIKE) != 0, lp + np.float32(1.0), dflp * lp), lp)
-        lp = lp.astype(np.float32)
+        ns, lp, clp = lp_trace(ns, crossed, ltp_on, lp, clp, spd, dflp)
         Vout[t] = V
         spk = (ns & NS_SPIKE) != 0
         spikes.append(np.nonzero(spk)[0].astype(np.uint32))
@@ -333,11 +389,5 @@ def simulate_ltp(na, steps: int, drive=None):
         np.add.at(H, (rec, post), w.astype(np.float64) * gate)
         # LTP of step t
         if spk.any():
-            sb = spk[post]
-            m = elig & (sa | sb)
-            wn = w[m]
-            a_, b_ = pre[m], post[m]
-            wn = np.where(sa[m], ltp_rule(wn, lp[b_], lneg[a_]), wn)
-            wn = np.where(sb[m], ltp_rule(wn, lp[a_], lpos[a_]), wn)
-            w[m] = wn
+            w = ltp_weights(w, pre, post, elig, spk, lp, lneg, lpos)
     return spikes, Vout, w

@@ -41,3 +41,21 @@ def test_ltp_rule_forms():
     g = np.array([2.0, 2.0], np.float32)
     out = prod_model.ltp_rule(g, np.array([0.5, 0.5]), np.array([0.1, -0.1]))
     np.testing.assert_array_equal(out, np.array([2.05, 1.9], np.float32))
+
+
+def test_aggregated_ltp_equals_per_record():
+    # the production engine's form of LTP (one conductance per post and
+    # receptor, a weight change dg corrected by df*dg*st, NMDA over the
+    # current weights, its phase order) against the reference's per-record
+    # form: the same spikes, potentials to float64 rounding, the same
+    # float32 weights
+    for tm in (False, True):
+        na = ltp_nets.ltp_net(fb, tm=tm)
+        sp_a, V_a, w_a = prod_model.simulate(na, 3000, ltp=True)
+        sp_r, V_r, w_r = prod_model.simulate_ltp(na, 3000)
+        assert sum(x.size for x in sp_r) > 200
+        for t in range(3000):
+            np.testing.assert_array_equal(sp_a[t], sp_r[t], err_msg="step %d" % t)
+        assert np.abs(V_a - V_r).max() < 1e-9
+        np.testing.assert_array_equal(w_a, w_r)
+        assert np.count_nonzero(w_r != np.asarray(na.syn["g"], np.float32)) > 100
