@@ -107,6 +107,7 @@ class EngineVtbl(C.Structure):
 
 
 _LIB: Optional[C.CDLL] = None
+ABI_VERSION = 2  # FS_ABI_VERSION of include/flysim_b200.h the structures above follow
 
 
 def lib() -> C.CDLL:
@@ -195,6 +196,9 @@ def lib() -> C.CDLL:
         fn = getattr(L, name)
         fn.restype = res
         fn.argtypes = args
+    if L.fs_abi_version() != ABI_VERSION:
+        raise FsError(FS_ERR_ARG, "native library ABI %d, these bindings need %d (rebuild it)"
+                      % (L.fs_abi_version(), ABI_VERSION))
     _LIB = L
     return L
 

@@ -32,7 +32,8 @@
 extern "C" {
 #endif
 
-#define FS_ABI_VERSION 1
+/* 2: fs_syn_list gained ltp (the struct grew); fs_get_weights */
+#define FS_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 enum {

@@ -20,7 +20,7 @@ def test_library_exports_every_declared_symbol(built):
     missing = [s for s in header_functions() if not hasattr(L, s)]
     assert not missing, missing
     assert len(header_functions()) >= 25
-    assert built.lib().fs_abi_version() == 1
+    assert built.lib().fs_abi_version() == built.ABI_VERSION == 2
 
 
 def test_model_counts_match_reference_rules(built):
