@@ -1,0 +1,67 @@
+"""The host code under AddressSanitizer and UndefinedBehaviorSanitizer (CPU).
+
+The flysim command line (flysim_b200/csrc/host: argv, .conf/.pro parser,
+network builder, cache, protocol loop, output writers and logs) is compiled
+with -fsanitize=address,undefined, with the CPU oracle (oracle/fs_oracle.cpp)
+standing in for the GPU engine (tests/asan_oracle_engine.cpp), and run on
+every golden case with the reference's own flags: no sanitizer report, and
+every output file and both logs byte-identical to what the reference wrote.
+The sanitizers are the race and memory checks the GPU side cannot have on
+this pool (compute-sanitizer is closed), applied to the code around it.
+"""
+import filecmp
+import json
+import os
+import shutil
+import subprocess
+
+import pytest
+
+from conftest import GOLDEN, ROOT, compare_outputs, file_digest, golden_cases
+
+HOST = os.path.join(ROOT, "flysim_b200", "csrc", "host")
+SAN = ["-fsanitize=address,undefined", "-fno-sanitize-recover=all", "-fno-omit-frame-pointer", "-O1", "-g"]
+
+
+@pytest.fixture(scope="module")
+def flysim_asan(tmp_path_factory):
+    if not shutil.which("g++"):
+        pytest.skip("no g++")
+    d = tmp_path_factory.mktemp("asan")
+    objs = []
+    srcs = [os.path.join(HOST, f + ".cpp") for f in
+            ("fs_cli", "fs_parse", "fs_build", "fs_cache", "fs_driver", "fs_model_api", "fs_netlog")]
+    srcs += [os.path.join(ROOT, "oracle", "fs_oracle.cpp"), os.path.join(ROOT, "tests", "asan_oracle_engine.cpp")]
+    for s in srcs:
+        o = str(d / (os.path.basename(s) + ".o"))
+        subprocess.run(["g++", "-std=c++17", *SAN, "-I", os.path.join(ROOT, "include"), "-I", HOST, "-c", s, "-o", o],
+                       check=True)
+        objs.append(o)
+    o = str(d / "fs_philox.o")
+    subprocess.run(["gcc", *SAN, "-I", os.path.join(ROOT, "include"), "-c",
+                    os.path.join(ROOT, "oracle", "fs_philox.c"), "-o", o], check=True)
+    objs.append(o)
+    exe = str(d / "flysim_asan")
+    subprocess.run(["g++", *SAN, *objs, "-o", exe, "-lpthread"], check=True)
+    return exe
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_cli_under_sanitizers_matches_reference(flysim_asan, case, tmp_path):
+    src = os.path.join(GOLDEN, case)
+    for f in ("net.conf", "net.pro"):
+        shutil.copy(os.path.join(src, f), str(tmp_path / f))
+    flags = json.load(open(os.path.join(src, "cmd.json")))
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=1:halt_on_error=1",
+               UBSAN_OPTIONS="halt_on_error=1:print_stacktrace=1")
+    r = subprocess.run([flysim_asan, "-conf", "net.conf", "-pro", "net.pro", *flags], cwd=str(tmp_path),
+                       capture_output=True, text=True, timeout=900, env=env)
+    report = r.stderr[-4000:]
+    assert r.returncode == 0, report
+    assert "runtime error" not in r.stderr and "Sanitizer" not in r.stderr, report
+    bad = compare_outputs(case, str(tmp_path))
+    assert not bad, bad
+    logs = json.load(open(os.path.join(src, "logs.json")))
+    for name in ("ConfsInfo.log", "network.log"):
+        assert file_digest(str(tmp_path / name)) == logs[name], name
+    assert filecmp.cmp(os.path.join(src, "net.conf"), str(tmp_path / "net.conf"), shallow=False)
