@@ -443,8 +443,23 @@ int run_protocol(Model &m, const fs_engine_vtbl *eng, void *ctx, const std::stri
       std::function<void()> f;
       ~Joiner() { f(); }
     } joiner{join};
+    // progress every 100 ms simulated, as the reference prints it
+    // (code/NetSimGnl2.cpp:169-188, :238-257, ReportStep = 100/dt at :271)
+    const unsigned long long report_step = std::max(1u, (unsigned)(100.0f / dt));
     for (; (i < endtime) || nolmt; i++) {
       int erc = 0;
+      if (i % report_step == 0) {
+        const double el = std::chrono::duration_cast<std::chrono::nanoseconds>(
+                              std::chrono::high_resolution_clock::now() - t1).count() * 1e-9;
+        const float evt = (float)i * dt;
+        if (nolmt)
+          std::printf("Expertment time=%.7gs real time=%.7gs :infinity End time             \r",
+                      (double)(evt * 1e-3f), el);
+        else
+          std::printf("Expertment time=%.7gs real time=%.7gs %.7g%%             \r", (double)(evt * 1e-3f), el,
+                      (double)(100.0f * (float)(i + 1) / (float)endtime));
+        std::fflush(stdout);
+      }
       if (events_at(i, false, erc)) {
         int r = flush();
         if (r) return fail(r);
