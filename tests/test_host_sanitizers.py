@@ -1,15 +1,16 @@
-"""The host code under AddressSanitizer and UndefinedBehaviorSanitizer (CPU).
+"""The host code under AddressSanitizer, UndefinedBehaviorSanitizer and
+ThreadSanitizer (CPU).
 
 The flysim command line (flysim_b200/csrc/host: argv, .conf/.pro parser,
 network builder, cache, protocol loop, output writers and logs) is compiled
 with -fsanitize=address,undefined, with the CPU oracle (oracle/fs_oracle.cpp)
 standing in for the GPU engine (tests/asan_oracle_engine.cpp), and run on
 every golden case with the reference's own flags: no sanitizer report, and
-every output file and both logs byte-identical to what the reference wrote.
+every output file and both logs byte-identical to what the reference wrote;
+under ThreadSanitizer on a few cases and on the set-up with four threads.
 The sanitizers are the race and memory checks the GPU side cannot have on
 this pool (compute-sanitizer is closed), applied to the code around it.
 """
-import filecmp
 import json
 import os
 import shutil
@@ -21,41 +22,48 @@ from conftest import GOLDEN, ROOT, compare_outputs, file_digest, golden_cases
 
 HOST = os.path.join(ROOT, "flysim_b200", "csrc", "host")
 SAN = ["-fsanitize=address,undefined", "-fno-sanitize-recover=all", "-fno-omit-frame-pointer", "-O1", "-g"]
+TSAN = ["-fsanitize=thread", "-O1", "-g"]
 
 
-@pytest.fixture(scope="module")
-def flysim_asan(tmp_path_factory):
+def _build(tmp_path_factory, name, flags):
     if not shutil.which("g++"):
         pytest.skip("no g++")
-    d = tmp_path_factory.mktemp("asan")
+    d = tmp_path_factory.mktemp(name)
     objs = []
     srcs = [os.path.join(HOST, f + ".cpp") for f in
             ("fs_cli", "fs_parse", "fs_build", "fs_cache", "fs_driver", "fs_model_api", "fs_netlog")]
     srcs += [os.path.join(ROOT, "oracle", "fs_oracle.cpp"), os.path.join(ROOT, "tests", "asan_oracle_engine.cpp")]
     for s in srcs:
         o = str(d / (os.path.basename(s) + ".o"))
-        subprocess.run(["g++", "-std=c++17", *SAN, "-I", os.path.join(ROOT, "include"), "-I", HOST, "-c", s, "-o", o],
+        subprocess.run(["g++", "-std=c++17", *flags, "-I", os.path.join(ROOT, "include"), "-I", HOST, "-c", s, "-o", o],
                        check=True)
         objs.append(o)
     o = str(d / "fs_philox.o")
-    subprocess.run(["gcc", *SAN, "-I", os.path.join(ROOT, "include"), "-c",
+    subprocess.run(["gcc", *flags, "-I", os.path.join(ROOT, "include"), "-c",
                     os.path.join(ROOT, "oracle", "fs_philox.c"), "-o", o], check=True)
     objs.append(o)
-    exe = str(d / "flysim_asan")
-    subprocess.run(["g++", *SAN, *objs, "-o", exe, "-lpthread"], check=True)
+    exe = str(d / name)
+    subprocess.run(["g++", *flags, *objs, "-o", exe, "-lpthread"], check=True)
     return exe
 
 
-@pytest.mark.parametrize("case", golden_cases())
-def test_cli_under_sanitizers_matches_reference(flysim_asan, case, tmp_path):
+@pytest.fixture(scope="module")
+def flysim_asan(tmp_path_factory):
+    return _build(tmp_path_factory, "flysim_asan", SAN)
+
+
+@pytest.fixture(scope="module")
+def flysim_tsan(tmp_path_factory):
+    return _build(tmp_path_factory, "flysim_tsan", TSAN)
+
+
+def _run_case(exe, case, tmp_path, env):
     src = os.path.join(GOLDEN, case)
     for f in ("net.conf", "net.pro"):
         shutil.copy(os.path.join(src, f), str(tmp_path / f))
     flags = json.load(open(os.path.join(src, "cmd.json")))
-    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=1:halt_on_error=1",
-               UBSAN_OPTIONS="halt_on_error=1:print_stacktrace=1")
-    r = subprocess.run([flysim_asan, "-conf", "net.conf", "-pro", "net.pro", *flags], cwd=str(tmp_path),
-                       capture_output=True, text=True, timeout=900, env=env)
+    r = subprocess.run([exe, "-conf", "net.conf", "-pro", "net.pro", *flags], cwd=str(tmp_path),
+                       capture_output=True, text=True, timeout=900, env=dict(os.environ, **env))
     report = r.stderr[-4000:]
     assert r.returncode == 0, report
     assert "runtime error" not in r.stderr and "Sanitizer" not in r.stderr, report
@@ -64,4 +72,30 @@ def test_cli_under_sanitizers_matches_reference(flysim_asan, case, tmp_path):
     logs = json.load(open(os.path.join(src, "logs.json")))
     for name in ("ConfsInfo.log", "network.log"):
         assert file_digest(str(tmp_path / name)) == logs[name], name
-    assert filecmp.cmp(os.path.join(src, "net.conf"), str(tmp_path / "net.conf"), shallow=False)
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_cli_under_sanitizers_matches_reference(flysim_asan, case, tmp_path):
+    _run_case(flysim_asan, case, tmp_path, {"ASAN_OPTIONS": "detect_leaks=1:halt_on_error=1",
+                                            "UBSAN_OPTIONS": "halt_on_error=1:print_stacktrace=1"})
+
+
+@pytest.mark.parametrize("case", ["two_pop", "repeats", "cli_flags"])
+def test_cli_under_thread_sanitizer(flysim_tsan, case, tmp_path):
+    # the formatter thread that writes a chunk's files while the engine
+    # computes the next, the threaded network.log and the -t set-up
+    _run_case(flysim_tsan, case, tmp_path, {"TSAN_OPTIONS": "halt_on_error=1:second_deadlock_stack=1"})
+
+
+def test_threaded_setup_under_thread_sanitizer(flysim_tsan, tmp_path):
+    # -t 4: the set-up's draws as the reference's four threads make them,
+    # pinned by the network.log of the reference's -t 4 run
+    src = os.path.join(GOLDEN, "two_pop")
+    for f in ("net.conf", "net.pro"):
+        shutil.copy(os.path.join(src, f), str(tmp_path / f))
+    r = subprocess.run([flysim_tsan, "-conf", "net.conf", "-pro", "net.pro", "-t", "4"], cwd=str(tmp_path),
+                       capture_output=True, text=True, timeout=900,
+                       env=dict(os.environ, TSAN_OPTIONS="halt_on_error=1"))
+    assert r.returncode == 0 and "Sanitizer" not in r.stderr, r.stderr[-4000:]
+    logs = json.load(open(os.path.join(src, "logs.json")))
+    assert file_digest(str(tmp_path / "network.log")) == logs["network.log -t 4"]
