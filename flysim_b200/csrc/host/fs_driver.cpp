@@ -204,6 +204,21 @@ int run_protocol(Model &m, const fs_engine_vtbl *eng, void *ctx, const std::stri
         return FS_ERR_IO;
       }
     }
+    // every return from here on closes the files with what was computed
+    // written out (an engine error mid-run leaves complete files up to the
+    // last finished chunk); it runs after the formatter thread has joined
+    // (the joiner below is destroyed first)
+    struct Closer {
+      std::vector<OutFile> &v;
+      ~Closer() {
+        for (OutFile &x : v) {
+          if (!x.f) continue;
+          if (!x.buf.empty()) std::fwrite(x.buf.data(), 1, x.buf.size(), x.f);
+          std::fclose(x.f);
+          x.f = nullptr;
+        }
+      }
+    } closer{files};
     std::printf("Iteration:%d\n", rep);
 
     // FileOut for one step
@@ -488,6 +503,8 @@ int run_protocol(Model &m, const fs_engine_vtbl *eng, void *ctx, const std::stri
     for (size_t k = 0; k < files.size(); k++) {
       if (!files[k].buf.empty()) std::fwrite(files[k].buf.data(), 1, files[k].buf.size(), files[k].f);
       std::fclose(files[k].f);
+      files[k].f = nullptr;
+      files[k].buf.clear();
     }
   }
   if (run_seconds) *run_seconds = total_run;

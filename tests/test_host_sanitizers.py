@@ -99,3 +99,34 @@ def test_threaded_setup_under_thread_sanitizer(flysim_tsan, tmp_path):
     assert r.returncode == 0 and "Sanitizer" not in r.stderr, r.stderr[-4000:]
     logs = json.load(open(os.path.join(src, "logs.json")))
     assert file_digest(str(tmp_path / "network.log")) == logs["network.log -t 4"]
+
+
+def test_engine_failure_mid_run_is_reported_cleanly(flysim_asan, tmp_path):
+    # host-side fault injection: the second chunk's step call fails as a
+    # device error would (FLYSIM_TEST_FAIL_STEP, tests/asan_oracle_engine.cpp).
+    # The run stops with an error status and message, the formatter thread
+    # joins, every output file is closed with the first chunk's steps in it
+    # (a prefix of the reference's file), and nothing leaks
+    src = os.path.join(GOLDEN, "two_pop")
+    for f in ("net.conf", "net.pro"):
+        shutil.copy(os.path.join(src, f), str(tmp_path / f))
+    r = subprocess.run([flysim_asan, "-conf", "net.conf", "-pro", "net.pro"], cwd=str(tmp_path),
+                       capture_output=True, text=True, timeout=900,
+                       env=dict(os.environ, FLYSIM_TEST_FAIL_STEP="2", ASAN_OPTIONS="detect_leaks=1",
+                                UBSAN_OPTIONS="halt_on_error=1"))
+    assert r.returncode != 0
+    assert "flysim:" in r.stderr and "Sanitizer" not in r.stderr, r.stderr[-4000:]
+    got = open(str(tmp_path / "Spikes.dat"), "rb").read()
+    ref = open(os.path.join(src, "Spikes.dat"), "rb").read()
+    assert 0 < len(got) < len(ref) and ref.startswith(got)
+
+
+def test_unwritable_output_is_an_error(flysim_asan, tmp_path):
+    src = os.path.join(GOLDEN, "two_pop")
+    for f in ("net.conf", "net.pro"):
+        shutil.copy(os.path.join(src, f), str(tmp_path / f))
+    r = subprocess.run([flysim_asan, "-conf", "net.conf", "-pro", "net.pro", "-os", "no_such_dir/Spikes.dat"],
+                       cwd=str(tmp_path), capture_output=True, text=True, timeout=900,
+                       env=dict(os.environ, ASAN_OPTIONS="detect_leaks=1", UBSAN_OPTIONS="halt_on_error=1"))
+    assert r.returncode != 0
+    assert "cannot open output file" in r.stderr and "Sanitizer" not in r.stderr, r.stderr[-4000:]
