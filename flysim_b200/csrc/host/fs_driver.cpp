@@ -169,8 +169,14 @@ int run_protocol(Model &m, const fs_engine_vtbl *eng, void *ctx, const std::stri
   for (int rep = 1; rep <= rp; rep++) {
     const Event &last = m.events.back();
     const bool nolmt = last.NoLmt;
-    const unsigned long long endtime = (unsigned long long)std::floor(last.TimEv * 1e3f / dt);
-    const unsigned one_ms = (unsigned)(1u / dt);
+    // Endtime = floor(T*1e3f/dt) (code/NetSimGnl2.cpp:270); a NoLimit run's
+    // FLT_MAX time overflows it, and the loop ignores it then
+    const float endf = std::floor(last.TimEv * 1e3f / dt);
+    const unsigned long long endtime =
+        (endf >= 0.0f && endf < 1.8e19f) ? (unsigned long long)endf : (endf >= 0.0f ? ~0ull : 0ull);
+    // steps per ms (1/dt); at least 1, so a step above 1 ms divides by 1 in
+    // the rate writer where the reference would divide by 0
+    const unsigned one_ms = std::max(1u, (unsigned)(1u / dt));
     // VarInit + reseed (code/NetSimGnl2.cpp:277, :319-323)
     int rc = eng->reset(ctx, m.rseeds[rep - 1], m.rseeds[rep - 1]);
     if (rc) return fail(rc);

@@ -1,4 +1,5 @@
 // C ABI of the host model (parser + builder + protocol driver).
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <mutex>
@@ -39,7 +40,7 @@ int fs_model_load_cached(const char *conf_path, const char *pro_path, const fs_m
   o.threads = 1;
   o.repeats = 1;
   if (opts) o = *opts;
-  if (!(o.dt > 0.0f)) o.dt = 0.1f;
+  if (!(o.dt > 0.0f) || !std::isfinite(o.dt)) o.dt = 0.1f;
   if (o.threads < 1) o.threads = 1;
   if (o.repeats < 1) o.repeats = 1;
   uint64_t key = 0;

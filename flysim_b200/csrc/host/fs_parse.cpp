@@ -103,6 +103,36 @@ float to_f(const std::string &s, const char *what) {
   }
 }
 
+// Values the reference uses as sizes, divisors or step counts without a
+// check (a negative N wraps its allocation, a zero FiringRateWindow divides
+// by zero, a NaN event time breaks the event sort): here they are errors
+// that name the keyword, where the reference crashes or runs undefined.
+uint32_t to_count(const std::string &s, const char *what) {
+  const int v = to_i(s, what);
+  if (v < 0) throw ParseError(std::string(what) + " must not be negative, got '" + s + "'");
+  return (uint32_t)v;
+}
+// a duration in ms rounded up to whole ms, at least 1
+uint32_t to_whole_ms(const std::string &s, const char *what) {
+  const float x = to_f(s, what);
+  if (!(x > 0.0f) || !(x < 2147483648.0f))
+    throw ParseError(std::string(what) + " must be a positive number of ms, got '" + s + "'");
+  return (uint32_t)std::ceil(x);
+}
+// a finite number
+float to_finite(const std::string &s, const char *what) {
+  const float x = to_f(s, what);
+  if (!std::isfinite(x)) throw ParseError(std::string(what) + " must be a finite number, got '" + s + "'");
+  return x;
+}
+// floor(x / dt) (+ add) as the reference's int members take it
+int to_steps(const std::string &s, const char *what, float dt, float add = 0.0f) {
+  const float v = std::floor(to_finite(s, what) / dt) + add;
+  if (!(v > -2147483648.0f && v < 2147483648.0f))
+    throw ParseError(std::string(what) + " is out of range, got '" + s + "'");
+  return (int)v;
+}
+
 // Receptor names of STATE_RepName / STATE_NeuCon_TarRep (code/parser.cpp:732-745, :844-857);
 // unknown names leave kw unchanged, as the reference's shared KwTmp does.
 void receptor_kw(const std::string &s, unsigned &kw) {
@@ -250,7 +280,7 @@ void parse_conf(Model &m, const std::string &path, int &state) {
           state = ST_Initial;
         }
         break;
-      case ST_N: pop().N = (uint32_t)to_i(s1, "N"); state = ST_NeuPopu; break;
+      case ST_N: pop().N = to_count(s1, "N"); state = ST_NeuPopu; break;
       case ST_Taum: pop().Taum = to_f(s1, "Taum"); state = ST_NeuPopu; break;
       case ST_Vth: pop().Vth = to_f(s1, "Threshold"); state = ST_NeuPopu; break;
       case ST_gl: pop().gl = to_f(s1, "LeakyConductance"); state = ST_NeuPopu; break;
@@ -258,11 +288,11 @@ void parse_conf(Model &m, const std::string &path, int &state) {
       case ST_Vreset: pop().Vreset = to_f(s1, "ResetPot"); state = ST_NeuPopu; break;
       case ST_Vresting: pop().El = to_f(s1, "RestPot"); state = ST_NeuPopu; break;
       case ST_RfPed:  // int member assigned floor(x/dt)+dt (code/parser.cpp:508)
-        pop().RfPed = (int)(std::floor(to_f(s1, "RefractoryPeriod") / dt) + dt);
+        pop().RfPed = to_steps(s1, "RefractoryPeriod", dt, dt);
         state = ST_NeuPopu;
         break;
       case ST_SpiDy:
-        pop().SpiDy = (int)std::floor(to_f(s1, "SpikeDly") / dt);
+        pop().SpiDy = to_steps(s1, "SpikeDly", dt);
         state = ST_NeuPopu;
         break;
       case ST_STP_pv: pop().pv = to_f(s1, "STP_pv"); state = ST_NeuPopu; break;
@@ -275,7 +305,7 @@ void parse_conf(Model &m, const std::string &path, int &state) {
       case ST_STP_tCar: pop().tCar = to_f(s1, "STP_tCar"); state = ST_NeuPopu; break;
       case ST_LTP_tLP: pop().tLP = to_f(s1, "LTP_tLP"); state = ST_NeuPopu; break;
       case ST_LTP_SpiLPDy:
-        pop().SpiLPDy = (int)std::floor(to_f(s1, "LTP_SpiLPDy") / dt);
+        pop().SpiLPDy = to_steps(s1, "LTP_SpiLPDy", dt);
         state = ST_NeuPopu;
         break;
       case ST_LTP_PosISI: pop().PosISI = to_f(s1, "LTP_PosISI"); state = ST_NeuPopu; break;
@@ -327,6 +357,8 @@ void parse_conf(Model &m, const std::string &path, int &state) {
         break;
       case ST_NeuCon_Conct: {
         float c = to_f(s1, "Connectivity");
+        if (!(c >= 0.0f))  // the target count ceil(N*c) would wrap (the reference's does)
+          throw ParseError("Connectivity must be a number in [0, 1], got '" + s1 + "'");
         if (c > 1.0f) c = 1.0f;  // code/parser.cpp:836
         link().conn = c;
         state = ST_NeuCon;
@@ -417,7 +449,7 @@ void parse_pro(Model &m, const std::string &path, int &state) {
           ev.TimEv = FLT_MAX;
         } else {
           ev.NoLmt = false;
-          ev.TimEv = to_f(s1, "EventTime") * 1e-3f;
+          ev.TimEv = to_finite(s1, "EventTime") * 1e-3f;
         }
         state = ST_TimEvDef;
         break;
@@ -500,8 +532,8 @@ void parse_pro(Model &m, const std::string &path, int &state) {
         else if (s1 == "DeltaMemPotLimit") { of.Type = s1; of.TypeID = OUT_DVOVF; }
         state = ST_OutCtr;
         break;
-      case ST_OutRWin: of.RWin = (uint32_t)std::ceil(to_f(s1, "FiringRateWindow")); state = ST_OutCtr; break;
-      case ST_OutFPnt: of.FPnt = (uint32_t)std::ceil(to_f(s1, "PrintStep")); state = ST_OutCtr; break;
+      case ST_OutRWin: of.RWin = to_whole_ms(s1, "FiringRateWindow"); state = ST_OutCtr; break;
+      case ST_OutFPnt: of.FPnt = to_whole_ms(s1, "PrintStep"); state = ST_OutCtr; break;
       case ST_OutSumAllPp:
         if (s1 == "true") of.Status |= OF_SUMALL; else of.Status &= ~(uint32_t)OF_SUMALL;
         state = ST_OutCtr;

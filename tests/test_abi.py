@@ -124,3 +124,25 @@ def test_array_network_matches_conf_builder(built, tmp_path):
         np.testing.assert_array_equal(a, na.fields[k])
     pb = np.ctypeslib.as_array(d.neurons.pb, (5 * c.n,))
     np.testing.assert_allclose(pb, na.fields["pb"], rtol=1e-6)
+
+
+def test_values_the_reference_leaves_undefined_are_parse_errors(built, tmp_path):
+    # a negative population size, a NaN connectivity and a zero rate window:
+    # the reference wraps an allocation, a target count or divides by zero;
+    # here each is FS_ERR_PARSE naming the keyword
+    d = os.path.join(GOLDEN, "keywords")
+    conf, pro = open(os.path.join(d, "net.conf")).read(), open(os.path.join(d, "net.pro")).read()
+    cases = [("net.conf", "N=30", "N=-1", "N"), ("net.conf", "Connectivity=0.3", "Connectivity=nan", "Connectivity")]
+    if "FiringRateWindow=" in pro:
+        import re
+        w = re.search(r"FiringRateWindow=[0-9.]+", pro).group(0)
+        cases.append(("net.pro", w, "FiringRateWindow=0", "FiringRateWindow"))
+    for which, old, new, key in cases:
+        text = {"net.conf": conf, "net.pro": pro}[which]
+        assert old in text, old
+        c, p = str(tmp_path / "c.conf"), str(tmp_path / "p.pro")
+        open(c, "w").write(conf.replace(old, new, 1) if which == "net.conf" else conf)
+        open(p, "w").write(pro.replace(old, new, 1) if which == "net.pro" else pro)
+        with pytest.raises(built.FsError) as ei:
+            built.Model(c, p)
+        assert ei.value.code == built.FS_ERR_PARSE and key in str(ei.value), str(ei.value)

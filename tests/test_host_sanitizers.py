@@ -21,7 +21,7 @@ import pytest
 from conftest import GOLDEN, ROOT, compare_outputs, file_digest, golden_cases
 
 HOST = os.path.join(ROOT, "flysim_b200", "csrc", "host")
-SAN = ["-fsanitize=address,undefined", "-fno-sanitize-recover=all", "-fno-omit-frame-pointer", "-O1", "-g"]
+SAN = ["-fsanitize=address,undefined,float-cast-overflow", "-fno-sanitize-recover=all", "-fno-omit-frame-pointer", "-O1", "-g"]
 TSAN = ["-fsanitize=thread", "-O1", "-g"]
 
 
@@ -130,3 +130,46 @@ def test_unwritable_output_is_an_error(flysim_asan, tmp_path):
                        env=dict(os.environ, ASAN_OPTIONS="detect_leaks=1", UBSAN_OPTIONS="halt_on_error=1"))
     assert r.returncode != 0
     assert "cannot open output file" in r.stderr and "Sanitizer" not in r.stderr, r.stderr[-4000:]
+
+
+def _mutations(text, seed, k_trunc=6, k_del=6, k_num=12):
+    """Deterministic damaged variants of an input file: truncations, a line
+    deleted, a number replaced by garbage or an out-of-range value."""
+    import random
+    import re
+    rng = random.Random(seed)
+    lines = text.split("\n")
+    out = [text[: len(text) * k // (k_trunc + 1)] for k in range(1, k_trunc + 1)]
+    for _ in range(k_del):
+        i = rng.randrange(len(lines))
+        out.append("\n".join(lines[:i] + lines[i + 1:]))
+    nums = list(re.finditer(r"-?\d+(\.\d+)?(e-?\d+)?", text))
+    for _ in range(k_num):
+        m = rng.choice(nums)
+        out.append(text[: m.start()] + rng.choice(["abc", "", "-1", "0", "0.5", "nan", "-0.2", "inf9", "-7e20"])
+                   + text[m.end():])
+    return out
+
+
+@pytest.mark.parametrize("case,which", [("small", "net.conf"), ("small", "net.pro"),
+                                        ("keywords", "net.conf"), ("keywords", "net.pro")])
+def test_damaged_inputs_run_or_fail_cleanly(flysim_asan, case, which, tmp_path):
+    # every damaged .conf / .pro either runs or ends with an error message:
+    # no sanitizer report, no signal (the reference crashes or runs undefined
+    # on several of them: a negative N, a NaN connectivity, a zero
+    # FiringRateWindow)
+    src = os.path.join(GOLDEN, case)
+    base = open(os.path.join(src, which)).read()
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=1", UBSAN_OPTIONS="halt_on_error=1:print_stacktrace=1")
+    for v, text in enumerate(_mutations(base, seed=len(base))):
+        d = tmp_path / str(v)
+        d.mkdir()
+        for f in ("net.conf", "net.pro"):
+            shutil.copy(os.path.join(src, f), str(d / f))
+        (d / which).write_text(text)
+        r = subprocess.run([flysim_asan, "-conf", "net.conf", "-pro", "net.pro"], cwd=str(d), capture_output=True,
+                           text=True, timeout=120, env=env)
+        assert r.returncode >= 0, (v, r.stderr[-3000:])
+        assert "Sanitizer" not in r.stderr and "runtime error" not in r.stderr, (v, r.stderr[-3000:])
+        if r.returncode:
+            assert "flysim:" in r.stderr, (v, r.stderr[-3000:])
