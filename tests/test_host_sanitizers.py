@@ -74,13 +74,15 @@ def _run_case(exe, case, tmp_path, env):
         assert file_digest(str(tmp_path / name)) == logs[name], name
 
 
-@pytest.mark.parametrize("case", golden_cases())
+# config1_1s is two_pop's network for a full second (a minute under the
+# sanitizers); tests/test_oracle_ref.py runs it through the oracle
+@pytest.mark.parametrize("case", [c for c in golden_cases() if c != "config1_1s"])
 def test_cli_under_sanitizers_matches_reference(flysim_asan, case, tmp_path):
     _run_case(flysim_asan, case, tmp_path, {"ASAN_OPTIONS": "detect_leaks=1:halt_on_error=1",
                                             "UBSAN_OPTIONS": "halt_on_error=1:print_stacktrace=1"})
 
 
-@pytest.mark.parametrize("case", ["two_pop", "repeats", "cli_flags"])
+@pytest.mark.parametrize("case", ["conn", "repeats", "cli_flags"])
 def test_cli_under_thread_sanitizer(flysim_tsan, case, tmp_path):
     # the formatter thread that writes a chunk's files while the engine
     # computes the next, the threaded network.log and the -t set-up
@@ -90,7 +92,7 @@ def test_cli_under_thread_sanitizer(flysim_tsan, case, tmp_path):
 def test_threaded_setup_under_thread_sanitizer(flysim_tsan, tmp_path):
     # -t 4: the set-up's draws as the reference's four threads make them,
     # pinned by the network.log of the reference's -t 4 run
-    src = os.path.join(GOLDEN, "two_pop")
+    src = os.path.join(GOLDEN, "conn")
     for f in ("net.conf", "net.pro"):
         shutil.copy(os.path.join(src, f), str(tmp_path / f))
     r = subprocess.run([flysim_tsan, "-conf", "net.conf", "-pro", "net.pro", "-t", "4"], cwd=str(tmp_path),
