@@ -175,3 +175,39 @@ def test_damaged_inputs_run_or_fail_cleanly(flysim_asan, case, which, tmp_path):
         assert "Sanitizer" not in r.stderr and "runtime error" not in r.stderr, (v, r.stderr[-3000:])
         if r.returncode:
             assert "flysim:" in r.stderr, (v, r.stderr[-3000:])
+
+
+def test_damaged_cache_is_rebuilt_under_sanitizers(flysim_asan, tmp_path):
+    # a network cache with flipped bytes (header, payload, hash) or cut
+    # short is never trusted: the run rebuilds from the text files and writes
+    # the reference's outputs, with no sanitizer report
+    case = "keywords"
+    src = os.path.join(GOLDEN, case)
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=1", UBSAN_OPTIONS="halt_on_error=1:print_stacktrace=1")
+
+    def run(d, cache):
+        for f in ("net.conf", "net.pro"):
+            shutil.copy(os.path.join(src, f), str(d / f))
+        flags = json.load(open(os.path.join(src, "cmd.json")))
+        r = subprocess.run([flysim_asan, "-conf", "net.conf", "-pro", "net.pro", "-cache", cache, *flags],
+                           cwd=str(d), capture_output=True, text=True, timeout=300, env=env)
+        assert r.returncode == 0 and "Sanitizer" not in r.stderr and "runtime error" not in r.stderr, \
+            r.stderr[-3000:]
+        assert not compare_outputs(case, str(d))
+        return r.stdout
+
+    cache = str(tmp_path / "net.cache")
+    first = tmp_path / "first"
+    first.mkdir()
+    run(first, cache)
+    good = open(cache, "rb").read()
+    assert len(good) > 64
+    cuts = [8, 20, len(good) // 2, len(good) - 3]
+    flips = [0, 9, 13, 17, 30, len(good) // 3, len(good) // 2, len(good) - 12, len(good) - 1]
+    damaged = [good[:c] for c in cuts] + [good[:i] + bytes([good[i] ^ 0x5A]) + good[i + 1:] for i in flips]
+    for v, blob in enumerate(damaged):
+        open(cache, "wb").write(blob)
+        d = tmp_path / ("v%d" % v)
+        d.mkdir()
+        out = run(d, cache)
+        assert "network read from cache" not in out, v
