@@ -568,8 +568,14 @@ def main():
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "note": "%s peak; algorithmic bytes per launch %.3g over %.2f ms (mean launch)"
-                                 % (peak_kind, alg, k_ms)},
+                         # the same launch measured by the DRAM bytes ncu counted (traffic)
+                         "dram_frac": (traffic / (k_ms * 1e-3) / 1e9 / peak) if traffic else None,
+                         "note": ("%s peak; algorithmic bytes per launch %.3g over %.2f ms (mean launch)"
+                                  % (peak_kind, alg, k_ms)) +
+                                 ("; the working set is L2-resident, so frac (algorithmic bytes) is nominal and "
+                                  "dram_frac (the ncu-counted DRAM bytes) is what reached HBM: the kernel is bound "
+                                  "by synchronisation and latency (profiles/k_prod_fp32_connectome20k_ncu.md)"
+                                  if ws < 100 else "")},
             "clocks": clk,
             "e2e": e2e,
             "cpu_baseline": cpu,
