@@ -138,6 +138,16 @@ def cases():
                                 with_delays=False)
     c["conn_ltp"] = dict(conf=conn_ltp, pro=dict(t_end_ms=200, seeds=(4,), outputs=OUTS), flags=["-LTP"])
 
+    # LTP keywords strong enough to move the weights within a trial, and two
+    # repeats: the reference's VarInit leaves the records' weights as LTP
+    # left them (code/EqsGnl2.cpp:339-401), so the second trial starts from
+    # the first trial's weights
+    def ltp_repeats(p):
+        netgen.write_connectome(netgen.connectome(n=150, regions=5, mean_degree=20, delays=False, seed=8), p,
+                                with_delays=False, ltp=dict(tLP=30, SpiLPDy=0.2, PosISI=0.05, NegISI=-0.02))
+    c["ltp_repeats"] = dict(conf=ltp_repeats, pro=dict(t_end_ms=150, seeds=(4, 6), outputs=OUTS),
+                            flags=["-LTP", "-rp", "2"])
+
     def conn(p):
         netgen.write_connectome(netgen.connectome(n=400, regions=8, mean_degree=40, delays=False, seed=2), p,
                                 with_delays=False)
