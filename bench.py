@@ -264,6 +264,51 @@ def same_network_block(c, args, world, rank, flush, barrier, cap_hint: float):
         eng.close()
 
 
+def scaled_network_block(args):
+    """The scaled network (1,000,000 neurons, ~100 M connections,
+    Tsodyks-Markram plasticity; the tile kernels) measured beside the
+    headline: device value over the launches of two 1 s steps after one
+    warm-up step (inputs far beyond L2), its launch time and the roofline by
+    algorithmic bytes and by the DRAM bytes ncu counted per timestep
+    (profiles/prod_fp32_scaled1m_traffic.json)."""
+    import flysim_b200 as fb
+    c, na = build_network(0, "scaled1m")
+    eng = fb.Engine(na.desc, "fp32", chunk_steps=STEPS_PER_BENCH_STEP)
+    try:
+        eng.reset(SEED)
+        eng.run_timed(STEPS_PER_BENCH_STEP)
+        s0 = eng.stats()
+        k = 2
+        ms = [eng.run_timed(STEPS_PER_BENCH_STEP) for _ in range(k)]
+        kern = eng.kernel_time()[0]
+        s1 = eng.stats()
+        layout = eng.layout()
+    finally:
+        eng.close()
+    tot = float(np.sum(ms))
+    spikes = s1["spikes"] - s0["spikes"]
+    lin = na.syn["rec"] != 4
+    alg = algorithmic_bytes(na, spikes / k, STEPS_PER_BENCH_STEP, float(np.count_nonzero(lin)) / na.n, True)
+    peak, peak_kind = load_peaks()
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "prod_fp32_scaled1m_traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get("dram_bytes_per_timestep", 0) * STEPS_PER_BENCH_STEP
+    return {"workload": "connectome-shaped network: %d LIF neurons, %d connections, delays 1-5 ms, "
+                        "Tsodyks-Markram plasticity on excitatory synapses, fp32 mode; one step = 1 s "
+                        "simulated; inputs larger than L2" % (na.n, c.n_connections),
+            "value": k * STEPS_PER_BENCH_STEP * DT * 1e-3 / (tot * 1e-3), "unit": UNIT, "steps": k,
+            "us_per_timestep": 1e3 * tot / (k * STEPS_PER_BENCH_STEP), "kernels": layout["kernel"],
+            "mean_rate_hz": spikes / (k * STEPS_PER_BENCH_STEP * DT * 1e-3) / na.n,
+            "roofline": {"bound": "hbm", "achieved": alg / (tot / k * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (tot / k * 1e-3) / 1e9 / peak, "traffic": traffic,
+                         "dram_frac": (traffic / (tot / k * 1e-3) / 1e9 / peak) if traffic else None,
+                         "note": "%s peak; algorithmic bytes per 1 s step %.3g (a batch reads each NMDA "
+                                 "edge once for its 10 steps, so frac overstates what moves); dram_frac: ncu's "
+                                 "DRAM bytes per timestep (250k capture scaled by synapse entries)"
+                                 % (peak_kind, alg)}}
+
+
 def run_compat(args, rank):
     """--mode compat: the reference-order engine (the mode whose files equal
     the reference's byte for byte) on the 20k network with delays 0, read
@@ -409,6 +454,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-same-network", action="store_true",
                     help="skip the delays-0 measurement of the network the reference arm runs")
+    ap.add_argument("--no-scaled-network", action="store_true",
+                    help="skip the 1,000,000-neuron block of the default line")
     ap.add_argument("--workload", default="connectome20k", choices=sorted(WORKLOADS))
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="run this many timesteps once and exit (for ncu captures)")
@@ -537,6 +584,15 @@ def main():
     if args.workload == "connectome20k" and not args.no_same_network:
         same = same_network_block(c, args, world, rank, flush, barrier, cap_hint=spikes / max(1, args.steps))
 
+    # the scaled network beside the headline (rank 0 at N=1 only; reported,
+    # not fatal, so the headline line prints whatever happens here)
+    scaled_blk = None
+    if rank == 0 and world == 1 and args.workload == "connectome20k" and not args.no_scaled_network:
+        try:
+            scaled_blk = scaled_network_block(args)
+        except Exception as ex:
+            scaled_blk = {"error": "%s: %s" % (type(ex).__name__, ex)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -580,6 +636,7 @@ def main():
             "e2e": e2e,
             "cpu_baseline": cpu,
             "same_network": same,
+            "scaled_network": scaled_blk,
         }
         print(json.dumps(line))
     eng.close()
