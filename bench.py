@@ -630,7 +630,7 @@ def main():
                                   % (peak_kind, alg, k_ms)) +
                                  ("; the working set is L2-resident, so frac (algorithmic bytes) is nominal and "
                                   "dram_frac (the ncu-counted DRAM bytes) is what reached HBM: the kernel is bound "
-                                  "by synchronisation and latency (profiles/k_prod_fp32_connectome20k_ncu.md)"
+                                  "by synchronisation and latency (its ncu capture: 6.5 KB of DRAM traffic per timestep)"
                                   if ws < 100 else "")},
             "clocks": clk,
             "e2e": e2e,
