@@ -1,6 +1,6 @@
 // ORACLE — test infrastructure only.  Nothing in the product links, loads or
 // runs this file; only tests/, __graft_entry__.smoke() and bench.py's
-// cpu_baseline leg use it, as the checker.
+// cpu_baseline leg use it, as what the engine's results are compared with.
 //
 // A CPU restatement of the reference's per-step integration, one step at a
 // time in the reference's own order and FP32 arithmetic, over the structure of

@@ -18,8 +18,9 @@ def pytest_configure(config):
 
 @pytest.fixture(scope="session")
 def built():
-    """Native library (and the oracle) built in-tree; on a GPU box the
-    prebuilt files are used as they are."""
+    """Native library (and the oracle) built in-tree; where they already
+    exist (a GPU machine that received the built files) they are used as
+    they are."""
     from flysim_b200 import build
     lib = os.path.join(ROOT, "flysim_b200", "_build", "libflysim_b200.so")
     if not os.path.exists(lib) or os.environ.get("FS_REBUILD"):
