@@ -146,3 +146,27 @@ def test_values_the_reference_leaves_undefined_are_parse_errors(built, tmp_path)
         with pytest.raises(built.FsError) as ei:
             built.Model(c, p)
         assert ei.value.code == built.FS_ERR_PARSE and key in str(ei.value), str(ei.value)
+
+
+def test_header_is_plain_c_and_links(built, tmp_path):
+    # the boundary is a C ABI: the header compiles as C99 with warnings as
+    # errors, and a C program links against the library and calls it (no
+    # GPU is needed for the version and the device count)
+    import shutil
+    import subprocess
+    if not shutil.which("gcc"):
+        pytest.skip("no gcc")
+    src = tmp_path / "abi.c"
+    src.write_text(
+        '#include <stdio.h>\n#include "flysim_b200.h"\n'
+        "int main(void) {\n"
+        "  int n = -1;\n"
+        "  int rc = fs_device_count(&n);\n"
+        '  printf("%d %d %d\\n", fs_abi_version(), FS_ABI_VERSION, rc == FS_OK || rc == FS_ERR_NODEVICE);\n'
+        "  return 0;\n}\n")
+    lib_dir = os.path.join(ROOT, "flysim_b200", "_build")
+    exe = str(tmp_path / "abi")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    str(src), "-o", exe, "-L", lib_dir, "-lflysim_b200", "-Wl,-rpath," + lib_dir], check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
+    assert out == ["2", "2", "1"], out
