@@ -157,9 +157,13 @@ def desc_from_arrays(n: int, dt: float, fields: dict, pre, post, rec, g, delay_s
 
 
 def connectome_net(c, dt: float = 0.1, with_delays: bool = True, tm: bool = False, ext_eff: Optional[float] = None,
-                   gaba_gain: float = 1.0) -> NetArrays:
+                   gaba_gain: float = 1.0, ltp: Optional[dict] = None) -> NetArrays:
     """Production network of a :class:`flysim_b200.netgen.Connectome`: the same
-    neurons and synapses as its .conf (one population per neuron)."""
+    neurons and synapses as its .conf (one population per neuron).  ``ltp``
+    (keys tLP, SpiLPDy in ms, PosISI, NegISI) switches long-term plasticity
+    on for every neuron and synapse, as -LTP with those keywords in every
+    population does (code/NetSimGnl2_BulPp.cpp:180-183, code/parser.cpp:559-575);
+    its delays must then be 0."""
     n = c.n
     fields = neuron_fields(n, dt, receptors={
         FS_AMPA: dict(Tau=2.0, Vrev=0.0, FExt=c.freq_ext, ExtEff=c.ext_eff if ext_eff is None else ext_eff),
@@ -182,4 +186,13 @@ def connectome_net(c, dt: float = 0.1, with_delays: bool = True, tm: bool = Fals
     tmd = None
     if tm:
         tmd = dict(enabled=c.excit.astype(np.uint8), U=0.2, tau_rec=200.0, tau_fac=600.0)
-    return desc_from_arrays(n, dt, fields, pre, post, rec, g, delay, tm=tmd)
+    act_ctr = DEFAULT_ACT
+    if ltp:
+        d32 = F32(dt)
+        fields["ltp_dfLP"][:] = np.exp(-d32 / F32(ltp["tLP"]))
+        fields["ltp_SpiLPDy"][:] = int(np.floor(F32(ltp["SpiLPDy"]) / d32))
+        fields["ltp_PosISI"][:] = F32(ltp["PosISI"])
+        fields["ltp_NegISI"][:] = F32(ltp["NegISI"])
+        fields["act"] |= ACT["LTP"]
+        act_ctr |= ACT["LTP"]
+    return desc_from_arrays(n, dt, fields, pre, post, rec, g, delay, tm=tmd, act_ctr=act_ctr)

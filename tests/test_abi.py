@@ -170,3 +170,22 @@ def test_header_is_plain_c_and_links(built, tmp_path):
                     str(src), "-o", exe, "-L", lib_dir, "-lflysim_b200", "-Wl,-rpath," + lib_dir], check=True)
     out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
     assert out == ["2", "2", "1"], out
+
+
+def test_array_network_with_ltp_matches_conf_builder(built, tmp_path):
+    """connectome_net(..., ltp=...) gives the LTP parameters, activity bits
+    and global flags the .conf route gives with -LTP and the keywords."""
+    from flysim_b200 import netgen, network
+    c = netgen.connectome(n=120, regions=4, mean_degree=15, seed=9, delays=False)
+    kw = dict(tLP=30, SpiLPDy=0.2, PosISI=0.02, NegISI=-0.01)
+    conf, pro = tmp_path / "c.conf", tmp_path / "c.pro"
+    netgen.write_connectome(c, str(conf), with_delays=False, ltp=kw)
+    netgen.write_pro(str(pro), 10, seeds=(1,))
+    m = built.Model(str(conf), str(pro), ltp=True)
+    d = m.desc().contents
+    na = network.connectome_net(c, with_delays=False, ltp=kw)
+    assert d.act_ctr == na.desc.act_ctr
+    np.testing.assert_array_equal(np.ctypeslib.as_array(d.neurons.act, (c.n,)), na.fields["act"])
+    for k in ("ltp_SpiLPDy", "ltp_PosISI", "ltp_NegISI"):
+        np.testing.assert_array_equal(np.ctypeslib.as_array(getattr(d.neurons, k), (c.n,)), na.fields[k])
+    np.testing.assert_allclose(np.ctypeslib.as_array(d.neurons.ltp_dfLP, (c.n,)), na.fields["ltp_dfLP"], rtol=1e-6)
